@@ -1,0 +1,370 @@
+#!/usr/bin/env python
+"""Benchmark of the teal residual / time-integration path on B200.
+
+Workload (one GPU): compressible Navier-Stokes Taylor-Green vortex on a periodic 128^3 hex mesh over
+[0, 2pi]^3, Re 1600, Ma 0.1, Pr 0.71, gamma 1.4; Roe flux, least-squares gradients, Venkatakrishnan
+limiter (K = 1), low-storage RK {time order 3, 3 stages}, CFL 0.99, FP64. A step is one RK step
+(3 residual evaluations + update). Metric: cell-updates/s = inner cells x steps / device seconds.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--n 128] [--precision fp64]
+
+With --gpus N (launched by torchrun) every rank advances its own replica of the workload (the path is
+one mesh per GPU; there is no exchange), timed on the device, max over ranks; `value` is the
+whole-job throughput. `--impl reference` times the reference solver (compiled from its own C
+sources) on the host cores.
+"""
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s"
+WORKLOAD = "taylor-green vortex 128^3 periodic hex, navier-stokes, roe + ls gradient + venkatakrishnan(1), lserk{3,3}, cfl 0.99"
+
+
+def tgv_state(center, gamma=1.4, mach=0.1):
+    """Taylor-Green initial field (the reference's run/taylor_green_vortex/run.c:10-21)."""
+    x, y, z = center[:, 0], center[:, 1], center[:, 2]
+    p0 = 1 / (gamma * mach**2)
+    out = np.zeros((center.shape[0], 5))
+    out[:, 1] = np.sin(x) * np.cos(y) * np.cos(z)
+    out[:, 2] = -np.cos(x) * np.sin(y) * np.cos(z)
+    out[:, 4] = p0 + (np.cos(2 * x) + np.cos(2 * y)) * (np.cos(2 * z) + 2) / 16
+    out[:, 0] = out[:, 4] / p0
+    return out
+
+
+def stage_bytes(C, F, ns=True):
+    """Algorithmic HBM bytes of one residual stage (unique-footprint count, FP64): Euler
+    408 C + 184 F, Navier-Stokes + 88 C + 32 F."""
+    b = 408 * C + 184 * F
+    if ns:
+        b += 88 * C + 32 * F
+    return b
+
+
+def kernel_bytes(C, F, S, NB, ns=True, fold=False):
+    """Unique bytes each hot-path kernel of one stage must move (FP64 layout of teal_b200)."""
+    grad_state = 120 + (0 if fold else 40)
+    return {
+        # q of cells and boundary ghosts, per slot: neighbour 4 + weight 24 + offset 24; counts,
+        # eps^2; writes gradient (+ limiter factors)
+        "gradient": 40 * (C + NB) + 52 * S + 9 * C + grad_state * C,
+        # per face: cells 8, area 8, basis 72, offsets 48 (+ correction 32), G write 40; per cell:
+        # q, gradient (+ psi); ghost rows
+        "face": (176 + (32 if ns else 0)) * F + (40 + grad_state) * C + 40 * NB,
+        # slot face indices, G read once, U0, volume, q write (last stage adds R, U0, projection)
+        "cell": 4 * S + 1 * C + 40 * F + (40 + 8 + 40) * C,
+    }
+
+
+def read_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    REASONS = {
+        "sw_power_cap": "clocks_event_reasons.sw_power_cap",
+        "hw_slowdown": "clocks_event_reasons.hw_slowdown",
+        "hw_thermal_slowdown": "clocks_event_reasons.hw_thermal_slowdown",
+        "sw_thermal_slowdown": "clocks_event_reasons.sw_thermal_slowdown",
+    }
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        q = "clocks.sm,clocks.max.sm," + ",".join(self.REASONS.values())
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=5)
+        sm, smax, reasons = [], [], set()
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 2 + len(self.REASONS):
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, val in zip(self.REASONS, parts[2:]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def reference_cpu(n, steps, warmup=0):
+    """Time the reference solver's own lserk step (oracle/_ref, one core) on a TGV mesh of n^3 cells.
+    Returns (cell-updates/s, seconds, steps)."""
+    from oracle import ref
+
+    m = ref.RefMesh((0, 0, 0), (2 * math.pi,) * 3, (n, n, n), (1, 1, 1))
+    e = ref.RefEquations(m, navierstokes=True)
+    e.set_convective_flux("roe")
+    e.set_limiter("venkatakrishnan", 1.0)
+    e.set_property("dynamic viscosity", 1 / 1600)
+    c = m.arrays()["cells.center"]
+    e.set_primitive(tgv_state(c))
+    sim = ref.RefSimulation(e, "lserk", 0.99, rk=(3, 3))
+    t = 0.0
+    for _ in range(warmup):
+        t, _, _ = sim.advance(t)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        t, _, _ = sim.advance(t)
+    dt = time.perf_counter() - t0
+    C = e.num_inner
+    return C * steps / dt, dt, steps
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    from oracle import ref
+
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref not built"}))
+        return
+    n_sample = args.ref_n
+    value, secs, steps = reference_cpu(n_sample, args.steps, warmup=min(args.warmup, 1))
+    line = {
+        "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000 * secs / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample_mesh": f"{n_sample}^3", "parallelism": "1 core"},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
+                         "sample": f"{steps} lserk steps of the same TGV case on a {n_sample}^3 mesh, one core "
+                                   "(single-process build of the reference)"},
+        "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="teal_b200")
+    ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--ref-n", type=int, default=48, help="mesh size of the CPU reference sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world, rank, local = dist_setup()
+
+    if args.impl == "reference":
+        run_reference_arm(args, world, rank)
+        return
+
+    import torch
+
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+
+    import teal_b200 as tb
+
+    n = args.n
+    t0 = time.perf_counter()
+    mesh = tb.Mesh.create((0, 0, 0), (2 * math.pi,) * 3, (n, n, n), (1, 1, 1))
+    t_mesh = time.perf_counter() - t0
+    eqns = tb.Equations.navierstokes(mesh)
+    eqns.set_convective_flux("roe")
+    eqns.set_limiter("venkatakrishnan", 1.0)
+    eqns.set_property("dynamic viscosity", 1 / 1600)
+    eqns.set_initial_condition("domain", tgv_state)
+    precision = tb.TG_PRECISION_FP64 if args.precision == "fp64" else tb.TG_PRECISION_FP32_FLUX
+    t0 = time.perf_counter()
+    ctx = eqns.context(precision)
+    t_upload = time.perf_counter() - t0
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    LSERK = tb.TG_ADVANCE_LSERK
+    rk = (3, 3)
+    C = mesh.num_inner_cells
+    F = mesh.num_faces
+    s = mesh.struct
+    NB = s.off_boundary_cells - C
+    S = 2 * s.num_inner_faces + (F - s.num_inner_faces)
+
+    # warm-up (graph capture happens here)
+    ctx.run(LSERK, 0.99, args.warmup, context=rk)
+    torch.cuda.synchronize()
+
+    # timed region: K steps replayed from the step's CUDA graph, state resident in HBM
+    sampler = ClockSampler(local)
+    sampler.start()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    launches0 = ctx.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    ctx.run(LSERK, 0.99, args.steps, context=rk)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    clocks = sampler.stop()
+    launches = ctx.launch_count() - launches0
+    ms = ev0.elapsed_time(ev1)
+    if pg:
+        t = torch.tensor([ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    value = C * args.steps * world / (ms / 1000.0)
+
+    # per-kernel CUDA-event timing of the same steps (plain launches, events on the same stream)
+    ksteps = min(args.steps, 5)
+    ctx.profile(True)
+    ctx.run(LSERK, 0.99, ksteps, context=rk)
+    prof = ctx.profile_read()
+    ctx.profile(False)
+
+    # end to end through the public API: every step uploads the state from pinned host memory,
+    # advances one step and reads the state and residual back (the drop-in Advance call)
+    e2e_steps = min(args.steps, 10)
+    host_in = torch.empty((mesh.num_cells, 5), dtype=torch.float64, pin_memory=True).numpy()
+    host_out = torch.empty((mesh.num_cells, 5), dtype=torch.float64, pin_memory=True).numpy()
+    host_in[:] = ctx.get_primitive()
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    t0 = time.perf_counter()
+    tt = 0.0
+    for _ in range(e2e_steps):
+        ctx.set_primitive(host_in)
+        tt, _, res = ctx.advance(LSERK, 0.99, tt, context=rk)
+        ctx.get_primitive(host_out)
+        host_in, host_out = host_out, host_in
+    e2e_s = time.perf_counter() - t0
+    if pg:
+        t = torch.tensor([e2e_s], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = C * e2e_steps * world / e2e_s
+
+    # roofline of one RK stage (boundary + gradient + face + cell kernels)
+    peak, peak_kind = read_peaks()
+    stages = ksteps * rk[1]
+    stage_ms = sum(prof[k][0] for k in ("boundary", "gradient", "face", "cell")) / stages
+    b_stage = stage_bytes(C, F, ns=True)
+    achieved = b_stage / (stage_ms / 1000.0) / 1e9
+    kb = kernel_bytes(C, F, S, NB, ns=True, fold=False)
+    kernels = {}
+    for k in ("gradient", "face", "cell"):
+        kms, kn = prof[k]
+        if kn:
+            avg = kms / kn
+            kernels[k] = {"avg_ms": avg, "launches": kn, "unique_bytes": kb[k],
+                          "gbs": kb[k] / (avg / 1000.0) / 1e9, "share": kms / max(1e-9, sum(v[0] for v in prof.values()))}
+    dominant = max(kernels, key=lambda k: kernels[k]["avg_ms"] * kernels[k]["launches"]) if kernels else None
+
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "stage_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tr = json.load(f)
+        if tr.get("n") and tr.get("bytes_per_stage"):
+            traffic = tr["bytes_per_stage"] * (C / (tr["n"] ** 3))
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32-flux/f64-accumulate",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "cells": C, "faces": F, "mesh": f"{n}^3", "global_batch": world,
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 gpu",
+                   "l2": "inputs larger than L2 (state + geometry ~3 GB per stage)"},
+        "roofline": {"bound": "hbm", "kernel": "rk stage (boundary+gradient+face+cell)", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "peak_kind": peak_kind, "algorithmic_bytes_per_launch": b_stage,
+                     "avg_launch_ms": stage_ms},
+        "kernels": kernels, "dominant_kernel": dominant,
+        "clocks": clocks,
+        "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": host_in[: C].nbytes,
+                "d2h_bytes_per_step": host_out.nbytes + 5 * 8, "steps": e2e_steps},
+        "gpu_launches": launches,
+        "setup_s": {"mesh": t_mesh, "upload": t_upload},
+    }
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle import ref
+
+            if ref.available():
+                v, secs, st = reference_cpu(args.ref_n, 2)
+                line["cpu_baseline"] = {"value": v, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
+                                        "sample": f"{st} lserk steps of the same TGV case on a {args.ref_n}^3 mesh "
+                                                  f"({secs:.1f} s), one core"}
+        except Exception as exc:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"error": str(exc)}
+    if rank == 0:
+        print(json.dumps(line))
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,276 @@
+/*
+ * teal_b200 — C ABI of the B200 (sm_100a) residual / time-integration path of the teal
+ * finite-volume solver (compressible Euler and Navier–Stokes on unstructured meshes).
+ *
+ * Plain pointers and sizes only. Every array argument uses teal's own host layout (AoS doubles,
+ * `int` pairs) so a teal program can hand its `Mesh` / `Equations` arrays over unchanged; the
+ * library owns the device copies and never frees caller memory. All functions return TG_OK (0) or
+ * a nonzero TG_ERR_* status; `tg_last_error()` gives the message (teal itself exits through
+ * `teal_error`, src/core/teal.c:134-144; a host wrapper maps a nonzero status onto that).
+ *
+ * Reference interfaces replaced (paths inside the teal source tree):
+ *   tg_mesh               <- Mesh arrays produced by mesh_create + mesh_generate (src/mesh.h:13-72)
+ *   tg_equations          <- Equations plugin table selected by name (src/equations.h:97-111)
+ *   tg_derivative         <- equations_derivative (src/equations.h:175; equations/derivative.c:269)
+ *   tg_gradient           <- equations_gradient (+ equations_limiter) (src/equations.h:169-172)
+ *   tg_timestep           <- equations_timestep (src/equations.h:163; equations/timestep.c:7)
+ *   tg_residual           <- equations_residual (src/equations.h:178; equations/residual.c:8)
+ *   tg_advance            <- Advance methods euler / lserk / implicit_euler (src/simulation.h:6-7;
+ *                            simulation/advance.c:11-195, simulation/gmres.c:52-149)
+ *   tg_teal_{euler,lserk,implicit_euler}
+ *                         <- the same, with teal's exact `Advance` signature, for installing into
+ *                            `Simulation.advance.method` (src/simulation.h:36-41)
+ *   tg_run                <- simulation_run's step loop with the state resident on the device
+ *                            (simulation/run.c:22-113)
+ */
+#ifndef TEAL_B200_H
+#define TEAL_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ----------------------------------------------------------------------------- */
+enum {
+    TG_OK = 0,
+    TG_ERR_INVALID = 1,    /* bad argument, unsupported plugin name or mesh layout */
+    TG_ERR_CUDA = 2,       /* CUDA runtime failure (message has the CUDA error string) */
+    TG_ERR_OOM = 3,        /* device allocation failed */
+    TG_ERR_NONFINITE = 4,  /* a non-finite value reached the state or a norm */
+    TG_ERR_TIMEOUT = 5,    /* a bounded device-side wait gave up */
+    TG_ERR_NO_DEVICE = 6   /* no CUDA device / the library was built without one in reach */
+};
+
+/* ---- plugin kinds (selected by teal's names; see the *_select functions) ----------------------- */
+enum { TG_EULER = 0, TG_NAVIERSTOKES = 1 };
+
+/* convective fluxes of euler_convective (src/euler/convective.c:593-623); godunov is rejected */
+enum {
+    TG_FLUX_NONE = 0,
+    TG_FLUX_ROE = 1,
+    TG_FLUX_HLL = 2,
+    TG_FLUX_HLLC = 3,
+    TG_FLUX_HLLE = 4,
+    TG_FLUX_AUSMD = 5,
+    TG_FLUX_AUSMDV = 6,
+    TG_FLUX_LXF = 7,
+    TG_FLUX_CENTRAL = 8
+};
+
+/* viscous fluxes of navierstokes_viscous (src/navierstokes/viscous.c:41-47) */
+enum { TG_VISCOUS_NONE = 0, TG_VISCOUS_CENTRAL = 1 };
+
+/* limiter kinds, same numbering as teal's LimiterKind (src/equations/limiter.h:5-9) */
+enum { TG_LIMITER_NONE = 0, TG_LIMITER_BARTH_JESPERSEN = 1, TG_LIMITER_VENKATAKRISHNAN = 2 };
+
+/* boundary conditions of euler_boundary / navierstokes_boundary
+ * (src/euler/boundary.c:273-297, src/navierstokes/boundary.c:20-26) */
+enum {
+    TG_BC_SYMMETRY = 1, /* "symmetry", "slipwall" */
+    TG_BC_SUPERSONIC_INFLOW = 2,
+    TG_BC_SUPERSONIC_OUTFLOW = 3,
+    TG_BC_SUBSONIC_INFLOW = 4,
+    TG_BC_SUBSONIC_OUTFLOW = 5,
+    TG_BC_PRESSURE_OUTFLOW = 6,
+    TG_BC_FARFIELD = 7,
+    TG_BC_ADIABATIC_WALL = 8 /* "adiabatic wall", "wall" (Navier–Stokes only) */
+};
+
+/* time integrators of simulation_set_advance (src/simulation/set.c:74-131) */
+enum { TG_ADVANCE_EULER = 0, TG_ADVANCE_LSERK = 1, TG_ADVANCE_IMPLICIT_EULER = 2 };
+
+/* arithmetic of the face-flux path: plain FP64, or FP32 gradients/limiter/fluxes with FP64
+ * accumulation, state update and Krylov arithmetic */
+enum { TG_PRECISION_FP64 = 0, TG_PRECISION_FP32_FLUX = 1 };
+
+/* Return the kind for a teal plugin name, or -1 when teal has no such name or this library does not
+ * run it on the device (then teal would call teal_error). */
+int tg_convective_select(const char *name);
+int tg_viscous_select(const char *name);
+int tg_limiter_select(const char *name);
+int tg_boundary_select(const char *name, int physics);
+int tg_advance_select(const char *name);
+
+/* ---- mesh: teal's Mesh arrays (src/mesh.h:13-72), one process ---------------------------------- */
+typedef struct {
+    /* MeshCells */
+    int num_cells;          /* inner + boundary ghosts + periodic ghosts */
+    int num_inner_cells;
+    int off_boundary_cells; /* first periodic ghost */
+    int off_periodic_cells; /* first neighbour-rank ghost (== num_cells on one process) */
+    const int *cell_cell_off;      /* [num_cells + 1] CSR of face neighbours */
+    const int *cell_cell_idx;      /* [cell_cell_off[num_cells]] */
+    const double *cell_volume;     /* [num_cells] */
+    const double *cell_center;     /* [num_cells][3] */
+    const double *cell_projection; /* [num_cells][3] */
+    const double *cell_offset;     /* [cell_cell_off[num_inner_cells]][3] */
+    double sum_volume;
+    /* MeshFaces */
+    int num_faces; /* inner (two-sided) + boundary + periodic (one-sided copies) */
+    int num_inner_faces;
+    int off_boundary_faces;
+    const int *face_cell;          /* [num_faces][2] left, right */
+    const double *face_area;       /* [num_faces] */
+    const double *face_basis;      /* [num_faces][3][3] rows: normal, tangent, tangent */
+    const double *face_weight;     /* [num_faces][2][3] LS weights of the left / right cell */
+    const double *face_offset;     /* [num_faces][2][3] face centre minus left / right centre */
+    const double *face_correction; /* [num_faces][4] unit vector left->right centre, distance */
+    /* MeshEntities */
+    int num_entities;
+    int num_inner_entities;
+    int off_boundary_entities;
+    const int *entity_face_off; /* [num_entities + 1] */
+    /* MeshNeighbors (periodic self-exchange on one process) */
+    int num_neighbors;
+    const int *neighbor_tag;      /* [num_neighbors][2] receive tag, send tag */
+    const int *neighbor_recv_off; /* [num_neighbors + 1] ghost cell ranges */
+    const int *neighbor_send_off; /* [num_neighbors + 1] */
+    const int *neighbor_send_idx; /* [neighbor_send_off[num_neighbors]] inner cells sent */
+} tg_mesh;
+
+/* ---- equations: the Equations plugin table, by kind (src/equations.h:97-111) -------------------- */
+typedef struct {
+    int physics;     /* TG_EULER / TG_NAVIERSTOKES */
+    int space_order; /* 1 or 2 */
+    int convective;  /* TG_FLUX_* */
+    int viscous;     /* TG_VISCOUS_* (Navier–Stokes only) */
+    int limiter;     /* TG_LIMITER_* */
+    /* Venkatakrishnan eps^2 per inner cell (teal's limiter.parameter); null = computed from
+     * limiter_coefficient as teal does (src/equations/limiter.c:8-21) */
+    const double *limiter_parameter;
+    double limiter_coefficient;
+    double property[3]; /* heat capacity ratio, dynamic viscosity, Prandtl number */
+    int num_boundaries; /* off_boundary_entities - num_inner_entities */
+    const int *boundary_kind;       /* [num_boundaries] TG_BC_* */
+    const double *boundary_context; /* [num_boundaries][5] primitive state (may be null) */
+} tg_equations;
+
+/* contexts of the Advance methods, teal's layouts (src/simulation.h:25-34) */
+typedef struct {
+    int time_order;
+    int num_stages;
+} tg_runge_kutta;
+
+typedef struct {
+    double newton_tolerance;
+    double krylov_tolerance;
+    int krylov_dimension;
+} tg_newton_krylov;
+
+/* ---- context lifecycle ------------------------------------------------------------------------- */
+typedef struct tg_ctx tg_ctx;
+
+/* Upload mesh + equations to the current CUDA device: structure-of-arrays geometry, periodic ghost
+ * -> owner redirection, per-cell face lists in face order. Host arrays may be freed afterwards. */
+int tg_create(const tg_mesh *mesh, const tg_equations *eqns, int precision, tg_ctx **ctx);
+int tg_destroy(tg_ctx *ctx);
+
+/* Thread-local message of the last failing call on this thread. */
+const char *tg_last_error(void);
+
+/* Run all device work of this context on `stream` (a cudaStream_t; null = the context's own). */
+int tg_set_stream(tg_ctx *ctx, void *stream);
+
+/* Resident primitive state: [num_cells][5] in teal's cell order (density, velocity, pressure).
+ * set: reads inner cells (ghost rows are ignored). get: writes inner cells, boundary ghosts as the
+ * last boundary pass left them, and periodic ghosts as copies of their owners. */
+int tg_set_primitive(tg_ctx *ctx, const double *primitive);
+int tg_get_primitive(tg_ctx *ctx, double *primitive);
+
+/* equations_derivative: boundary pass, gradient, limiter, viscous and convective fluxes, finalize.
+ * primitive: [num_cells][5] host array (inner rows are read; null = the resident state, whose
+ * boundary ghost rows are refreshed); a host-given state is evaluated in scratch memory and leaves
+ * the resident state unchanged. derivative: [num_inner][5]. */
+int tg_derivative(tg_ctx *ctx, const double *primitive, double *derivative, double time);
+
+/* equations_gradient (+ equations_limiter when `limited`) of the resident state after a boundary
+ * pass: gradient [num_inner][5][3]. */
+int tg_gradient(tg_ctx *ctx, double time, int limited, double *gradient);
+
+/* equations_timestep of the resident state (minimum stable step, before the Courant factor). */
+int tg_timestep(tg_ctx *ctx, double *step);
+
+/* equations_residual of a derivative [num_inner][5] given on the host -> residual[5]. */
+int tg_residual(tg_ctx *ctx, const double *derivative, double *residual);
+
+/* One Advance step on the resident state: method TG_ADVANCE_*, context tg_runge_kutta /
+ * tg_newton_krylov (null = teal's defaults). Returns the unclipped step in *step0 and advances
+ * *time by min(step0, max_step); residual[5] gets equations_residual of the last derivative. */
+int tg_advance(tg_ctx *ctx, int method, const void *context, double courant, double *time,
+               double max_step, double *residual, double *step0);
+
+/* simulation_run's loop with the state resident: up to max_iter steps or until max_time, or until
+ * the residual of `variable` (-1 = maximum) drops below `threshold` (threshold <= 0: never).
+ * Steps are replayed from CUDA graphs; the host synchronises only when it must test the residual.
+ * On return *time and *iter hold the end state, residual[5] the last residual. */
+int tg_run(tg_ctx *ctx, int method, const void *context, double courant, int max_iter,
+           double max_time, int variable, double threshold, double *time, int *iter,
+           double *residual);
+
+/* ---- drop-in Advance methods with teal's signature (src/simulation.h:6-7) ----------------------- */
+
+/* Bind a teal `Equations *` (used only as a lookup key) to a context and to the host primitive
+ * array teal reads (`eqns->primitive.data`, [num_cells][5]). The host state is uploaded now;
+ * after every drop-in Advance call the new state is copied back into that array. */
+int tg_bind(const void *eqns, tg_ctx *ctx, double *host_primitive);
+int tg_unbind(const void *eqns);
+
+/* On failure these print tg_last_error() to stderr and exit(EXIT_FAILURE), as teal_error does. */
+double tg_teal_euler(const void *eqns, double *time, void *residual, double max_step,
+                     double courant, const void *context);
+double tg_teal_lserk(const void *eqns, double *time, void *residual, double max_step,
+                     double courant, const void *context);
+double tg_teal_implicit_euler(const void *eqns, double *time, void *residual, double max_step,
+                              double courant, const void *context);
+
+/* ---- host mesh generation (the single-process Cartesian case of mesh_create + mesh_generate,
+ *      src/mesh/create.c:509-544, src/mesh/generate.c:779-815) ---------------------------------- */
+typedef struct tg_host_mesh tg_host_mesh;
+
+/* Build a Cartesian hex box [min, max] with num cells per axis and per-axis periodicity; node
+ * displacement (optional, [(nx+1)(ny+1)(nz+1)][3], node order x fastest) is added before the
+ * geometry is generated, as mesh_modify would. */
+int tg_host_mesh_cartesian(const double *min_coord, const double *max_coord, const int *num_cells,
+                           const int *periodic, const double *displacement, tg_host_mesh **mesh);
+/* View of the generated arrays (pointers stay owned by the host mesh). */
+int tg_host_mesh_view(const tg_host_mesh *mesh, tg_mesh *view);
+/* Entity names (teal's: "domain", "left", "right", ...) and their cell ranges. */
+int tg_host_mesh_entity(const tg_host_mesh *mesh, int index, const char **name, int *cell_beg,
+                        int *cell_end);
+int tg_host_mesh_destroy(tg_host_mesh *mesh);
+
+/* ---- measurement -------------------------------------------------------------------------------
+ * tg_profile: reset the per-kernel timers and enable (1) or disable (0) CUDA-event timing of every
+ * hot-path launch; while enabled, steps run as plain launches instead of graph replays.
+ * tg_profile_read: accumulated milliseconds and launch counts per category TG_PROF_*.
+ * tg_launch_count: kernels this context has launched on its hot path (graph replays included). */
+enum {
+    TG_PROF_BOUNDARY = 0,
+    TG_PROF_GRADIENT = 1,
+    TG_PROF_FACE = 2,
+    TG_PROF_CELL = 3,
+    TG_PROF_REDUCE = 4,
+    TG_PROF_CATEGORIES = 5
+};
+int tg_profile(tg_ctx *ctx, int enable);
+int tg_profile_read(tg_ctx *ctx, double *ms, long *launches);
+int tg_launch_count(tg_ctx *ctx, long *count);
+
+/* ---- device layout introspection (tests of the device upload) --------------------------------
+ * Copy a device layout array to `out` (count elements of the named array's type):
+ *   "face_lr"   int[num_faces][2]  left, right with periodic ghosts redirected to their owners
+ *   "slot_face" int[6][num_inner]  face f (cell is left) or ~f (cell is right), sorted by face
+ *   "slot_nbr"  int[6][num_inner]  neighbour state row of each slot (padding: the cell itself)
+ *   "slot_cnt"  uint8[num_inner]   faces per cell
+ *   "owner"     int[num periodic ghosts]  owner cell of each periodic ghost
+ * Returns TG_ERR_INVALID for an unknown name or a count that does not match. */
+int tg_layout(tg_ctx *ctx, const char *name, void *out, long count);
+
+/* ---- version / build info ---------------------------------------------------------------------- */
+const char *tg_build_info(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TEAL_B200_H */

@@ -1,0 +1,306 @@
+/*
+ * ctypes-callable harness around the reference solver compiled in place (oracle/_ref). Test
+ * infrastructure only: tests, fixtures and the CPU-baseline leg of bench.py call it to obtain the
+ * reference's own results. It only calls the reference's public API (src/*.h) and reads its
+ * structs; it computes nothing itself.
+ */
+#include <stdlib.h>
+#include <string.h>
+
+#include "equations.h"
+#include "euler.h"
+#include "mesh.h"
+#include "navierstokes.h"
+#include "simulation.h"
+#include "teal.h"
+
+int ref_init(void)
+{
+    static int done = 0;
+    if (!done) {
+        static char arg0[] = "teal_ref";
+        static char arg1[] = "-q";
+        static char *argv_store[] = {arg0, arg1, 0};
+        int argc = 2;
+        char **argv = argv_store;
+        teal_init(&argc, &argv);
+        done = 1;
+    }
+    return 0;
+}
+
+void ref_set_quiet(int quiet)
+{
+    teal.quiet = quiet;
+}
+
+/* ---- mesh ----------------------------------------------------------------------------------- */
+
+static void (*modify_fn)(Vector *) = 0;
+static double jitter_amp = 0;
+
+void *ref_mesh_cartesian(const double *min, const double *max, const int *num, const int *periodic)
+{
+    Vector lo = {min[0], min[1], min[2]};
+    Vector hi = {max[0], max[1], max[2]};
+    Triple n = {num[0], num[1], num[2]};
+    Triple p = {periodic[0], periodic[1], periodic[2]};
+    Mesh *mesh = mesh_create(lo, hi, n, p);
+    return mesh;
+}
+
+/* apply a node displacement table (in node order at the time of the call) before generation */
+static const double *displacement = 0;
+static int displacement_num = 0;
+static int displacement_cur = 0;
+static void displace(Vector *coord)
+{
+    if (displacement_cur < displacement_num) {
+        coord->x += displacement[(3 * displacement_cur) + 0];
+        coord->y += displacement[(3 * displacement_cur) + 1];
+        coord->z += displacement[(3 * displacement_cur) + 2];
+    }
+    displacement_cur += 1;
+}
+
+void ref_mesh_displace(void *mesh, const double *disp, int num)
+{
+    displacement = disp;
+    displacement_num = num;
+    displacement_cur = 0;
+    mesh_modify(mesh, displace);
+    displacement = 0;
+    (void)modify_fn;
+    (void)jitter_amp;
+}
+
+void ref_mesh_split(void *mesh, const char *entity, const double *root, const double *normal)
+{
+    mesh_split(mesh, entity, (Vector){root[0], root[1], root[2]},
+               (Vector){normal[0], normal[1], normal[2]});
+}
+
+void ref_mesh_generate(void *mesh)
+{
+    mesh_generate(mesh);
+}
+
+void ref_mesh_validate(void *mesh)
+{
+    mesh_validate(mesh);
+}
+
+void ref_mesh_destroy(void *mesh)
+{
+    mesh_destroy(mesh);
+}
+
+/* counts[0..15]: nodes.num, nodes.num_inner, cells.num, cells.num_inner, cells.off_boundary,
+ * cells.off_periodic, faces.num, faces.num_inner, faces.off_boundary, cells.cell nnz,
+ * entities.num, entities.num_inner, entities.off_boundary, neighbors.num, neighbors.send nnz,
+ * cells.node nnz */
+void ref_mesh_counts(const void *mesh_, long *counts)
+{
+    const Mesh *mesh = mesh_;
+    counts[0] = mesh->nodes.num;
+    counts[1] = mesh->nodes.num_inner;
+    counts[2] = mesh->cells.num;
+    counts[3] = mesh->cells.num_inner;
+    counts[4] = mesh->cells.off_boundary;
+    counts[5] = mesh->cells.off_periodic;
+    counts[6] = mesh->faces.num;
+    counts[7] = mesh->faces.num_inner;
+    counts[8] = mesh->faces.off_boundary;
+    counts[9] = mesh->cells.cell.off[mesh->cells.num];
+    counts[10] = mesh->entities.num;
+    counts[11] = mesh->entities.num_inner;
+    counts[12] = mesh->entities.off_boundary;
+    counts[13] = mesh->neighbors.num;
+    counts[14] = mesh->neighbors.send.off[mesh->neighbors.num];
+    counts[15] = mesh->cells.node.off[mesh->cells.num];
+}
+
+double ref_mesh_sum_volume(const void *mesh_)
+{
+    return ((const Mesh *)mesh_)->cells.sum_volume;
+}
+
+const void *ref_mesh_array(const void *mesh_, const char *name)
+{
+    const Mesh *mesh = mesh_;
+    if (!strcmp(name, "nodes.coord")) return mesh->nodes.coord;
+    if (!strcmp(name, "cells.node.off")) return mesh->cells.node.off;
+    if (!strcmp(name, "cells.node.idx")) return mesh->cells.node.idx;
+    if (!strcmp(name, "cells.cell.off")) return mesh->cells.cell.off;
+    if (!strcmp(name, "cells.cell.idx")) return mesh->cells.cell.idx;
+    if (!strcmp(name, "cells.volume")) return mesh->cells.volume;
+    if (!strcmp(name, "cells.center")) return mesh->cells.center;
+    if (!strcmp(name, "cells.projection")) return mesh->cells.projection;
+    if (!strcmp(name, "cells.offset")) return mesh->cells.offset;
+    if (!strcmp(name, "faces.cell_idx")) return mesh->faces.cell_idx;
+    if (!strcmp(name, "faces.area")) return mesh->faces.area;
+    if (!strcmp(name, "faces.center")) return mesh->faces.center;
+    if (!strcmp(name, "faces.basis")) return mesh->faces.basis;
+    if (!strcmp(name, "faces.weight")) return mesh->faces.weight;
+    if (!strcmp(name, "faces.offset")) return mesh->faces.offset;
+    if (!strcmp(name, "faces.correction")) return mesh->faces.correction;
+    if (!strcmp(name, "entities.cell_off")) return mesh->entities.cell_off;
+    if (!strcmp(name, "entities.face_off")) return mesh->entities.face_off;
+    if (!strcmp(name, "neighbors.tag")) return mesh->neighbors.tag;
+    if (!strcmp(name, "neighbors.rank")) return mesh->neighbors.rank;
+    if (!strcmp(name, "neighbors.recv_off")) return mesh->neighbors.recv_off;
+    if (!strcmp(name, "neighbors.send.off")) return mesh->neighbors.send.off;
+    if (!strcmp(name, "neighbors.send.idx")) return mesh->neighbors.send.idx;
+    return 0;
+}
+
+const char *ref_mesh_entity_name(const void *mesh_, int idx)
+{
+    const Mesh *mesh = mesh_;
+    if (idx < 0 || idx >= mesh->entities.num) {
+        return 0;
+    }
+    return mesh->entities.name[idx];
+}
+
+/* ---- equations ------------------------------------------------------------------------------ */
+
+void *ref_equations(void *mesh, int navierstokes)
+{
+    return navierstokes ? navierstokes_create(mesh) : euler_create(mesh);
+}
+
+void ref_set_space_order(void *eqns, int order)
+{
+    equations_set_space_order(eqns, order);
+}
+
+void ref_set_convective(void *eqns, const char *name)
+{
+    equations_set_convective_flux(eqns, (name && name[0]) ? name : 0);
+}
+
+void ref_set_viscous(void *eqns, const char *name)
+{
+    equations_set_viscous_flux(eqns, (name && name[0]) ? name : 0);
+}
+
+void ref_set_limiter(void *eqns, const char *name, double coefficient)
+{
+    equations_set_limiter(eqns, (name && name[0]) ? name : 0, coefficient);
+}
+
+void ref_set_property(void *eqns, const char *name, double value)
+{
+    equations_set_property(eqns, name, value);
+}
+
+void ref_set_boundary(void *eqns, const char *entity, const char *name, const double *context)
+{
+    double *copy_ = 0;
+    if (context) {
+        copy_ = malloc(5 * sizeof(double)); /* lives as long as the process: BCs keep the pointer */
+        memcpy(copy_, context, 5 * sizeof(double));
+    }
+    equations_set_boundary_condition(eqns, entity, name, 0, copy_);
+}
+
+double *ref_primitive(void *eqns)
+{
+    return ((Equations *)eqns)->primitive.data;
+}
+
+const double *ref_limiter_parameter(void *eqns)
+{
+    return ((Equations *)eqns)->limiter.parameter;
+}
+
+void ref_derivative(void *eqns, double *primitive, double *derivative, double time)
+{
+    equations_derivative(eqns, primitive, derivative, time);
+}
+
+void ref_boundary(void *eqns, double *primitive, double time)
+{
+    equations_boundary(eqns, primitive, time);
+}
+
+void ref_gradient(void *eqns, double *primitive, double *gradient)
+{
+    equations_gradient(eqns, primitive, gradient);
+}
+
+void ref_limiter(void *eqns, const double *primitive, double *gradient)
+{
+    equations_limiter(eqns, primitive, gradient);
+}
+
+double ref_timestep(void *eqns, const double *primitive)
+{
+    return equations_timestep(eqns, primitive);
+}
+
+void ref_residual(void *eqns, const double *derivative, double *residual)
+{
+    equations_residual(eqns, derivative, residual);
+}
+
+void ref_equations_destroy(void *eqns)
+{
+    equations_destroy(eqns);
+}
+
+/* ---- simulation ----------------------------------------------------------------------------- */
+
+/* method: "euler", "lserk" or "implicit euler"; iparam/dparam: RungeKutta{time_order, num_stages}
+ * or NewtonKrylov{newton_tolerance, krylov_tolerance, krylov_dimension} (null = defaults) */
+void *ref_simulation(void *eqns, const char *method, double courant, const int *iparam,
+                     const double *dparam)
+{
+    Simulation *sim = simulation_create(eqns, "");
+    if (!strcmp(method, "lserk") && iparam) {
+        RungeKutta rk = {iparam[0], iparam[1]};
+        simulation_set_advance(sim, method, courant, &rk);
+    }
+    else if (!strcmp(method, "implicit euler") && dparam) {
+        NewtonKrylov nk = {dparam[0], dparam[1], (int)dparam[2]};
+        simulation_set_advance(sim, method, courant, &nk);
+    }
+    else {
+        simulation_set_advance(sim, method, courant, 0);
+    }
+    return sim;
+}
+
+void ref_simulation_set_max_iter(void *sim, int iter)
+{
+    simulation_set_max_iter(sim, iter);
+}
+
+void ref_simulation_set_max_time(void *sim, double time)
+{
+    simulation_set_max_time(sim, time);
+}
+
+void ref_simulation_set_termination(void *sim, const char *condition, double threshold)
+{
+    simulation_set_termination(sim, condition, threshold);
+}
+
+double ref_simulation_run(void *sim)
+{
+    return simulation_run(sim);
+}
+
+/* one call of the configured Advance method, as simulation_run makes it (run.c:69-70) */
+double ref_advance(void *sim_, double *time, double *residual, double max_step)
+{
+    Simulation *sim = sim_;
+    return sim->advance.method(sim->eqns, time, residual, max_step, sim->advance.courant,
+                               sim->advance.context);
+}
+
+void ref_simulation_destroy(void *sim)
+{
+    simulation_destroy(sim);
+}

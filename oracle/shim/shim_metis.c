@@ -1,0 +1,106 @@
+/*
+ * Restatement of METIS 5's dual-graph rule for `METIS_MeshToDual` (METIS 5.1.0, libmetis/mesh.c,
+ * CreateGraphDual / FindCommonElements; the dependency is absent from the reference tree, which
+ * only calls it at mesh/generate.c:35-43). Test infrastructure only.
+ *
+ * Two elements i and j are joined when the number of nodes they share, `overlap`, satisfies
+ *     overlap >= ncommon || overlap >= len(i) - 1 || overlap >= len(j) - 1.
+ * For element i the neighbours are listed in order of first encounter while scanning i's nodes in
+ * order and, for each node, the elements that hold it in increasing element number.
+ */
+#include <stdlib.h>
+
+#include "metis.h"
+
+int METIS_MeshToDual(idx_t *ne_, idx_t *nn_, idx_t *eptr, idx_t *eind, idx_t *ncommon_,
+                     idx_t *numflag, idx_t **xadj_out, idx_t **adjncy_out)
+{
+    idx_t ne = *ne_, nn = *nn_, ncommon = *ncommon_;
+    if (*numflag != 0 || ne < 0 || nn < 0) {
+        return METIS_ERROR;
+    }
+
+    /* node -> element lists, elements ascending */
+    idx_t *nptr = calloc((size_t)nn + 1, sizeof(idx_t));
+    for (idx_t e = 0; e < ne; e++) {
+        for (idx_t k = eptr[e]; k < eptr[e + 1]; k++) {
+            nptr[eind[k] + 1] += 1;
+        }
+    }
+    for (idx_t n = 0; n < nn; n++) {
+        nptr[n + 1] += nptr[n];
+    }
+    idx_t *nind = malloc(((size_t)nptr[nn] + 1) * sizeof(idx_t));
+    idx_t *cur = malloc(((size_t)nn + 1) * sizeof(idx_t));
+    for (idx_t n = 0; n < nn; n++) {
+        cur[n] = nptr[n];
+    }
+    for (idx_t e = 0; e < ne; e++) {
+        for (idx_t k = eptr[e]; k < eptr[e + 1]; k++) {
+            nind[cur[eind[k]]++] = e;
+        }
+    }
+
+    idx_t *marker = calloc((size_t)ne + 1, sizeof(idx_t));
+    idx_t *nbrs = malloc(((size_t)ne + 1) * sizeof(idx_t));
+
+    /* two passes: count, then fill */
+    idx_t *xadj = calloc((size_t)ne + 1, sizeof(idx_t));
+    idx_t *adjncy = 0;
+    for (int pass = 0; pass < 2; pass++) {
+        for (idx_t e = 0; e < ne; e++) {
+            idx_t len_e = eptr[e + 1] - eptr[e];
+            idx_t nnbrs = 0;
+            for (idx_t k = eptr[e]; k < eptr[e + 1]; k++) {
+                idx_t node = eind[k];
+                for (idx_t m = nptr[node]; m < nptr[node + 1]; m++) {
+                    idx_t other = nind[m];
+                    if (other == e) {
+                        continue;
+                    }
+                    if (marker[other] == 0) {
+                        nbrs[nnbrs++] = other;
+                    }
+                    marker[other] += 1;
+                }
+            }
+            idx_t kept = 0;
+            for (idx_t m = 0; m < nnbrs; m++) {
+                idx_t other = nbrs[m];
+                idx_t overlap = marker[other];
+                idx_t len_o = eptr[other + 1] - eptr[other];
+                if (overlap >= ncommon || overlap >= len_e - 1 || overlap >= len_o - 1) {
+                    if (pass == 1) {
+                        adjncy[xadj[e] + kept] = other;
+                    }
+                    kept += 1;
+                }
+                marker[other] = 0;
+            }
+            if (pass == 0) {
+                xadj[e + 1] = kept;
+            }
+        }
+        if (pass == 0) {
+            for (idx_t e = 0; e < ne; e++) {
+                xadj[e + 1] += xadj[e];
+            }
+            adjncy = malloc(((size_t)xadj[ne] + 1) * sizeof(idx_t));
+        }
+    }
+
+    free(nptr);
+    free(nind);
+    free(cur);
+    free(marker);
+    free(nbrs);
+    *xadj_out = xadj;
+    *adjncy_out = adjncy;
+    return METIS_OK;
+}
+
+int METIS_Free(void *ptr)
+{
+    free(ptr);
+    return METIS_OK;
+}

@@ -1,0 +1,122 @@
+// Device helpers shared by all kernels: state / geometry loads, teal's is_close, and fixed-shape
+// (deterministic) block reductions.
+#pragma once
+
+#include <cfloat>
+
+#include "device.cuh"
+
+namespace tg {
+
+constexpr int BLOCK = 256;
+constexpr int REDUCE_BLOCK = 1024;
+
+// ---- small helpers ---------------------------------------------------------------------------
+
+template <typename R>
+__device__ __forceinline__ Prim<R> load_prim(const double *__restrict__ q, int ld, int i)
+{
+    Prim<R> p;
+    p.rho = R(__ldg(q + i));
+    p.u.x = R(__ldg(q + ld + i));
+    p.u.y = R(__ldg(q + 2 * ld + i));
+    p.u.z = R(__ldg(q + 3 * ld + i));
+    p.p = R(__ldg(q + 4 * ld + i));
+    return p;
+}
+
+__device__ __forceinline__ void store_prim(double *__restrict__ q, int ld, int i, const Prim<double> &p)
+{
+    q[i] = p.rho;
+    q[ld + i] = p.u.x;
+    q[2 * ld + i] = p.u.y;
+    q[3 * ld + i] = p.u.z;
+    q[4 * ld + i] = p.p;
+}
+
+template <typename R>
+__device__ __forceinline__ Basis<R> load_basis(const R *__restrict__ b, int ld, int f)
+{
+    Basis<R> m;
+    m.x = v3(__ldg(b + f), __ldg(b + ld + f), __ldg(b + 2 * ld + f));
+    m.y = v3(__ldg(b + 3 * ld + f), __ldg(b + 4 * ld + f), __ldg(b + 5 * ld + f));
+    m.z = v3(__ldg(b + 6 * ld + f), __ldg(b + 7 * ld + f), __ldg(b + 8 * ld + f));
+    return m;
+}
+
+template <typename R>
+__device__ __forceinline__ V3<R> load_v3(const R *__restrict__ a, int ld, int i)
+{
+    return v3(__ldg(a + i), __ldg(a + ld + i), __ldg(a + 2 * ld + i));
+}
+
+template <typename R>
+__device__ __forceinline__ R prim_get(const Prim<R> &p, int v)
+{
+    return v == 0 ? p.rho : v == 1 ? p.u.x : v == 2 ? p.u.y : v == 3 ? p.u.z : p.p;
+}
+
+template <typename R>
+__device__ __forceinline__ Prim<R> prim_from(const R *a)
+{
+    return Prim<R>{a[0], v3(a[1], a[2], a[3]), a[4]};
+}
+
+// is_close(x, 0) of src/core/utils.c:29-34 (absolute 1e-8, relative 1e-5)
+template <typename R>
+__device__ __forceinline__ bool is_close_zero(R x)
+{
+    return fabs(x) <= fmax(R(1e-8), R(1e-5) * fabs(x));
+}
+
+// ---- block reductions (fixed shape => deterministic) -----------------------------------------
+
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double *sh)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v += __shfl_down_sync(0xffffffffu, v, o);
+    }
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) {
+        sh[warp] = v;
+    }
+    __syncthreads();
+    double r = 0;
+    if (warp == 0) {
+        r = (lane < NT / 32) ? sh[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            r += __shfl_down_sync(0xffffffffu, r, o);
+        }
+    }
+    return r;  // valid in thread 0
+}
+
+template <int NT>
+__device__ __forceinline__ double block_min(double v, double *sh)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v = fmin(v, __shfl_down_sync(0xffffffffu, v, o));
+    }
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) {
+        sh[warp] = v;
+    }
+    __syncthreads();
+    double r = DBL_MAX;
+    if (warp == 0) {
+        r = (lane < NT / 32) ? sh[lane] : DBL_MAX;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            r = fmin(r, __shfl_down_sync(0xffffffffu, r, o));
+        }
+    }
+    return r;
+}
+
+}  // namespace tg

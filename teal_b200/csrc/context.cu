@@ -1,0 +1,1495 @@
+// Host side of teal_b200: device upload of teal's mesh / equations, kernel sequencing of
+// equations_derivative and of the Advance methods, CUDA-graph replay of steps, and the C ABI.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/teal_b200.h"
+#include "gmres.cuh"
+#include "kernels.cuh"
+#include "launch.cuh"
+
+using namespace tg;
+
+// ---- errors ----------------------------------------------------------------------------------
+
+static thread_local std::string g_error;
+
+static int fail(int code, const char *fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_error = buf;
+    return code;
+}
+
+#define CU(call)                                                                                 \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess) {                                                                 \
+            return fail(e_ == cudaErrorMemoryAllocation ? TG_ERR_OOM : TG_ERR_CUDA, "%s: %s (%s:%d)", \
+                        #call, cudaGetErrorString(e_), __FILE__, __LINE__);                      \
+        }                                                                                        \
+    } while (0)
+
+#define TRY(call)                                                                                \
+    do {                                                                                         \
+        int r_ = (call);                                                                         \
+        if (r_ != TG_OK) {                                                                       \
+            return r_;                                                                           \
+        }                                                                                        \
+    } while (0)
+
+extern "C" const char *tg_last_error(void)
+{
+    return g_error.c_str();
+}
+
+extern "C" const char *tg_build_info(void)
+{
+    return "teal_b200 sm_100a " __DATE__;
+}
+
+// ---- plugin selection by teal's names ---------------------------------------------------------
+
+extern "C" int tg_convective_select(const char *name)
+{
+    if (!name) return -1;
+    static const struct {
+        const char *n;
+        int k;
+    } t[] = {{"roe", TG_FLUX_ROE},     {"hll", TG_FLUX_HLL},       {"hllc", TG_FLUX_HLLC},
+             {"hlle", TG_FLUX_HLLE},   {"ausmd", TG_FLUX_AUSMD},   {"ausmdv", TG_FLUX_AUSMDV},
+             {"lxf", TG_FLUX_LXF},     {"central", TG_FLUX_CENTRAL}};
+    for (auto &e : t) {
+        if (!strcmp(name, e.n)) return e.k;
+    }
+    return -1;  // includes "godunov" (exact Riemann solver): not run on the device
+}
+
+extern "C" int tg_viscous_select(const char *name)
+{
+    if (name && !strcmp(name, "central")) return TG_VISCOUS_CENTRAL;
+    return -1;
+}
+
+extern "C" int tg_limiter_select(const char *name)
+{
+    if (!name) return -1;
+    if (!strcmp(name, "barth jespersen") || !strcmp(name, "minmod")) return TG_LIMITER_BARTH_JESPERSEN;
+    if (!strcmp(name, "venkatakrishnan")) return TG_LIMITER_VENKATAKRISHNAN;
+    return -1;
+}
+
+extern "C" int tg_boundary_select(const char *name, int physics)
+{
+    if (!name) return -1;
+    if (physics == TG_NAVIERSTOKES && (!strcmp(name, "adiabatic wall") || !strcmp(name, "wall")))
+        return TG_BC_ADIABATIC_WALL;
+    if (!strcmp(name, "symmetry") || !strcmp(name, "slipwall")) return TG_BC_SYMMETRY;
+    if (!strcmp(name, "supersonic inflow")) return TG_BC_SUPERSONIC_INFLOW;
+    if (!strcmp(name, "supersonic outflow")) return TG_BC_SUPERSONIC_OUTFLOW;
+    if (!strcmp(name, "subsonic inflow")) return TG_BC_SUBSONIC_INFLOW;
+    if (!strcmp(name, "subsonic outflow")) return TG_BC_SUBSONIC_OUTFLOW;
+    if (!strcmp(name, "pressure outflow")) return TG_BC_PRESSURE_OUTFLOW;
+    if (!strcmp(name, "farfield")) return TG_BC_FARFIELD;
+    return -1;
+}
+
+extern "C" int tg_advance_select(const char *name)
+{
+    if (!name) return -1;
+    if (!strcmp(name, "euler")) return TG_ADVANCE_EULER;
+    if (!strcmp(name, "lserk")) return TG_ADVANCE_LSERK;
+    if (!strcmp(name, "implicit euler")) return TG_ADVANCE_IMPLICIT_EULER;
+    return -1;
+}
+
+// ---- context ---------------------------------------------------------------------------------
+
+template <typename T>
+static int dalloc(T **p, size_t n)
+{
+    *p = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return fail(TG_ERR_OOM, "cudaMalloc of %zu bytes failed: %s", n * sizeof(T), cudaGetErrorString(e));
+    }
+    return TG_OK;
+}
+
+struct GeomBuf {
+    double *area = nullptr, *basis = nullptr, *offl = nullptr, *offr = nullptr, *corr = nullptr;
+    double *slot_w = nullptr, *slot_off = nullptr;
+    float *area32 = nullptr, *basis32 = nullptr, *offl32 = nullptr, *offr32 = nullptr, *corr32 = nullptr;
+    float *slot_w32 = nullptr, *slot_off32 = nullptr;
+};
+
+// workspace of the Jacobian-free Newton-GMRES implicit step
+struct Gmres {
+    int dim = 0;
+    double *U = nullptr;     // [5][C] Newton iterate (conserved)
+    double *Ustart = nullptr; // [5][C] conserved state at the start of the step
+    double *r = nullptr;     // [5][C] Newton residual
+    double *delta = nullptr; // [5][C] increment
+    double *V = nullptr;     // [dim + 1][5][C] Krylov basis
+    double *w = nullptr;     // [5][C]
+    double *q1 = nullptr;    // [5][N] perturbed primitive state
+    double *R1 = nullptr;    // [5][C] derivative of the perturbed state
+    double *part = nullptr;  // block partials
+    double *sc = nullptr;    // device scalars (see GmresScalars)
+};
+
+struct tg_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+
+    // sizes
+    Sizes s{};
+    int num_cells = 0;          // teal's cells.num
+    int off_boundary_cells = 0; // first periodic ghost
+    int num_periodic = 0;
+
+    // equations
+    int physics = 0, order = 2, flux = 0, viscous = 0, limiter = 0, precision = 0;
+    double prop[3] = {1.4, 0, 0.71};
+    double sum_volume = 0;
+    BoundaryTable bt{};
+
+    // device mesh
+    int2 *lr = nullptr;
+    int *slot_nbr = nullptr, *slot_face = nullptr;
+    uint8_t *slot_cnt = nullptr;
+    int *owner = nullptr;      // periodic ghost -> owner cell
+    int *bface_ent = nullptr;  // boundary face -> boundary index
+    double *volume = nullptr, *proj = nullptr, *eps2 = nullptr;
+    GeomBuf gb;
+    Geometry<double> g64{};
+    Geometry<float> g32{};
+
+    // state
+    double *q = nullptr, *U0 = nullptr, *R = nullptr;
+    double *qs = nullptr;  // scratch state for derivatives of host-given states (allocated on use)
+    void *grad = nullptr, *psi = nullptr, *G = nullptr;
+    double *part_dt = nullptr, *part_res = nullptr;
+    int nblk = 0;
+    StepState *st = nullptr;      // device
+    StepState *st_host = nullptr; // pinned mirror
+    double *aos = nullptr;        // device scratch for teal-layout transfers
+    size_t aos_len = 0;
+    double *pinned = nullptr;     // pinned host staging buffer
+    size_t pinned_len = 0;
+    bool prepared = false;        // U0 and part_dt valid for the resident state
+
+    // implicit solver workspace (allocated on first use)
+    Gmres gm{};
+
+    // kernel launch count and optional per-kernel event timing
+    long launches = 0;
+    long graph_kernels = 0;
+    bool prof_on = false;
+    std::vector<cudaEvent_t> prof_pool;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof_open;
+    double prof_ms[TG_PROF_CATEGORIES] = {0};
+    long prof_n[TG_PROF_CATEGORIES] = {0};
+
+    // step graph cache
+    cudaGraphExec_t graph = nullptr;
+    int graph_method = -1, graph_stages = 0, graph_order = 0;
+    double graph_courant = 0;
+    int graph_use_max_time = -1;
+};
+
+static const double LSERK_ALPHA[3][6][7] = {
+    // tabulated low-storage RK coefficients, teal's table (src/simulation/advance.c:50-75)
+    {
+        {0.0000, 1.0000, 0.0000, 0.0000, 0.0000, 0.0000, 0.0000},
+        {0.0000, 0.3333, 1.0000, 0.0000, 0.0000, 0.0000, 0.0000},
+        {0.0000, 0.1481, 0.4000, 1.0000, 0.0000, 0.0000, 0.0000},
+        {0.0000, 0.0833, 0.2069, 0.4265, 1.0000, 0.0000, 0.0000},
+        {0.0000, 0.0533, 0.1263, 0.2375, 0.4414, 1.0000, 0.0000},
+        {0.0000, 0.0370, 0.0851, 0.1521, 0.2562, 0.4512, 1.0000},
+    },
+    {
+        {0.0000, 1.0000, 0.0000, 0.0000, 0.0000, 0.0000, 0.0000},
+        {0.0000, 0.4242, 1.0000, 0.0000, 0.0000, 0.0000, 0.0000},
+        {0.0000, 0.1918, 0.4929, 1.0000, 0.0000, 0.0000, 0.0000},
+        {0.0000, 0.1084, 0.2602, 0.5052, 1.0000, 0.0000, 0.0000},
+        {0.0000, 0.0695, 0.1602, 0.2898, 0.5060, 1.0000, 0.0000},
+        {0.0000, 0.0482, 0.1085, 0.1885, 0.3050, 0.5063, 1.0000},
+    },
+    {
+        {0.0000, 1.0000, 0.0000, 0.0000, 0.0000, 0.0000, 0.0000},
+        {0.0000, 0.6612, 1.0000, 0.0000, 0.0000, 0.0000, 0.0000},
+        {0.0000, 0.2884, 0.5010, 1.0000, 0.0000, 0.0000, 0.0000},
+        {0.0000, 0.1666, 0.3027, 0.5275, 1.0000, 0.0000, 0.0000},
+        {0.0000, 0.1067, 0.1979, 0.3232, 0.5201, 1.0000, 0.0000},
+        {0.0000, 0.0742, 0.1393, 0.2198, 0.3302, 0.5181, 1.0000},
+    },
+};
+
+static void free_ctx(tg_ctx *c)
+{
+    if (!c) return;
+    for (auto &e : c->prof_pool) cudaEventDestroy(e);
+    for (auto &p : c->prof_open) {
+        cudaEventDestroy(p.second.first);
+        cudaEventDestroy(p.second.second);
+    }
+    if (c->graph) cudaGraphExecDestroy(c->graph);
+    void *ptrs[] = {c->lr, c->slot_nbr, c->slot_face, c->slot_cnt, c->owner, c->bface_ent, c->volume,
+                    c->proj, c->eps2, c->gb.area, c->gb.basis, c->gb.offl, c->gb.offr, c->gb.corr,
+                    c->gb.slot_w, c->gb.slot_off, c->gb.area32, c->gb.basis32, c->gb.offl32,
+                    c->gb.offr32, c->gb.corr32, c->gb.slot_w32, c->gb.slot_off32, c->q, c->U0, c->R, c->qs,
+                    c->grad, c->psi, c->G, c->part_dt, c->part_res, c->st, c->aos};
+    for (void *p : ptrs) {
+        if (p) cudaFree(p);
+    }
+    void *gp[] = {c->gm.U, c->gm.Ustart, c->gm.r, c->gm.delta, c->gm.V, c->gm.w, c->gm.q1, c->gm.R1,
+                  c->gm.part, c->gm.sc};
+    for (void *p : gp) {
+        if (p) cudaFree(p);
+    }
+    if (c->st_host) cudaFreeHost(c->st_host);
+    if (c->pinned) cudaFreeHost(c->pinned);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+}
+
+static int grid_of(long n)
+{
+    return (int)((n + BLOCK - 1) / BLOCK);
+}
+
+// per-kernel event timing of the hot-path launches (categories TG_PROF_*)
+static cudaEvent_t prof_event(tg_ctx *c)
+{
+    if (!c->prof_pool.empty()) {
+        cudaEvent_t e = c->prof_pool.back();
+        c->prof_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+struct Launch {
+    tg_ctx *c;
+    int cat;
+    cudaEvent_t a = nullptr, b = nullptr;
+    Launch(tg_ctx *c_, int cat_) : c(c_), cat(cat_)
+    {
+        c->launches += 1;
+        if (c->prof_on) {
+            a = prof_event(c);
+            b = prof_event(c);
+            cudaEventRecord(a, c->stream);
+        }
+    }
+    ~Launch()
+    {
+        if (c->prof_on) {
+            cudaEventRecord(b, c->stream);
+            c->prof_open.push_back({cat, {a, b}});
+        }
+    }
+};
+
+// periodic ghost -> owner cell, by matching each receive tag with the send posted under it
+// (the single-process halo exchange of src/equations/exchange.c:8-36 and src/mesh/create.c:351-440)
+static int build_owner_map(const tg_mesh *m, std::vector<int> &owner)
+{
+    int off = m->off_boundary_cells;
+    int num = m->num_cells - off;
+    owner.assign(num, -1);
+    std::vector<char> used(m->num_neighbors, 0);
+    for (int k = 0; k < m->num_neighbors; k++) {
+        int tag = m->neighbor_tag[2 * k + 0];
+        int match = -1;
+        for (int j = 0; j < m->num_neighbors; j++) {
+            if (!used[j] && m->neighbor_tag[2 * j + 1] == tag) {
+                match = j;
+                break;
+            }
+        }
+        if (match < 0) {
+            return fail(TG_ERR_INVALID, "periodic receive with tag %d has no matching send", tag);
+        }
+        used[match] = 1;
+        int nrecv = m->neighbor_recv_off[k + 1] - m->neighbor_recv_off[k];
+        int nsend = m->neighbor_send_off[match + 1] - m->neighbor_send_off[match];
+        if (nrecv != nsend) {
+            return fail(TG_ERR_INVALID, "periodic exchange size mismatch (%d vs %d)", nrecv, nsend);
+        }
+        for (int i = 0; i < nrecv; i++) {
+            int ghost = m->neighbor_recv_off[k] + i - off;
+            int src = m->neighbor_send_idx[m->neighbor_send_off[match] + i];
+            if (ghost < 0 || ghost >= num || src < 0 || src >= m->num_inner_cells) {
+                return fail(TG_ERR_INVALID, "periodic exchange index out of range");
+            }
+            owner[ghost] = src;
+        }
+    }
+    for (int i = 0; i < num; i++) {
+        if (owner[i] < 0) {
+            return fail(TG_ERR_INVALID, "ghost cell %d receives no state", off + i);
+        }
+    }
+    return TG_OK;
+}
+
+template <typename T>
+static int upload(T **dst, const T *src, size_t n, cudaStream_t st)
+{
+    TRY(dalloc(dst, n));
+    if (n) CU(cudaMemcpyAsync(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice, st));
+    return TG_OK;
+}
+
+static int validate(const tg_mesh *m, const tg_equations *e)
+{
+    if (!m || !e) return fail(TG_ERR_INVALID, "null mesh or equations");
+    if (m->num_inner_cells <= 0 || m->num_cells < m->num_inner_cells ||
+        m->off_boundary_cells < m->num_inner_cells || m->off_boundary_cells > m->num_cells)
+        return fail(TG_ERR_INVALID, "invalid cell counts");
+    if (m->off_periodic_cells != m->num_cells)
+        return fail(TG_ERR_INVALID, "neighbour-rank ghost cells are not supported (one process)");
+    if (m->num_faces <= 0 || m->num_inner_faces < 0 || m->num_inner_faces > m->off_boundary_faces ||
+        m->off_boundary_faces > m->num_faces)
+        return fail(TG_ERR_INVALID, "invalid face counts");
+    if (!m->face_cell || !m->face_area || !m->face_basis || !m->face_weight || !m->face_offset ||
+        !m->cell_volume || !m->cell_projection)
+        return fail(TG_ERR_INVALID, "missing mesh array");
+    if (e->physics != TG_EULER && e->physics != TG_NAVIERSTOKES)
+        return fail(TG_ERR_INVALID, "invalid physics %d", e->physics);
+    if (e->space_order != 1 && e->space_order != 2)
+        return fail(TG_ERR_INVALID, "invalid space order (%d)", e->space_order);
+    if (e->convective < TG_FLUX_NONE || e->convective > TG_FLUX_CENTRAL)
+        return fail(TG_ERR_INVALID, "invalid convective flux kind %d", e->convective);
+    if (e->viscous != TG_VISCOUS_NONE && e->viscous != TG_VISCOUS_CENTRAL)
+        return fail(TG_ERR_INVALID, "invalid viscous flux kind %d", e->viscous);
+    if (e->viscous == TG_VISCOUS_CENTRAL && e->physics != TG_NAVIERSTOKES)
+        return fail(TG_ERR_INVALID, "viscous flux needs the Navier-Stokes equations");
+    if (e->viscous == TG_VISCOUS_CENTRAL && !m->face_correction)
+        return fail(TG_ERR_INVALID, "viscous flux needs face corrections");
+    if (e->limiter < TG_LIMITER_NONE || e->limiter > TG_LIMITER_VENKATAKRISHNAN)
+        return fail(TG_ERR_INVALID, "invalid limiter kind (%d)", e->limiter);
+    int nb = m->off_boundary_entities - m->num_inner_entities;
+    if (nb != e->num_boundaries)
+        return fail(TG_ERR_INVALID, "boundary count %d does not match the mesh (%d)", e->num_boundaries, nb);
+    if (nb > MAX_BOUNDARIES) return fail(TG_ERR_INVALID, "more than %d boundaries", MAX_BOUNDARIES);
+    for (int i = 0; i < nb; i++) {
+        int k = e->boundary_kind ? e->boundary_kind[i] : 0;
+        if (k < TG_BC_SYMMETRY || k > TG_BC_ADIABATIC_WALL)
+            return fail(TG_ERR_INVALID, "boundary %d has no device boundary condition", i);
+        if (k == TG_BC_ADIABATIC_WALL && e->physics != TG_NAVIERSTOKES)
+            return fail(TG_ERR_INVALID, "adiabatic wall needs the Navier-Stokes equations");
+    }
+    return TG_OK;
+}
+
+static int alloc_geom32(tg_ctx *c)
+{
+    const Sizes &s = c->s;
+    TRY(dalloc(&c->gb.area32, s.F));
+    TRY(dalloc(&c->gb.basis32, 9 * (size_t)s.F));
+    TRY(dalloc(&c->gb.offl32, 3 * (size_t)s.F));
+    TRY(dalloc(&c->gb.offr32, 3 * (size_t)s.F));
+    if (c->gb.corr) TRY(dalloc(&c->gb.corr32, 4 * (size_t)s.F));
+    TRY(dalloc(&c->gb.slot_w32, 3 * MAX_SLOTS * (size_t)s.C));
+    TRY(dalloc(&c->gb.slot_off32, 3 * MAX_SLOTS * (size_t)s.C));
+    return TG_OK;
+}
+
+__global__ static void k_to_float(size_t n, const double *__restrict__ a, float *__restrict__ b)
+{
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i < n) b[i] = float(a[i]);
+}
+
+static int to_float(const double *a, float *b, size_t n, cudaStream_t st)
+{
+    if (!a || !b || n == 0) return TG_OK;
+    k_to_float<<<(unsigned)((n + BLOCK - 1) / BLOCK), BLOCK, 0, st>>>(n, a, b);
+    CU(cudaGetLastError());
+    return TG_OK;
+}
+
+extern "C" int tg_create(const tg_mesh *m, const tg_equations *e, int precision, tg_ctx **out)
+{
+    if (!out) return fail(TG_ERR_INVALID, "null output pointer");
+    *out = nullptr;
+    TRY(validate(m, e));
+    if (precision != TG_PRECISION_FP64 && precision != TG_PRECISION_FP32_FLUX)
+        return fail(TG_ERR_INVALID, "invalid precision %d", precision);
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(TG_ERR_NO_DEVICE, "no CUDA device available");
+
+    std::vector<int> owner;
+    TRY(build_owner_map(m, owner));
+
+    tg_ctx *c = new tg_ctx();
+    int rc = [&]() -> int {
+        CU(cudaGetDevice(&c->device));
+        CU(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+        c->stream = c->own_stream;
+        cudaStream_t st = c->stream;
+
+        Sizes &s = c->s;
+        s.C = m->num_inner_cells;
+        s.N = m->off_boundary_cells;
+        s.F = m->num_faces;
+        s.F_in = m->num_inner_faces;
+        s.F_bd = m->off_boundary_faces;
+        c->num_cells = m->num_cells;
+        c->off_boundary_cells = m->off_boundary_cells;
+        c->num_periodic = m->num_cells - m->off_boundary_cells;
+        c->physics = e->physics;
+        c->order = e->space_order;
+        c->flux = e->convective;
+        c->viscous = e->viscous;
+        c->limiter = e->limiter;
+        c->precision = precision;
+        for (int i = 0; i < 3; i++) c->prop[i] = e->property[i];
+        c->sum_volume = m->sum_volume;
+
+        // boundary table and boundary face -> boundary index
+        c->bt.num = e->num_boundaries;
+        std::vector<int> bent(s.F_bd - s.F_in, -1);
+        for (int i = 0; i < e->num_boundaries; i++) {
+            c->bt.kind[i] = e->boundary_kind[i];
+            for (int v = 0; v < 5; v++) c->bt.ctx[i][v] = e->boundary_context ? e->boundary_context[5 * i + v] : 0.0;
+            int ent = m->num_inner_entities + i;
+            int beg = m->entity_face_off[ent], end = m->entity_face_off[ent + 1];
+            if (beg < s.F_in || end > s.F_bd || beg > end)
+                return fail(TG_ERR_INVALID, "boundary entity %d face range [%d, %d) invalid", i, beg, end);
+            for (int f = beg; f < end; f++) bent[f - s.F_in] = i;
+        }
+        for (size_t i = 0; i < bent.size(); i++) {
+            if (bent[i] < 0) return fail(TG_ERR_INVALID, "boundary face %zu belongs to no boundary", i + s.F_in);
+            int r = m->face_cell[2 * (s.F_in + i) + 1];
+            if (r < s.C || r >= s.N) return fail(TG_ERR_INVALID, "boundary face right cell out of range");
+        }
+
+        // raw teal arrays -> device temporaries
+        int *d_face_cell = nullptr, *d_owner_tmp = nullptr, *d_err = nullptr, *d_cnt = nullptr;
+        double *d_weight = nullptr, *d_offset = nullptr, *d_tmp = nullptr;
+        auto cleanup = [&]() {
+            cudaFree(d_face_cell);
+            cudaFree(d_owner_tmp);
+            cudaFree(d_err);
+            cudaFree(d_cnt);
+            cudaFree(d_weight);
+            cudaFree(d_offset);
+            cudaFree(d_tmp);
+        };
+        int r2 = [&]() -> int {
+            TRY(upload(&d_face_cell, m->face_cell, 2 * (size_t)s.F, st));
+            TRY(upload(&c->owner, owner.data(), owner.size(), st));
+            TRY(dalloc(&d_err, 1));
+            CU(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+            TRY(dalloc(&c->lr, s.F));
+            k_redirect<<<grid_of(s.F), BLOCK, 0, st>>>(s.F, s.F_bd, m->off_boundary_cells, d_face_cell,
+                                                       c->owner, (int)owner.size(), c->lr, d_err);
+            CU(cudaGetLastError());
+
+            // slots
+            TRY(dalloc(&d_cnt, 2 * (size_t)s.C));
+            CU(cudaMemsetAsync(d_cnt, 0, 2 * sizeof(int) * s.C, st));
+            TRY(dalloc(&c->slot_face, MAX_SLOTS * (size_t)s.C));
+            TRY(dalloc(&c->slot_nbr, MAX_SLOTS * (size_t)s.C));
+            TRY(dalloc(&c->slot_cnt, s.C));
+            TRY(dalloc(&c->gb.slot_w, 3 * MAX_SLOTS * (size_t)s.C));
+            TRY(dalloc(&c->gb.slot_off, 3 * MAX_SLOTS * (size_t)s.C));
+            k_slot_count<<<grid_of(s.F), BLOCK, 0, st>>>(s.F, s.F_in, c->lr, d_cnt);
+            k_slot_fill<<<grid_of(s.F), BLOCK, 0, st>>>(s.F, s.F_in, s.C, c->lr, d_cnt + s.C, c->slot_face);
+            TRY(upload(&d_weight, m->face_weight, 6 * (size_t)s.F, st));
+            TRY(upload(&d_offset, m->face_offset, 6 * (size_t)s.F, st));
+            k_slot_finish<double><<<grid_of(s.C), BLOCK, 0, st>>>(s.C, c->lr, d_cnt, d_weight, d_offset,
+                                                                  c->slot_face, c->slot_nbr, c->slot_cnt,
+                                                                  c->gb.slot_w, c->gb.slot_off, d_err);
+            CU(cudaGetLastError());
+
+            // face geometry, structure of arrays
+            TRY(upload(&c->gb.area, m->face_area, s.F, st));
+            TRY(dalloc(&c->gb.basis, 9 * (size_t)s.F));
+            TRY(dalloc(&c->gb.offl, 3 * (size_t)s.F));
+            TRY(dalloc(&c->gb.offr, 3 * (size_t)s.F));
+            TRY(dalloc(&d_tmp, 9 * (size_t)s.F));
+            CU(cudaMemcpyAsync(d_tmp, m->face_basis, 9 * sizeof(double) * s.F, cudaMemcpyHostToDevice, st));
+            k_transpose<double><<<grid_of(s.F), BLOCK, 0, st>>>(s.F, 9, d_tmp, c->gb.basis);
+            // offsets: AoS [F][2][3] -> left [3][F], right [3][F]
+            std::vector<double> ol(3 * (size_t)s.F), orr(3 * (size_t)s.F);
+            for (int f = 0; f < s.F; f++) {
+                for (int d = 0; d < 3; d++) {
+                    ol[(size_t)f * 3 + d] = m->face_offset[(size_t)f * 6 + d];
+                    orr[(size_t)f * 3 + d] = m->face_offset[(size_t)f * 6 + 3 + d];
+                }
+            }
+            CU(cudaStreamSynchronize(st));  // d_tmp reuse
+            CU(cudaMemcpyAsync(d_tmp, ol.data(), 3 * sizeof(double) * s.F, cudaMemcpyHostToDevice, st));
+            k_transpose<double><<<grid_of(s.F), BLOCK, 0, st>>>(s.F, 3, d_tmp, c->gb.offl);
+            CU(cudaStreamSynchronize(st));
+            CU(cudaMemcpyAsync(d_tmp, orr.data(), 3 * sizeof(double) * s.F, cudaMemcpyHostToDevice, st));
+            k_transpose<double><<<grid_of(s.F), BLOCK, 0, st>>>(s.F, 3, d_tmp, c->gb.offr);
+            if (e->viscous == TG_VISCOUS_CENTRAL) {
+                TRY(dalloc(&c->gb.corr, 4 * (size_t)s.F));
+                CU(cudaStreamSynchronize(st));
+                CU(cudaMemcpyAsync(d_tmp, m->face_correction, 4 * sizeof(double) * s.F,
+                                   cudaMemcpyHostToDevice, st));
+                k_transpose<double><<<grid_of(s.F), BLOCK, 0, st>>>(s.F, 4, d_tmp, c->gb.corr);
+            }
+            CU(cudaGetLastError());
+
+            // cells
+            TRY(upload(&c->volume, m->cell_volume, s.C, st));
+            TRY(dalloc(&c->proj, 3 * (size_t)s.C));
+            CU(cudaStreamSynchronize(st));
+            CU(cudaMemcpyAsync(d_tmp, m->cell_projection, 3 * sizeof(double) * s.C, cudaMemcpyHostToDevice, st));
+            k_transpose<double><<<grid_of(s.C), BLOCK, 0, st>>>(s.C, 3, d_tmp, c->proj);
+            if (e->limiter == TG_LIMITER_VENKATAKRISHNAN) {
+                std::vector<double> eps2(s.C);
+                for (int i = 0; i < s.C; i++) {
+                    if (e->limiter_parameter) {
+                        eps2[i] = e->limiter_parameter[i];
+                    }
+                    else {  // eps^2 = (K * V^(1/3))^3, src/equations/limiter.c:8-21
+                        double x = e->limiter_coefficient * cbrt(m->cell_volume[i]);
+                        eps2[i] = (x * x) * x;
+                    }
+                }
+                TRY(upload(&c->eps2, eps2.data(), s.C, st));
+                CU(cudaStreamSynchronize(st));
+            }
+            if (s.F_bd > s.F_in) TRY(upload(&c->bface_ent, bent.data(), bent.size(), st));
+            CU(cudaGetLastError());
+
+            int h_err = 0;
+            CU(cudaMemcpyAsync(&h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+            CU(cudaStreamSynchronize(st));
+            if (h_err == 1) return fail(TG_ERR_INVALID, "a cell has more than %d or no faces", MAX_SLOTS);
+            if (h_err == 2) return fail(TG_ERR_INVALID, "periodic face right cell is not a periodic ghost");
+            return TG_OK;
+        }();
+        cleanup();
+        TRY(r2);
+
+        // FP32 copies for the FP32 flux form
+        if (precision == TG_PRECISION_FP32_FLUX) {
+            TRY(alloc_geom32(c));
+            TRY(to_float(c->gb.area, c->gb.area32, s.F, st));
+            TRY(to_float(c->gb.basis, c->gb.basis32, 9 * (size_t)s.F, st));
+            TRY(to_float(c->gb.offl, c->gb.offl32, 3 * (size_t)s.F, st));
+            TRY(to_float(c->gb.offr, c->gb.offr32, 3 * (size_t)s.F, st));
+            TRY(to_float(c->gb.corr, c->gb.corr32, 4 * (size_t)s.F, st));
+            TRY(to_float(c->gb.slot_w, c->gb.slot_w32, 3 * MAX_SLOTS * (size_t)s.C, st));
+            TRY(to_float(c->gb.slot_off, c->gb.slot_off32, 3 * MAX_SLOTS * (size_t)s.C, st));
+        }
+        c->g64 = Geometry<double>{c->lr,       c->gb.area, c->gb.basis, c->gb.offl,   c->gb.offr,   c->gb.corr,
+                                  c->slot_nbr, c->slot_face, c->slot_cnt, c->gb.slot_w, c->gb.slot_off};
+        c->g32 = Geometry<float>{c->lr,       c->gb.area32, c->gb.basis32, c->gb.offl32,   c->gb.offr32,
+                                 c->gb.corr32, c->slot_nbr, c->slot_face, c->slot_cnt, c->gb.slot_w32,
+                                 c->gb.slot_off32};
+
+        // state
+        size_t rsz = precision == TG_PRECISION_FP64 ? sizeof(double) : sizeof(float);
+        TRY(dalloc(&c->q, 5 * (size_t)s.N));
+        CU(cudaMemsetAsync(c->q, 0, 5 * sizeof(double) * s.N, st));
+        TRY(dalloc(&c->U0, 5 * (size_t)s.C));
+        TRY(dalloc(&c->R, 5 * (size_t)s.C));
+        if (c->order == 2) {
+            CU(cudaMalloc(&c->grad, 15 * rsz * s.C));
+            CU(cudaMalloc(&c->psi, 5 * rsz * s.C));
+        }
+        CU(cudaMalloc(&c->G, 5 * rsz * s.F));
+        c->nblk = grid_of(s.C);
+        TRY(dalloc(&c->part_dt, c->nblk));
+        TRY(dalloc(&c->part_res, 5 * (size_t)c->nblk));
+        TRY(dalloc(&c->st, 1));
+        CU(cudaMallocHost(&c->st_host, sizeof(StepState)));
+        memset(c->st_host, 0, sizeof(StepState));
+        c->st_host->max_step = DBL_MAX;
+        c->st_host->max_time = DBL_MAX;
+        CU(cudaMemcpyAsync(c->st, c->st_host, sizeof(StepState), cudaMemcpyHostToDevice, st));
+        c->aos_len = (size_t)15 * (c->num_cells > s.F ? c->num_cells : s.F);
+        TRY(dalloc(&c->aos, c->aos_len));
+        CU(cudaStreamSynchronize(st));
+        return TG_OK;
+    }();
+    if (rc != TG_OK) {
+        std::string msg = g_error;
+        cudaDeviceSynchronize();
+        free_ctx(c);
+        g_error = msg;
+        return rc;
+    }
+    *out = c;
+    return TG_OK;
+}
+
+extern "C" int tg_destroy(tg_ctx *c)
+{
+    if (!c) return TG_OK;
+    cudaStreamSynchronize(c->stream);
+    free_ctx(c);
+    return TG_OK;
+}
+
+extern "C" int tg_set_stream(tg_ctx *c, void *stream)
+{
+    if (!c) return fail(TG_ERR_INVALID, "null context");
+    CU(cudaStreamSynchronize(c->stream));
+    c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+    if (c->graph) {
+        cudaGraphExecDestroy(c->graph);
+        c->graph = nullptr;
+        c->graph_method = -1;
+    }
+    return TG_OK;
+}
+
+// ---- host transfers --------------------------------------------------------------------------
+
+static int ensure_pinned(tg_ctx *c, size_t n)
+{
+    if (c->pinned_len >= n) return TG_OK;
+    if (c->pinned) cudaFreeHost(c->pinned);
+    c->pinned = nullptr;
+    c->pinned_len = 0;
+    CU(cudaMallocHost(&c->pinned, n * sizeof(double)));
+    c->pinned_len = n;
+    return TG_OK;
+}
+
+// host AoS -> device (through pinned staging when the source is pageable)
+static int h2d(tg_ctx *c, double *dst, const double *src, size_t n)
+{
+    cudaPointerAttributes at;
+    bool pinned = cudaPointerGetAttributes(&at, src) == cudaSuccess && at.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    if (pinned) {
+        CU(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        return TG_OK;
+    }
+    TRY(ensure_pinned(c, n));
+    memcpy(c->pinned, src, n * sizeof(double));
+    CU(cudaMemcpyAsync(dst, c->pinned, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    return TG_OK;
+}
+
+static int d2h(tg_ctx *c, double *dst, const double *src, size_t n)
+{
+    cudaPointerAttributes at;
+    bool pinned = cudaPointerGetAttributes(&at, dst) == cudaSuccess && at.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    if (pinned) {
+        CU(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CU(cudaStreamSynchronize(c->stream));
+        return TG_OK;
+    }
+    TRY(ensure_pinned(c, n));
+    CU(cudaMemcpyAsync(c->pinned, src, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    memcpy(dst, c->pinned, n * sizeof(double));
+    return TG_OK;
+}
+
+extern "C" int tg_set_primitive(tg_ctx *c, const double *prim)
+{
+    if (!c || !prim) return fail(TG_ERR_INVALID, "null argument");
+    TRY(h2d(c, c->aos, prim, 5 * (size_t)c->s.C));
+    k_prim_aos_to_soa<<<grid_of(c->s.C), BLOCK, 0, c->stream>>>(c->s.C, c->s.N, c->aos, c->q);
+    CU(cudaGetLastError());
+    c->prepared = false;
+    return TG_OK;
+}
+
+extern "C" int tg_get_primitive(tg_ctx *c, double *prim)
+{
+    if (!c || !prim) return fail(TG_ERR_INVALID, "null argument");
+    k_prim_soa_to_aos<<<grid_of(c->num_cells), BLOCK, 0, c->stream>>>(c->s.N, c->num_cells, c->s.N, c->owner,
+                                                                        c->q, c->aos);
+    CU(cudaGetLastError());
+    TRY(d2h(c, prim, c->aos, 5 * (size_t)c->num_cells));
+    return TG_OK;
+}
+
+// ---- kernel sequencing -----------------------------------------------------------------------
+
+static Props props_of(const tg_ctx *c)
+{
+    Props p;
+    for (int i = 0; i < 3; i++) p.v[i] = c->prop[i];
+    return p;
+}
+
+static bool is_ns(const tg_ctx *c)
+{
+    return c->physics == TG_NAVIERSTOKES;
+}
+
+// teal's O2 path keeps the unlimited gradient only when a viscous flux needs it
+static bool fold_psi(const tg_ctx *c)
+{
+    return !(c->viscous == TG_VISCOUS_CENTRAL) || c->limiter == TG_LIMITER_NONE;
+}
+
+static int run_boundary(tg_ctx *c, double *q)
+{
+    int nbf = c->s.F_bd - c->s.F_in;
+    if (nbf <= 0) return TG_OK;
+    Launch l(c, TG_PROF_BOUNDARY);
+    k_boundary<<<grid_of(nbf), BLOCK, 0, c->stream>>>(c->s, c->lr, c->gb.basis, c->bface_ent, c->bt, q,
+                                                      c->prop[0]);
+    CU(cudaGetLastError());
+    return TG_OK;
+}
+
+template <typename R>
+static void launch_gradient(tg_ctx *c, const Geometry<R> &g, bool fold, const double *q)
+{
+    dim3 grid(grid_of(c->s.C));
+    R *grad = (R *)c->grad;
+    R *psi = (R *)c->psi;
+    switch (c->limiter) {
+        case TG_LIMITER_NONE:
+            k_gradient<R, 0, true><<<grid, BLOCK, 0, c->stream>>>(c->s, g, c->eps2, q, grad, psi);
+            break;
+        case TG_LIMITER_BARTH_JESPERSEN:
+            if (fold)
+                k_gradient<R, 1, true><<<grid, BLOCK, 0, c->stream>>>(c->s, g, c->eps2, q, grad, psi);
+            else
+                k_gradient<R, 1, false><<<grid, BLOCK, 0, c->stream>>>(c->s, g, c->eps2, q, grad, psi);
+            break;
+        default:
+            if (fold)
+                k_gradient<R, 2, true><<<grid, BLOCK, 0, c->stream>>>(c->s, g, c->eps2, q, grad, psi);
+            else
+                k_gradient<R, 2, false><<<grid, BLOCK, 0, c->stream>>>(c->s, g, c->eps2, q, grad, psi);
+            break;
+    }
+}
+
+// gradient with an explicit limiter choice (tg_gradient reports the unlimited one on request)
+static int run_gradient(tg_ctx *c, const double *q, int limiter_override = -1)
+{
+    int saved = c->limiter;
+    if (limiter_override >= 0) c->limiter = limiter_override;
+    bool fold = fold_psi(c);
+    Launch l(c, TG_PROF_GRADIENT);
+    if (c->precision == TG_PRECISION_FP64)
+        launch_gradient<double>(c, c->g64, fold, q);
+    else
+        launch_gradient<float>(c, c->g32, fold, q);
+    c->limiter = saved;
+    CU(cudaGetLastError());
+    return TG_OK;
+}
+
+static int run_face(tg_ctx *c, const double *q)
+{
+    FaceLaunch a;
+    a.s = c->s;
+    a.geom = c->precision == TG_PRECISION_FP64 ? (const void *)&c->g64 : (const void *)&c->g32;
+    a.q = q;
+    a.grad = c->grad;
+    a.psi = c->psi;
+    a.gamma = c->prop[0];
+    a.mu = c->prop[1];
+    a.prandtl = c->prop[2];
+    a.G = c->G;
+    bool ns = c->viscous == TG_VISCOUS_CENTRAL;
+    bool fold = fold_psi(c);
+    Launch l(c, TG_PROF_FACE);
+    cudaError_t e;
+    switch (c->flux) {
+        case TG_FLUX_ROE: e = launch_face<FK_ROE>(c->precision, ns, c->order, fold, a, c->stream); break;
+        case TG_FLUX_HLL: e = launch_face<FK_HLL>(c->precision, ns, c->order, fold, a, c->stream); break;
+        case TG_FLUX_HLLC: e = launch_face<FK_HLLC>(c->precision, ns, c->order, fold, a, c->stream); break;
+        case TG_FLUX_HLLE: e = launch_face<FK_HLLE>(c->precision, ns, c->order, fold, a, c->stream); break;
+        case TG_FLUX_AUSMD: e = launch_face<FK_AUSMD>(c->precision, ns, c->order, fold, a, c->stream); break;
+        case TG_FLUX_AUSMDV: e = launch_face<FK_AUSMDV>(c->precision, ns, c->order, fold, a, c->stream); break;
+        case TG_FLUX_LXF: e = launch_face<FK_LXF>(c->precision, ns, c->order, fold, a, c->stream); break;
+        case TG_FLUX_CENTRAL: e = launch_face<FK_CENTRAL>(c->precision, ns, c->order, fold, a, c->stream); break;
+        default: e = launch_face<FK_NONE>(c->precision, ns, c->order, fold, a, c->stream); break;
+    }
+    CU(e);
+    return TG_OK;
+}
+
+template <int MODE>
+static int launch_cell(tg_ctx *c, double alpha, int last, double *q, double *Rout)
+{
+    CellData cd{c->volume, c->proj, c->eps2};
+    dim3 grid(c->nblk);
+    Props p = props_of(c);
+    bool ns = is_ns(c);
+    Launch l(c, TG_PROF_CELL);
+    if (c->precision == TG_PRECISION_FP64) {
+        const double *G = (const double *)c->G;
+        if (ns)
+            k_cell<MODE, true, double><<<grid, BLOCK, 0, c->stream>>>(c->s, c->slot_face, c->slot_cnt, cd, G, c->U0,
+                                                                       q, Rout, c->st, alpha, last, p,
+                                                                       c->part_dt, c->part_res);
+        else
+            k_cell<MODE, false, double><<<grid, BLOCK, 0, c->stream>>>(c->s, c->slot_face, c->slot_cnt, cd, G, c->U0,
+                                                                        q, Rout, c->st, alpha, last, p,
+                                                                        c->part_dt, c->part_res);
+    }
+    else {
+        const float *G = (const float *)c->G;
+        if (ns)
+            k_cell<MODE, true, float><<<grid, BLOCK, 0, c->stream>>>(c->s, c->slot_face, c->slot_cnt, cd, G, c->U0,
+                                                                      q, Rout, c->st, alpha, last, p,
+                                                                      c->part_dt, c->part_res);
+        else
+            k_cell<MODE, false, float><<<grid, BLOCK, 0, c->stream>>>(c->s, c->slot_face, c->slot_cnt, cd, G, c->U0,
+                                                                       q, Rout, c->st, alpha, last, p,
+                                                                       c->part_dt, c->part_res);
+    }
+    CU(cudaGetLastError());
+    return TG_OK;
+}
+
+// boundary pass, gradient + limiter, face fluxes: everything of a residual before the gather
+static int run_fluxes(tg_ctx *c, double *q)
+{
+    TRY(run_boundary(c, q));
+    if (c->order == 2) TRY(run_gradient(c, q));
+    TRY(run_face(c, q));
+    return TG_OK;
+}
+
+static int run_prepare(tg_ctx *c)
+{
+    CellData cd{c->volume, c->proj, c->eps2};
+    if (is_ns(c))
+        k_prepare<true><<<c->nblk, BLOCK, 0, c->stream>>>(c->s, cd, c->q, c->U0, props_of(c), c->part_dt);
+    else
+        k_prepare<false><<<c->nblk, BLOCK, 0, c->stream>>>(c->s, cd, c->q, c->U0, props_of(c), c->part_dt);
+    CU(cudaGetLastError());
+    c->prepared = true;
+    return TG_OK;
+}
+
+// ---- public single-evaluation entry points ----------------------------------------------------
+
+extern "C" int tg_derivative(tg_ctx *c, const double *prim, double *deriv, double time)
+{
+    (void)time;  // device boundary conditions do not depend on time
+    if (!c || !deriv) return fail(TG_ERR_INVALID, "null argument");
+    double *q = c->q;
+    if (prim) {  // evaluate a host-given state in scratch memory; the resident state stays as it is
+        if (!c->qs) {
+            TRY(dalloc(&c->qs, 5 * (size_t)c->s.N));
+            CU(cudaMemsetAsync(c->qs, 0, 5 * sizeof(double) * c->s.N, c->stream));
+        }
+        q = c->qs;
+        TRY(h2d(c, c->aos, prim, 5 * (size_t)c->s.C));
+        k_prim_aos_to_soa<<<grid_of(c->s.C), BLOCK, 0, c->stream>>>(c->s.C, c->s.N, c->aos, q);
+        CU(cudaGetLastError());
+    }
+    TRY(run_fluxes(c, q));
+    TRY(launch_cell<0>(c, 0.0, 0, q, c->R));
+    k_soa5_to_aos<<<grid_of(c->s.C), BLOCK, 0, c->stream>>>(c->s.C, c->R, c->aos);
+    CU(cudaGetLastError());
+    TRY(d2h(c, deriv, c->aos, 5 * (size_t)c->s.C));
+    return TG_OK;
+}
+
+extern "C" int tg_gradient(tg_ctx *c, double time, int limited, double *gradient)
+{
+    (void)time;
+    if (!c || !gradient) return fail(TG_ERR_INVALID, "null argument");
+    if (c->order != 2) return fail(TG_ERR_INVALID, "gradients exist only at space order 2");
+    TRY(run_boundary(c, c->q));
+    int lim = limited ? c->limiter : TG_LIMITER_NONE;
+    TRY(run_gradient(c, c->q, lim));
+    bool fold = limited ? (fold_psi(c) || lim == TG_LIMITER_NONE) : true;
+    // with fold the stored gradient already carries psi
+    if (c->precision == TG_PRECISION_FP64)
+        k_grad_to_aos<double><<<grid_of(c->s.C), BLOCK, 0, c->stream>>>(
+            c->s.C, (const double *)c->grad, fold ? nullptr : (const double *)c->psi, c->aos);
+    else
+        k_grad_to_aos<float><<<grid_of(c->s.C), BLOCK, 0, c->stream>>>(
+            c->s.C, (const float *)c->grad, fold ? nullptr : (const float *)c->psi, c->aos);
+    CU(cudaGetLastError());
+    TRY(d2h(c, gradient, c->aos, 15 * (size_t)c->s.C));
+    return TG_OK;
+}
+
+static int read_state(tg_ctx *c)
+{
+    CU(cudaMemcpyAsync(c->st_host, c->st, sizeof(StepState), cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    return TG_OK;
+}
+
+static int write_state(tg_ctx *c)
+{
+    CU(cudaMemcpyAsync(c->st, c->st_host, sizeof(StepState), cudaMemcpyHostToDevice, c->stream));
+    return TG_OK;
+}
+
+extern "C" int tg_timestep(tg_ctx *c, double *step)
+{
+    if (!c || !step) return fail(TG_ERR_INVALID, "null argument");
+    TRY(run_prepare(c));
+    TRY(read_state(c));
+    c->st_host->use_max_time = 0;
+    c->st_host->max_step = DBL_MAX;
+    TRY(write_state(c));
+    k_step_begin<<<1, REDUCE_BLOCK, 0, c->stream>>>(c->part_dt, c->nblk, 1.0, c->st);
+    CU(cudaGetLastError());
+    TRY(read_state(c));
+    *step = c->st_host->step0;
+    return TG_OK;
+}
+
+extern "C" int tg_residual(tg_ctx *c, const double *deriv, double *residual)
+{
+    if (!c || !deriv || !residual) return fail(TG_ERR_INVALID, "null argument");
+    TRY(h2d(c, c->aos, deriv, 5 * (size_t)c->s.C));
+    k_aos5_to_soa<<<grid_of(c->s.C), BLOCK, 0, c->stream>>>(c->s.C, c->aos, c->R);
+    k_residual_part<<<c->nblk, BLOCK, 0, c->stream>>>(c->s, c->volume, c->R, c->part_res);
+    k_step_end<<<1, REDUCE_BLOCK, 0, c->stream>>>(c->part_res, c->nblk, c->sum_volume, 0, c->st);
+    CU(cudaGetLastError());
+    TRY(read_state(c));
+    for (int v = 0; v < 5; v++) residual[v] = c->st_host->residual[v];
+    return TG_OK;
+}
+
+// ---- explicit steps --------------------------------------------------------------------------
+
+static int rk_params(const tg_ctx *c, int method, const void *context, int *stages, const double **alpha)
+{
+    static const double euler_alpha[2] = {0.0, 1.0};
+    if (method == TG_ADVANCE_EULER) {
+        *stages = 1;
+        *alpha = euler_alpha;
+        return TG_OK;
+    }
+    int order = c->order, ns = c->order + 1;  // teal's default (src/simulation/set.c:88-96)
+    if (context) {
+        const tg_runge_kutta *rk = (const tg_runge_kutta *)context;
+        order = rk->time_order;
+        ns = rk->num_stages;
+    }
+    if (order < 1 || order > 3) return fail(TG_ERR_INVALID, "invalid time order (%d)", order);
+    if (ns < 1 || ns > 6) return fail(TG_ERR_INVALID, "invalid number of stages (%d)", ns);
+    *stages = ns;
+    *alpha = LSERK_ALPHA[order - 1][ns - 1];
+    return TG_OK;
+}
+
+// one explicit step on the resident state (U0 and the time-step partials must be current)
+static int enqueue_explicit_step(tg_ctx *c, int stages, const double *alpha, double courant)
+{
+    {
+        Launch l(c, TG_PROF_REDUCE);
+        k_step_begin<<<1, REDUCE_BLOCK, 0, c->stream>>>(c->part_dt, c->nblk, courant, c->st);
+    }
+    CU(cudaGetLastError());
+    for (int i = 0; i < stages; i++) {
+        TRY(run_fluxes(c, c->q));
+        TRY(launch_cell<1>(c, alpha[i + 1], i == stages - 1, c->q, c->R));
+    }
+    {
+        Launch l(c, TG_PROF_REDUCE);
+        k_step_end<<<1, REDUCE_BLOCK, 0, c->stream>>>(c->part_res, c->nblk, c->sum_volume, 1, c->st);
+    }
+    CU(cudaGetLastError());
+    return TG_OK;
+}
+
+// one explicit step: a replay of the step's CUDA graph, or plain launches while events time them
+static int launch_step(tg_ctx *c, int stages, const double *alpha, double courant)
+{
+    if (c->prof_on) return enqueue_explicit_step(c, stages, alpha, courant);
+    CU(cudaGraphLaunch(c->graph, c->stream));
+    c->launches += c->graph_kernels;
+    return TG_OK;
+}
+
+static int step_graph(tg_ctx *c, int method, int stages, const double *alpha, double courant, int use_max_time)
+{
+    if (c->graph && c->graph_method == method && c->graph_stages == stages && c->graph_courant == courant &&
+        c->graph_use_max_time == use_max_time && c->graph_order == c->order) {
+        return TG_OK;
+    }
+    if (c->graph) {
+        cudaGraphExecDestroy(c->graph);
+        c->graph = nullptr;
+    }
+    cudaGraph_t g;
+    CU(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    long before = c->launches;
+    bool prof = c->prof_on;
+    c->prof_on = false;
+    int rc = enqueue_explicit_step(c, stages, alpha, courant);
+    c->prof_on = prof;
+    c->graph_kernels = c->launches - before;
+    c->launches = before;
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (rc != TG_OK) {
+        if (e == cudaSuccess) cudaGraphDestroy(g);
+        return rc;
+    }
+    CU(e);
+    cudaError_t e2 = cudaGraphInstantiate(&c->graph, g, 0);
+    cudaGraphDestroy(g);
+    CU(e2);
+    c->graph_method = method;
+    c->graph_stages = stages;
+    c->graph_courant = courant;
+    c->graph_use_max_time = use_max_time;
+    c->graph_order = c->order;
+    return TG_OK;
+}
+
+static int check_error(tg_ctx *c)
+{
+    if (c->st_host->error) {
+        c->st_host->error = 0;
+        write_state(c);
+        return fail(TG_ERR_NONFINITE, "non-finite time step or residual");
+    }
+    return TG_OK;
+}
+
+static int implicit_euler_step(tg_ctx *c, const void *context, double courant, double *time,
+                               double max_step, double *residual, double *step0);
+
+extern "C" int tg_advance(tg_ctx *c, int method, const void *context, double courant, double *time,
+                          double max_step, double *residual, double *step0)
+{
+    if (!c || !time) return fail(TG_ERR_INVALID, "null argument");
+    if (!(courant > 0)) return fail(TG_ERR_INVALID, "invalid courant number (%g)", courant);
+    if (method == TG_ADVANCE_IMPLICIT_EULER) {
+        return implicit_euler_step(c, context, courant, time, max_step, residual, step0);
+    }
+    if (method != TG_ADVANCE_EULER && method != TG_ADVANCE_LSERK)
+        return fail(TG_ERR_INVALID, "invalid advance method (%d)", method);
+    int stages;
+    const double *alpha;
+    TRY(rk_params(c, method, context, &stages, &alpha));
+    if (!c->prepared) TRY(run_prepare(c));
+    c->st_host->time = *time;
+    c->st_host->max_step = max_step;
+    c->st_host->use_max_time = 0;
+    c->st_host->error = 0;
+    TRY(write_state(c));
+    TRY(step_graph(c, method, stages, alpha, courant, 0));
+    TRY(launch_step(c, stages, alpha, courant));
+    TRY(read_state(c));
+    TRY(check_error(c));
+    *time = c->st_host->time;
+    if (residual)
+        for (int v = 0; v < 5; v++) residual[v] = c->st_host->residual[v];
+    if (step0) *step0 = c->st_host->step0;
+    return TG_OK;
+}
+
+extern "C" int tg_run(tg_ctx *c, int method, const void *context, double courant, int max_iter,
+                      double max_time, int variable, double threshold, double *time, int *iter,
+                      double *residual)
+{
+    if (!c || !time || !iter) return fail(TG_ERR_INVALID, "null argument");
+    if (variable < -1 || variable > 4) return fail(TG_ERR_INVALID, "invalid termination variable");
+    if (method == TG_ADVANCE_IMPLICIT_EULER) {
+        // implicit steps synchronise inside the Newton loop; run them one by one
+        int it = 0;
+        double res[5] = {0, 0, 0, 0, 0};
+        while (it < max_iter && *time < max_time) {
+            double s0;
+            TRY(tg_advance(c, method, context, courant, time, max_time - *time, res, &s0));
+            it++;
+            if (threshold > 0) {
+                double m = 0;
+                for (int v = 0; v < 5; v++) m = res[v] > m ? res[v] : m;
+                if (((variable >= 0) ? res[variable] : m) < threshold) break;
+            }
+        }
+        *iter = it;
+        if (residual)
+            for (int v = 0; v < 5; v++) residual[v] = res[v];
+        return TG_OK;
+    }
+    if (method != TG_ADVANCE_EULER && method != TG_ADVANCE_LSERK)
+        return fail(TG_ERR_INVALID, "invalid advance method (%d)", method);
+    int stages;
+    const double *alpha;
+    TRY(rk_params(c, method, context, &stages, &alpha));
+    if (!c->prepared) TRY(run_prepare(c));
+    c->st_host->time = *time;
+    c->st_host->max_time = max_time;
+    c->st_host->use_max_time = 1;
+    c->st_host->error = 0;
+    TRY(write_state(c));
+    TRY(step_graph(c, method, stages, alpha, courant, 1));
+    bool check_each = threshold > 0 || max_time < DBL_MAX;
+    int it = 0;
+    while (it < max_iter) {
+        TRY(launch_step(c, stages, alpha, courant));
+        it++;
+        if (check_each) {
+            TRY(read_state(c));
+            TRY(check_error(c));
+            const double *res = c->st_host->residual;
+            if (threshold > 0) {
+                double m = 0;
+                for (int v = 0; v < 5; v++) m = res[v] > m ? res[v] : m;
+                if (((variable >= 0) ? res[variable] : m) < threshold) break;
+            }
+            // teal's loop condition is_less(time, max_time) (src/simulation/run.c:68)
+            double t = c->st_host->time;
+            bool close = fabs(t - max_time) <= fmax(1e-8, 1e-5 * fmax(fabs(t), fabs(max_time)));
+            if (!(t < max_time) || close) break;
+        }
+    }
+    TRY(read_state(c));
+    TRY(check_error(c));
+    *time = c->st_host->time;
+    *iter = it;
+    if (residual)
+        for (int v = 0; v < 5; v++) residual[v] = c->st_host->residual[v];
+    return TG_OK;
+}
+
+// ---- implicit Euler with Jacobian-free Newton-GMRES (advance.c:119-195, gmres.c:52-149) --------
+
+static int gm_alloc(tg_ctx *c, int dim)
+{
+    Gmres &g = c->gm;
+    if (g.V && g.dim >= dim) return TG_OK;
+    void *old[] = {g.U, g.Ustart, g.r, g.delta, g.V, g.w, g.q1, g.R1, g.part, g.sc};
+    for (void *p : old) {
+        if (p) cudaFree(p);
+    }
+    g = Gmres{};
+    size_t n = 5 * (size_t)c->s.C;
+    TRY(dalloc(&g.U, n));
+    TRY(dalloc(&g.Ustart, n));
+    TRY(dalloc(&g.r, n));
+    TRY(dalloc(&g.delta, n));
+    TRY(dalloc(&g.V, (size_t)(dim + 1) * n));
+    TRY(dalloc(&g.w, n));
+    TRY(dalloc(&g.q1, 5 * (size_t)c->s.N));
+    CU(cudaMemset(g.q1, 0, 5 * sizeof(double) * c->s.N));
+    TRY(dalloc(&g.R1, n));
+    TRY(dalloc(&g.part, 1024));
+    TRY(dalloc(&g.sc, GS_HEAD + (size_t)(dim + 1) * dim + 4 * (size_t)dim + 2));
+    g.dim = dim;
+    return TG_OK;
+}
+
+static const int DOT_BLOCKS = 1024;
+
+// dst = x . y (or |x| when x == y and take_sqrt)
+static int gm_dot(tg_ctx *c, const double *x, const double *y, double *dst, int take_sqrt)
+{
+    long n = 5L * c->s.C;
+    int nb = (int)((n + BLOCK - 1) / BLOCK);
+    nb = nb < DOT_BLOCKS ? nb : DOT_BLOCKS;
+    k_dot_part<<<nb, BLOCK, 0, c->stream>>>(n, x, y, c->gm.part);
+    k_reduce_scalar<<<1, REDUCE_BLOCK, 0, c->stream>>>(c->gm.part, nb, dst, take_sqrt);
+    CU(cudaGetLastError());
+    return TG_OK;
+}
+
+static int gm_read(tg_ctx *c, int idx, double *out)
+{
+    CU(cudaMemcpyAsync(out, c->gm.sc + idx, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    return TG_OK;
+}
+
+// derivative of a primitive state q (boundary rows refreshed) into Rout
+static int gm_derivative(tg_ctx *c, double *q, double *Rout)
+{
+    TRY(run_fluxes(c, q));
+    TRY(launch_cell<0>(c, 0.0, 0, q, Rout));
+    return TG_OK;
+}
+
+// one GMRES cycle for the increment (gmres.c:52-149)
+static int gm_solve(tg_ctx *c, double krylov_tol, int dim)
+{
+    Gmres &g = c->gm;
+    long n = 5L * c->s.C;
+    int gb = (int)((n + BLOCK - 1) / BLOCK);
+    double *sc = g.sc;
+    double norm;
+    TRY(gm_read(c, GS_NORM, &norm));
+    if (norm <= 0) {
+        CU(cudaMemsetAsync(g.delta, 0, n * sizeof(double), c->stream));
+        return TG_OK;
+    }
+    k_gmres_start<<<gb, BLOCK, 0, c->stream>>>(n, dim, g.r, g.V, g.delta, sc, krylov_tol);
+    CU(cudaGetLastError());
+    int m = 0;
+    for (; m < dim; m++) {
+        double *Vm = g.V + (long)m * n;
+        // matvec (gmres.c:12-50)
+        TRY(gm_dot(c, Vm, Vm, sc + GS_VNORM, 1));
+        k_perturb<<<grid_of(c->s.C), BLOCK, 0, c->stream>>>(c->s.C, c->s.N, g.U, Vm, sc, c->prop[0], g.q1);
+        CU(cudaGetLastError());
+        TRY(gm_derivative(c, g.q1, g.R1));
+        k_matvec_finish<<<gb, BLOCK, 0, c->stream>>>(n, Vm, g.R1, c->R, sc, g.w);
+        // modified Gram-Schmidt
+        for (int i = 0; i <= m; i++) {
+            TRY(gm_dot(c, g.V + (long)i * n, g.w, sc + GS_DOT, 0));
+            k_store_h<<<1, 1, 0, c->stream>>>(sc, dim, i, m);
+            k_mgs_axpy<<<gb, BLOCK, 0, c->stream>>>(n, g.V + (long)i * n, sc, dim, i, m, g.w);
+        }
+        TRY(gm_dot(c, g.w, g.w, sc + GS_DOT, 1));
+        k_store_h<<<1, 1, 0, c->stream>>>(sc, dim, m + 1, m);
+        k_givens<<<1, 1, 0, c->stream>>>(sc, dim, m);
+        CU(cudaGetLastError());
+        double done;
+        TRY(gm_read(c, GS_DONE, &done));
+        if (done != 0.0) {
+            m += 1;
+            break;
+        }
+        k_normalize<<<gb, BLOCK, 0, c->stream>>>(n, g.w, sc, dim, m, g.V + (long)(m + 1) * n);
+    }
+    k_backsolve<<<1, 1, 0, c->stream>>>(sc, dim, m);
+    k_accumulate<<<gb, BLOCK, 0, c->stream>>>(n, g.V, sc, dim, m, g.delta);
+    CU(cudaGetLastError());
+    return TG_OK;
+}
+
+static int implicit_euler_step(tg_ctx *c, const void *context, double courant, double *time,
+                               double max_step, double *residual, double *step0)
+{
+    double newton_tol = 0.1, krylov_tol = 0.3;  // teal's defaults (src/simulation/set.c:113-115)
+    int dim = 32;
+    if (context) {
+        const tg_newton_krylov *nk = (const tg_newton_krylov *)context;
+        newton_tol = nk->newton_tolerance;
+        krylov_tol = nk->krylov_tolerance;
+        dim = nk->krylov_dimension;
+    }
+    if (!(newton_tol > 0)) return fail(TG_ERR_INVALID, "invalid newton tolerance (%g)", newton_tol);
+    if (!(krylov_tol > 0)) return fail(TG_ERR_INVALID, "invalid krylov tolerance (%g)", krylov_tol);
+    if (dim <= 0) return fail(TG_ERR_INVALID, "invalid krylov dimension (%d)", dim);
+    TRY(gm_alloc(c, dim));
+    Gmres &g = c->gm;
+    long n = 5L * c->s.C;
+    int gb = (int)((n + BLOCK - 1) / BLOCK);
+    double *sc = g.sc;
+
+    // step from the CFL condition; U = cons(q) (advance.c:136-143)
+    TRY(run_prepare(c));
+    c->st_host->time = *time;
+    c->st_host->max_step = max_step;
+    c->st_host->use_max_time = 0;
+    c->st_host->error = 0;
+    TRY(write_state(c));
+    k_step_begin<<<1, REDUCE_BLOCK, 0, c->stream>>>(c->part_dt, c->nblk, courant, c->st);
+    CU(cudaGetLastError());
+    TRY(read_state(c));
+    TRY(check_error(c));
+    double step = c->st_host->step;
+    CU(cudaMemcpyAsync(g.U, c->U0, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    CU(cudaMemcpyAsync(g.Ustart, c->U0, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    CU(cudaMemcpyAsync(sc + GS_STEP, &c->st_host->step, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    c->prepared = false;
+
+    double t = *time + step;
+    TRY(gm_derivative(c, c->q, c->R));
+    k_newton_init<<<gb, BLOCK, 0, c->stream>>>(n, c->R, sc, g.r);
+    TRY(gm_dot(c, g.r, g.r, sc + GS_NORM, 1));
+    TRY(gm_dot(c, g.U, g.U, sc + GS_CONS_NORM, 1));
+    k_fd_scale<<<1, 1, 0, c->stream>>>(sc);
+    CU(cudaGetLastError());
+    double norm;
+    TRY(gm_read(c, GS_NORM, &norm));
+    if (!std::isfinite(norm)) return fail(TG_ERR_NONFINITE, "non-finite Newton residual");
+    double tol_norm = newton_tol * norm;
+    long max_iter = 128L * (c->s.C + 1);
+    for (long it = 0; it < max_iter && norm > tol_norm; it++) {
+        TRY(gm_solve(c, krylov_tol, dim));
+        k_newton_update<<<grid_of(c->s.C), BLOCK, 0, c->stream>>>(c->s.C, c->s.N, g.U, g.delta, c->prop[0], c->q);
+        TRY(gm_derivative(c, c->q, c->R));
+        k_newton_residual<<<gb, BLOCK, 0, c->stream>>>(n, g.U, g.Ustart, c->R, sc, g.r);
+        TRY(gm_dot(c, g.r, g.r, sc + GS_NORM, 1));
+        TRY(gm_dot(c, g.U, g.U, sc + GS_CONS_NORM, 1));
+        k_fd_scale<<<1, 1, 0, c->stream>>>(sc);
+        CU(cudaGetLastError());
+        TRY(gm_read(c, GS_NORM, &norm));
+        if (!std::isfinite(norm)) return fail(TG_ERR_NONFINITE, "non-finite Newton residual");
+    }
+    // residual of the last derivative (advance.c:188)
+    k_residual_part<<<c->nblk, BLOCK, 0, c->stream>>>(c->s, c->volume, c->R, c->part_res);
+    k_step_end<<<1, REDUCE_BLOCK, 0, c->stream>>>(c->part_res, c->nblk, c->sum_volume, 0, c->st);
+    CU(cudaGetLastError());
+    TRY(read_state(c));
+    TRY(check_error(c));
+    *time = t;
+    if (residual)
+        for (int v = 0; v < 5; v++) residual[v] = c->st_host->residual[v];
+    if (step0) *step0 = c->st_host->step0;
+    return TG_OK;
+}
+
+// ---- profiling ---------------------------------------------------------------------------------
+
+extern "C" int tg_profile(tg_ctx *c, int enable)
+{
+    if (!c) return fail(TG_ERR_INVALID, "null context");
+    CU(cudaStreamSynchronize(c->stream));
+    for (auto &p : c->prof_open) {
+        c->prof_pool.push_back(p.second.first);
+        c->prof_pool.push_back(p.second.second);
+    }
+    c->prof_open.clear();
+    for (int i = 0; i < TG_PROF_CATEGORIES; i++) {
+        c->prof_ms[i] = 0;
+        c->prof_n[i] = 0;
+    }
+    c->prof_on = enable != 0;
+    return TG_OK;
+}
+
+extern "C" int tg_profile_read(tg_ctx *c, double *ms, long *launches)
+{
+    if (!c) return fail(TG_ERR_INVALID, "null context");
+    CU(cudaStreamSynchronize(c->stream));
+    for (auto &p : c->prof_open) {
+        float t = 0;
+        CU(cudaEventElapsedTime(&t, p.second.first, p.second.second));
+        c->prof_ms[p.first] += t;
+        c->prof_n[p.first] += 1;
+        c->prof_pool.push_back(p.second.first);
+        c->prof_pool.push_back(p.second.second);
+    }
+    c->prof_open.clear();
+    for (int i = 0; i < TG_PROF_CATEGORIES; i++) {
+        if (ms) ms[i] = c->prof_ms[i];
+        if (launches) launches[i] = c->prof_n[i];
+    }
+    return TG_OK;
+}
+
+extern "C" int tg_launch_count(tg_ctx *c, long *count)
+{
+    if (!c || !count) return fail(TG_ERR_INVALID, "null argument");
+    *count = c->launches;
+    return TG_OK;
+}
+
+// ---- layout introspection --------------------------------------------------------------------
+
+extern "C" int tg_layout(tg_ctx *c, const char *name, void *out, long count)
+{
+    if (!c || !name || !out) return fail(TG_ERR_INVALID, "null argument");
+    const void *src = nullptr;
+    size_t bytes = 0;
+    long expect = 0;
+    if (!strcmp(name, "face_lr")) {
+        src = c->lr, expect = 2L * c->s.F, bytes = sizeof(int);
+    }
+    else if (!strcmp(name, "slot_face")) {
+        src = c->slot_face, expect = (long)MAX_SLOTS * c->s.C, bytes = sizeof(int);
+    }
+    else if (!strcmp(name, "slot_nbr")) {
+        src = c->slot_nbr, expect = (long)MAX_SLOTS * c->s.C, bytes = sizeof(int);
+    }
+    else if (!strcmp(name, "slot_cnt")) {
+        src = c->slot_cnt, expect = c->s.C, bytes = 1;
+    }
+    else if (!strcmp(name, "owner")) {
+        src = c->owner, expect = c->num_periodic, bytes = sizeof(int);
+    }
+    else {
+        return fail(TG_ERR_INVALID, "unknown layout array (%s)", name);
+    }
+    if (count != expect) return fail(TG_ERR_INVALID, "layout array %s has %ld elements, not %ld", name, expect, count);
+    if (count == 0) return TG_OK;
+    CU(cudaMemcpyAsync(out, src, bytes * count, cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    return TG_OK;
+}
+
+// ---- drop-in Advance methods ------------------------------------------------------------------
+
+struct Binding {
+    tg_ctx *ctx;
+    double *host_primitive;
+};
+static std::map<const void *, Binding> g_bindings;
+static std::mutex g_bind_mutex;
+
+extern "C" int tg_bind(const void *eqns, tg_ctx *c, double *host_primitive)
+{
+    if (!eqns || !c || !host_primitive) return fail(TG_ERR_INVALID, "null argument");
+    TRY(tg_set_primitive(c, host_primitive));
+    std::lock_guard<std::mutex> lock(g_bind_mutex);
+    g_bindings[eqns] = Binding{c, host_primitive};
+    return TG_OK;
+}
+
+extern "C" int tg_unbind(const void *eqns)
+{
+    std::lock_guard<std::mutex> lock(g_bind_mutex);
+    g_bindings.erase(eqns);
+    return TG_OK;
+}
+
+static double dropin(int method, const void *eqns, double *time, void *residual, double max_step,
+                     double courant, const void *context)
+{
+    Binding b{nullptr, nullptr};
+    {
+        std::lock_guard<std::mutex> lock(g_bind_mutex);
+        auto it = g_bindings.find(eqns);
+        if (it != g_bindings.end()) b = it->second;
+    }
+    double step0 = 0;
+    int rc = b.ctx ? TG_OK : fail(TG_ERR_INVALID, "equations are not bound to a device context");
+    if (rc == TG_OK) rc = tg_advance(b.ctx, method, context, courant, time, max_step, (double *)residual, &step0);
+    if (rc == TG_OK) rc = tg_get_primitive(b.ctx, b.host_primitive);
+    if (rc != TG_OK) {
+        fprintf(stderr, "[0] ERROR: %s\n", tg_last_error());
+        fflush(stderr);
+        exit(EXIT_FAILURE);
+    }
+    return step0;
+}
+
+extern "C" double tg_teal_euler(const void *eqns, double *time, void *residual, double max_step,
+                                double courant, const void *context)
+{
+    return dropin(TG_ADVANCE_EULER, eqns, time, residual, max_step, courant, context);
+}
+
+extern "C" double tg_teal_lserk(const void *eqns, double *time, void *residual, double max_step,
+                                double courant, const void *context)
+{
+    return dropin(TG_ADVANCE_LSERK, eqns, time, residual, max_step, courant, context);
+}
+
+extern "C" double tg_teal_implicit_euler(const void *eqns, double *time, void *residual, double max_step,
+                                         double courant, const void *context)
+{
+    return dropin(TG_ADVANCE_IMPLICIT_EULER, eqns, time, residual, max_step, courant, context);
+}

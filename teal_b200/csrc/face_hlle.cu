@@ -1,0 +1,6 @@
+// Face-flux kernel variants for the hlle convective flux (see kernels.cuh k_face).
+#include "launch.cuh"
+
+namespace tg {
+TG_INSTANTIATE_FACE(FK_HLLE)
+}  // namespace tg

@@ -1,0 +1,531 @@
+// Kernels of the residual / time-integration path. One thread per cell or per face; every sum over
+// a cell's faces runs through that cell's slot list in face order, so results are deterministic
+// and need no floating-point atomics.
+#pragma once
+
+#include "common.cuh"
+
+namespace tg {
+
+// ---- boundary pass (src/equations/boundary.c:5-43) -------------------------------------------
+
+__global__ void k_boundary(Sizes s, const int2 *__restrict__ lr, const double *__restrict__ basis,
+                           const int *__restrict__ bface_ent, BoundaryTable bt, double *q,
+                           double gamma)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int f = s.F_in + i;
+    if (f >= s.F_bd) {
+        return;
+    }
+    int2 c = lr[f];
+    int e = bface_ent[i];
+    Prim<double> in = load_prim<double>(q, s.N, c.x);
+    Basis<double> b = load_basis(basis, s.F, f);
+    Prim<double> ctx = prim_from(bt.ctx[e]);
+    Prim<double> out = boundary_state(bt.kind[e], in, ctx, gamma, b);
+    store_prim(q, s.N, c.y, out);
+}
+
+// ---- least-squares gradient + limiter (src/equations/gradient.c:7-58, limiter.c:23-113) -------
+//
+// FOLD: store the limited gradient (Euler: only the limited one is used); otherwise store the
+// unlimited gradient and the limiter factors psi (Navier–Stokes: the viscous flux needs both).
+template <typename R, int LIM, bool FOLD>
+__global__ void __launch_bounds__(BLOCK) k_gradient(Sizes s, Geometry<R> g,
+                                                    const double *__restrict__ eps2,
+                                                    const double *__restrict__ q, R *__restrict__ grad,
+                                                    R *__restrict__ psi_out)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= s.C) {
+        return;
+    }
+    const int C = s.C, N = s.N;
+    double qc[5];
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        qc[v] = __ldg(q + v * N + c);
+    }
+    R gr[15];
+#pragma unroll
+    for (int k = 0; k < 15; k++) {
+        gr[k] = R(0);
+    }
+    double mn[5], mx[5];
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        mn[v] = mx[v] = qc[v];
+    }
+    int cnt = g.slot_cnt[c];
+    for (int j = 0; j < cnt; j++) {
+        int n = __ldg(g.slot_nbr + j * C + c);
+        R wx = __ldg(g.slot_w + (0 * MAX_SLOTS + j) * C + c);
+        R wy = __ldg(g.slot_w + (1 * MAX_SLOTS + j) * C + c);
+        R wz = __ldg(g.slot_w + (2 * MAX_SLOTS + j) * C + c);
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+            double qn = __ldg(q + v * N + n);
+            R d = R(qn - qc[v]);
+            gr[3 * v + 0] += d * wx;
+            gr[3 * v + 1] += d * wy;
+            gr[3 * v + 2] += d * wz;
+            if (LIM != 0) {
+                mn[v] = fmin(mn[v], qn);
+                mx[v] = fmax(mx[v], qn);
+            }
+        }
+    }
+
+    R psi[5] = {R(1), R(1), R(1), R(1), R(1)};
+    if (LIM != 0) {
+        R e2 = (LIM == 2) ? R(__ldg(eps2 + c)) : R(0);
+        for (int j = 0; j < cnt; j++) {
+            R ox = __ldg(g.slot_off + (0 * MAX_SLOTS + j) * C + c);
+            R oy = __ldg(g.slot_off + (1 * MAX_SLOTS + j) * C + c);
+            R oz = __ldg(g.slot_off + (2 * MAX_SLOTS + j) * C + c);
+#pragma unroll
+            for (int v = 0; v < 5; v++) {
+                R d2 = ((gr[3 * v] * ox) + (gr[3 * v + 1] * oy)) + (gr[3 * v + 2] * oz);
+                if (is_close_zero(d2)) {
+                    continue;
+                }
+                R d1 = R(((d2 > R(0)) ? mx[v] : mn[v]) - qc[v]);
+                if (LIM == 1) {  // Barth–Jespersen (limiter.c:54-58)
+                    psi[v] = fmin(psi[v], fmin(R(1), d1 / d2));
+                }
+                else {  // Venkatakrishnan (limiter.c:100-106)
+                    R top = (((d1 * d1) + e2) * d2) + ((R(2) * (d2 * d2)) * d1);
+                    R bot = (((d1 * d1) + (R(2) * (d2 * d2))) + (d1 * d2)) + e2;
+                    psi[v] = fmin(psi[v], (top / bot) / d2);
+                }
+            }
+        }
+    }
+
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            R val = gr[3 * v + d];
+            if (FOLD && LIM != 0) {
+                val *= psi[v];
+            }
+            grad[(3 * v + d) * C + c] = val;
+        }
+        if (!FOLD) {
+            psi_out[v * C + c] = psi[v];
+        }
+    }
+}
+
+// per-cell time step of the equations' Timestep plugin
+template <bool NS>
+__device__ __forceinline__ double cell_timestep(const Prim<double> &p, const double *prop,
+                                                const CellData &cd, int C, int c)
+{
+    double vol = __ldg(cd.volume + c);
+    V3<double> proj = load_v3(cd.projection, C, c);
+    if (NS) {
+        return navierstokes_timestep(p, prop[0], prop[1], prop[2], vol, proj);
+    }
+    return euler_timestep(p, prop[0], vol, proj);
+}
+
+struct Props {
+    double v[3];
+};
+
+// ---- cell gather, finalize and stage update (derivative.c:229-267, advance.c:96-108) ---------
+//
+// MODE 0: R = -sum / V (equations_derivative); MODE 1: one low-storage RK stage
+// U = U0 + R * alpha * step, q = prim(U). With `last`, also: R kept, U0 <- cons(q) for the next
+// step, per-block minimum time step and per-block volume-weighted sums of R^2.
+template <int MODE, bool NS, typename GT>
+__global__ void __launch_bounds__(BLOCK) k_cell(Sizes s, const int *__restrict__ slot_face,
+                                                const uint8_t *__restrict__ slot_cnt, CellData cd,
+                                                const GT *__restrict__ G, double *__restrict__ U0,
+                                                double *__restrict__ q, double *__restrict__ Rout,
+                                                const StepState *__restrict__ st, double alpha,
+                                                int last, Props prop, double *__restrict__ part_dt,
+                                                double *__restrict__ part_res)
+{
+    __shared__ double sh[BLOCK / 32];
+    const int C = s.C, F = s.F, N = s.N;
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    bool active = c < C;
+    double r[5] = {0, 0, 0, 0, 0};
+    double vol = 1;
+    if (active) {
+        double acc[5] = {0, 0, 0, 0, 0};
+        int cnt = slot_cnt[c];
+        for (int j = 0; j < cnt; j++) {
+            int sf = __ldg(slot_face + j * C + c);
+            if (sf >= 0) {
+#pragma unroll
+                for (int v = 0; v < 5; v++) {
+                    acc[v] += double(__ldg(G + v * F + sf));
+                }
+            }
+            else {
+                int f = ~sf;
+#pragma unroll
+                for (int v = 0; v < 5; v++) {
+                    acc[v] -= double(__ldg(G + v * F + f));
+                }
+            }
+        }
+        vol = __ldg(cd.volume + c);
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+            r[v] = -acc[v] / vol;
+        }
+    }
+    if (MODE == 0) {
+        if (active) {
+#pragma unroll
+            for (int v = 0; v < 5; v++) {
+                Rout[v * C + c] = r[v];
+            }
+        }
+        return;
+    }
+
+    double step = st->step;
+    double dt_cell = DBL_MAX;
+    if (active) {
+        Cons<double> u;
+        u.rho = __ldg(U0 + c) + ((r[0] * alpha) * step);
+        u.m.x = __ldg(U0 + C + c) + ((r[1] * alpha) * step);
+        u.m.y = __ldg(U0 + 2 * C + c) + ((r[2] * alpha) * step);
+        u.m.z = __ldg(U0 + 3 * C + c) + ((r[3] * alpha) * step);
+        u.e = __ldg(U0 + 4 * C + c) + ((r[4] * alpha) * step);
+        Prim<double> p = cons_to_prim(u, prop.v[0]);
+        store_prim(q, N, c, p);
+        if (last) {
+#pragma unroll
+            for (int v = 0; v < 5; v++) {
+                Rout[v * C + c] = r[v];
+            }
+            Cons<double> u0 = prim_to_cons(p, prop.v[0]);
+            U0[c] = u0.rho;
+            U0[C + c] = u0.m.x;
+            U0[2 * C + c] = u0.m.y;
+            U0[3 * C + c] = u0.m.z;
+            U0[4 * C + c] = u0.e;
+            dt_cell = cell_timestep<NS>(p, prop.v, cd, C, c);
+        }
+    }
+    if (last) {
+        double m = block_min<BLOCK>(dt_cell, sh);
+        if (threadIdx.x == 0) {
+            part_dt[blockIdx.x] = m;
+        }
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+            double t = active ? vol * (r[v] * r[v]) : 0.0;
+            double sum = block_sum<BLOCK>(t, sh);
+            if (threadIdx.x == 0) {
+                part_res[v * gridDim.x + blockIdx.x] = sum;
+            }
+        }
+    }
+}
+
+// U0 = cons(q) and per-block minimum time step of the current state (start of a run / after the
+// host changed the state)
+template <bool NS>
+__global__ void __launch_bounds__(BLOCK) k_prepare(Sizes s, CellData cd, const double *__restrict__ q,
+                                                   double *__restrict__ U0, Props prop,
+                                                   double *__restrict__ part_dt)
+{
+    __shared__ double sh[BLOCK / 32];
+    const int C = s.C;
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    double dt_cell = DBL_MAX;
+    if (c < C) {
+        Prim<double> p = load_prim<double>(q, s.N, c);
+        Cons<double> u0 = prim_to_cons(p, prop.v[0]);
+        U0[c] = u0.rho;
+        U0[C + c] = u0.m.x;
+        U0[2 * C + c] = u0.m.y;
+        U0[3 * C + c] = u0.m.z;
+        U0[4 * C + c] = u0.e;
+        dt_cell = cell_timestep<NS>(p, prop.v, cd, C, c);
+    }
+    double m = block_min<BLOCK>(dt_cell, sh);
+    if (threadIdx.x == 0) {
+        part_dt[blockIdx.x] = m;
+    }
+}
+
+// per-block sums of V * R^2 of a derivative (equations_residual, residual.c:8-33)
+__global__ void __launch_bounds__(BLOCK) k_residual_part(Sizes s, const double *__restrict__ volume,
+                                                         const double *__restrict__ Rin,
+                                                         double *__restrict__ part_res)
+{
+    __shared__ double sh[BLOCK / 32];
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    bool active = c < s.C;
+    double vol = active ? volume[c] : 0.0;
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        double r = active ? Rin[v * s.C + c] : 0.0;
+        double sum = block_sum<BLOCK>(active ? vol * (r * r) : 0.0, sh);
+        if (threadIdx.x == 0) {
+            part_res[v * gridDim.x + blockIdx.x] = sum;
+        }
+    }
+}
+
+// start of a step: step0 = courant * min(partials), step = min(step0, max step)
+__global__ void __launch_bounds__(REDUCE_BLOCK) k_step_begin(const double *__restrict__ part_dt,
+                                                             int nparts, double courant, StepState *st)
+{
+    __shared__ double sh[REDUCE_BLOCK / 32];
+    double m = DBL_MAX;
+    for (int i = threadIdx.x; i < nparts; i += REDUCE_BLOCK) {
+        m = fmin(m, part_dt[i]);
+    }
+    m = block_min<REDUCE_BLOCK>(m, sh);
+    if (threadIdx.x == 0) {
+        double step0 = courant * m;
+        double max_step = st->use_max_time ? (st->max_time - st->time) : st->max_step;
+        st->step0 = step0;
+        st->step = fmin(step0, max_step);
+        if (!isfinite(step0) || !(step0 > 0)) {
+            st->error = 1;
+        }
+    }
+}
+
+// end of a step: time += step, residual = sqrt(sum / sum_volume)
+__global__ void __launch_bounds__(REDUCE_BLOCK) k_step_end(const double *__restrict__ part_res,
+                                                           int nparts, double sum_volume, int advance,
+                                                           StepState *st)
+{
+    __shared__ double sh[REDUCE_BLOCK / 32];
+    for (int v = 0; v < 5; v++) {
+        double t = 0;
+        // fixed-order strided partial sums, then a fixed tree
+        for (int i = threadIdx.x; i < nparts; i += REDUCE_BLOCK) {
+            t += part_res[v * nparts + i];
+        }
+        double sum = block_sum<REDUCE_BLOCK>(t, sh);
+        if (threadIdx.x == 0) {
+            double res = sqrt(sum / sum_volume);
+            st->residual[v] = res;
+            if (!isfinite(res)) {
+                st->error = 1;
+            }
+        }
+    }
+    if (threadIdx.x == 0 && advance) {
+        st->time += st->step;
+    }
+}
+
+// ---- device mesh upload: per-cell slot lists (integer work, checked against a host recompute) --
+
+// count faces per inner cell
+__global__ void k_slot_count(int F, int F_in, const int2 *__restrict__ lr, int *__restrict__ cnt)
+{
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= F) {
+        return;
+    }
+    int2 c = lr[f];
+    atomicAdd(cnt + c.x, 1);
+    if (f < F_in) {
+        atomicAdd(cnt + c.y, 1);
+    }
+}
+
+// scatter face references into the ELL slots (arbitrary order; sorted afterwards)
+__global__ void k_slot_fill(int F, int F_in, int C, const int2 *__restrict__ lr, int *__restrict__ cursor,
+                            int *__restrict__ slot_face)
+{
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= F) {
+        return;
+    }
+    int2 c = lr[f];
+    int j = atomicAdd(cursor + c.x, 1);
+    if (j < MAX_SLOTS) {
+        slot_face[j * C + c.x] = f;
+    }
+    if (f < F_in) {
+        int k = atomicAdd(cursor + c.y, 1);
+        if (k < MAX_SLOTS) {
+            slot_face[k * C + c.y] = ~f;
+        }
+    }
+}
+
+__device__ __forceinline__ int face_of(int sf)
+{
+    return sf >= 0 ? sf : ~sf;
+}
+
+// sort each cell's slots by face index, then fill neighbour, weight and offset of each slot
+template <typename G>
+__global__ void k_slot_finish(int C, const int2 *__restrict__ lr, const int *__restrict__ cnt_in,
+                              const double *__restrict__ weight_aos, const double *__restrict__ offset_aos,
+                              int *__restrict__ slot_face, int *__restrict__ slot_nbr,
+                              uint8_t *__restrict__ slot_cnt, G *__restrict__ slot_w,
+                              G *__restrict__ slot_off, int *__restrict__ error)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= C) {
+        return;
+    }
+    int cnt = cnt_in[c];
+    if (cnt > MAX_SLOTS || cnt < 1) {
+        atomicExch(error, 1);
+        cnt = cnt > MAX_SLOTS ? MAX_SLOTS : cnt;
+    }
+    int sf[MAX_SLOTS];
+    for (int j = 0; j < cnt; j++) {
+        sf[j] = slot_face[j * C + c];
+    }
+    for (int i = 1; i < cnt; i++) {  // insertion sort by face index
+        int key = sf[i];
+        int j = i - 1;
+        while (j >= 0 && face_of(sf[j]) > face_of(key)) {
+            sf[j + 1] = sf[j];
+            j -= 1;
+        }
+        sf[j + 1] = key;
+    }
+    slot_cnt[c] = (uint8_t)cnt;
+    for (int j = 0; j < MAX_SLOTS; j++) {
+        if (j < cnt) {
+            int f = face_of(sf[j]);
+            int side = sf[j] >= 0 ? 0 : 1;
+            int2 p = lr[f];
+            slot_face[j * C + c] = sf[j];
+            slot_nbr[j * C + c] = side == 0 ? p.y : p.x;
+            for (int d = 0; d < 3; d++) {
+                slot_w[(d * MAX_SLOTS + j) * C + c] = G(weight_aos[(size_t)f * 6 + side * 3 + d]);
+                slot_off[(d * MAX_SLOTS + j) * C + c] = G(offset_aos[(size_t)f * 6 + side * 3 + d]);
+            }
+        }
+        else {  // padding: a self-reference with zero weight and offset
+            slot_face[j * C + c] = 0;
+            slot_nbr[j * C + c] = c;
+            for (int d = 0; d < 3; d++) {
+                slot_w[(d * MAX_SLOTS + j) * C + c] = G(0);
+                slot_off[(d * MAX_SLOTS + j) * C + c] = G(0);
+            }
+        }
+    }
+}
+
+// AoS [n][k] -> SoA [k][n] with an element type change
+template <typename T>
+__global__ void k_transpose(int n, int k, const double *__restrict__ aos, T *__restrict__ soa)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+    for (int j = 0; j < k; j++) {
+        soa[(size_t)j * n + i] = T(aos[(size_t)i * k + j]);
+    }
+}
+
+// periodic faces: redirect the ghost right cell to its owner
+__global__ void k_redirect(int F, int F_bd, int off_periodic_ghost, const int *__restrict__ face_cell,
+                           const int *__restrict__ owner, int num_owner, int2 *__restrict__ lr,
+                           int *__restrict__ error)
+{
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= F) {
+        return;
+    }
+    int l = face_cell[2 * f], r = face_cell[2 * f + 1];
+    if (f >= F_bd) {
+        int g = r - off_periodic_ghost;
+        if (g < 0 || g >= num_owner) {
+            atomicExch(error, 2);
+            r = l;
+        }
+        else {
+            r = owner[g];
+        }
+    }
+    lr[f] = make_int2(l, r);
+}
+
+// SoA state rows <-> teal's AoS [cells][5]
+__global__ void k_prim_aos_to_soa(int n, int N, const double *__restrict__ aos, double *__restrict__ q)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        q[v * N + i] = aos[(size_t)i * 5 + v];
+    }
+}
+
+// rows [0, n): direct; rows of periodic ghosts: copied from the owner
+__global__ void k_prim_soa_to_aos(int n_direct, int n_total, int N, const int *__restrict__ owner,
+                                  const double *__restrict__ q, double *__restrict__ aos)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_total) {
+        return;
+    }
+    int src = i < n_direct ? i : owner[i - n_direct];
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        aos[(size_t)i * 5 + v] = q[v * N + src];
+    }
+}
+
+// SoA [5][C] -> AoS [C][5] (derivative) and back
+__global__ void k_soa5_to_aos(int C, const double *__restrict__ soa, double *__restrict__ aos)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= C) {
+        return;
+    }
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        aos[(size_t)i * 5 + v] = soa[v * C + i];
+    }
+}
+
+__global__ void k_aos5_to_soa(int C, const double *__restrict__ aos, double *__restrict__ soa)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= C) {
+        return;
+    }
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        soa[v * C + i] = aos[(size_t)i * 5 + v];
+    }
+}
+
+// gradient [15][C] -> teal's [C][5][3] (limited if psi given)
+template <typename R>
+__global__ void k_grad_to_aos(int C, const R *__restrict__ grad, const R *__restrict__ psi,
+                              double *__restrict__ aos)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= C) {
+        return;
+    }
+    for (int k = 0; k < 15; k++) {
+        R g = grad[k * C + i];
+        if (psi) {
+            g *= psi[(k / 3) * C + i];
+        }
+        aos[(size_t)i * 15 + k] = double(g);
+    }
+}
+
+}  // namespace tg
