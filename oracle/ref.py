@@ -180,6 +180,7 @@ class RefEquations:
         lib().ref_set_viscous(self.ptr, (name or "").encode())
 
     def set_limiter(self, name, coefficient=0.0):
+        self.limiter = name
         lib().ref_set_limiter(self.ptr, (name or "").encode(), coefficient)
 
     def set_property(self, name, value):
@@ -218,7 +219,7 @@ class RefEquations:
         lib().ref_boundary(self.ptr, _d(work), time)
         grad = np.zeros((self.num_cells, 5, 3))
         lib().ref_gradient(self.ptr, _d(work), _d(grad))
-        if limited:
+        if limited and getattr(self, "limiter", "minmod"):  # teal's limiter pass needs a limiter kind
             lib().ref_limiter(self.ptr, _d(work), _d(grad))
         return grad
 

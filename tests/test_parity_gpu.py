@@ -194,10 +194,15 @@ def test_implicit_euler_newton_gmres():
     prim = np.tile(np.array(FREE), (dm.num_cells, 1))
     rng = np.random.default_rng(4)
     prim[:, 0] *= 1 + 0.05 * rng.random(dm.num_cells)
-    (tr, sr, rr, pr), (td, sd, rd, pd) = run_both(re, de, prim, "implicit euler", 20.0, 2, nk=(0.1, 0.3, 10))
-    assert abs(td - tr) <= 1e-12 * tr
+    # step 1 starts from the same state: same CFL step
+    (tr, sr, rr, pr), (td, sd, rd, pd) = run_both(re, de, prim, "implicit euler", 20.0, 1, nk=(0.1, 0.3, 10))
+    assert abs(td - tr) <= 1e-13 * tr
     assert rel_l2(pd, pr).max() <= 1e-6
     assert np.allclose(rd, rr, rtol=1e-5)
+    # two steps: the second step size follows the (1e-7-close) state of the first
+    (tr, sr, rr, pr), (td, sd, rd, pd) = run_both(re, de, prim, "implicit euler", 20.0, 2, nk=(0.1, 0.3, 10))
+    assert abs(td - tr) <= 1e-6 * tr
+    assert rel_l2(pd, pr).max() <= 1e-6
 
 
 def test_run_matches_repeated_advance():
