@@ -62,6 +62,44 @@ __device__ __forceinline__ Prim<R> prim_from(const R *a)
     return Prim<R>{a[0], v3(a[1], a[2], a[3]), a[4]};
 }
 
+// Re-read of a value another part of the kernel already loaded: a volatile read-only load, so the
+// compiler neither merges it with the first load nor keeps the first value live in a register
+// across the code in between (the line is still in L1)
+__device__ __forceinline__ double reload(const double *p)
+{
+    double v;
+    asm volatile("ld.global.nc.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ float reload(const float *p)
+{
+    float v;
+    asm volatile("ld.global.nc.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
+}
+
+template <typename R>
+__device__ __forceinline__ Basis<R> reload_basis(const R *__restrict__ b, int ld, int f)
+{
+    Basis<R> m;
+    m.x = v3(reload(b + f), reload(b + ld + f), reload(b + 2 * ld + f));
+    m.y = v3(reload(b + 3 * ld + f), reload(b + 4 * ld + f), reload(b + 5 * ld + f));
+    m.z = v3(reload(b + 6 * ld + f), reload(b + 7 * ld + f), reload(b + 8 * ld + f));
+    return m;
+}
+
+template <typename R>
+__device__ __forceinline__ Prim<R> reload_prim(const double *__restrict__ q, int ld, int i)
+{
+    Prim<R> p;
+    p.rho = R(reload(q + i));
+    p.u.x = R(reload(q + ld + i));
+    p.u.y = R(reload(q + 2 * ld + i));
+    p.u.z = R(reload(q + 3 * ld + i));
+    p.p = R(reload(q + 4 * ld + i));
+    return p;
+}
+
 // is_close(x, 0) of src/core/utils.c:29-34 (absolute 1e-8, relative 1e-5)
 template <typename R>
 __device__ __forceinline__ bool is_close_zero(R x)

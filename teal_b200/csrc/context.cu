@@ -765,24 +765,24 @@ static int run_boundary(tg_ctx *c, double *q)
 template <typename R>
 static void launch_gradient(tg_ctx *c, const Geometry<R> &g, bool fold, const double *q)
 {
-    dim3 grid(grid_of(c->s.C));
+    dim3 grid((c->s.C + GRAD_CELLS - 1) / GRAD_CELLS);
     R *grad = (R *)c->grad;
     R *psi = (R *)c->psi;
     switch (c->limiter) {
         case TG_LIMITER_NONE:
-            k_gradient<R, 0, true><<<grid, BLOCK, 0, c->stream>>>(c->s, g, c->eps2, q, grad, psi);
+            k_gradient<R, 0, true><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, grad, psi);
             break;
         case TG_LIMITER_BARTH_JESPERSEN:
             if (fold)
-                k_gradient<R, 1, true><<<grid, BLOCK, 0, c->stream>>>(c->s, g, c->eps2, q, grad, psi);
+                k_gradient<R, 1, true><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, grad, psi);
             else
-                k_gradient<R, 1, false><<<grid, BLOCK, 0, c->stream>>>(c->s, g, c->eps2, q, grad, psi);
+                k_gradient<R, 1, false><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, grad, psi);
             break;
         default:
             if (fold)
-                k_gradient<R, 2, true><<<grid, BLOCK, 0, c->stream>>>(c->s, g, c->eps2, q, grad, psi);
+                k_gradient<R, 2, true><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, grad, psi);
             else
-                k_gradient<R, 2, false><<<grid, BLOCK, 0, c->stream>>>(c->s, g, c->eps2, q, grad, psi);
+                k_gradient<R, 2, false><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, grad, psi);
             break;
     }
 }

@@ -9,19 +9,32 @@ namespace tg {
 //
 // Writes G[v][f] = (convective - viscous) flux * area; the cell gather adds G to the left cell and
 // subtracts it from the right one, as teal's face loops do.
-template <typename R>
-__device__ __forceinline__ void load_grad(const R *__restrict__ grad, int C, int c, R (&g)[15])
+// Reconstructed face state of one side: q + (psi * grad) . offset per variable, streamed one
+// variable at a time so only the result stays live (derivative.c:158-164)
+template <typename R, bool FOLD>
+__device__ __forceinline__ void reconstruct(const Prim<R> &q, const R *__restrict__ grad,
+                                            const R *__restrict__ psi, int C, int c, V3<R> off, R (&out)[5])
 {
+    R qv[5] = {q.rho, q.u.x, q.u.y, q.u.z, q.p};
 #pragma unroll
-    for (int k = 0; k < 15; k++) {
-        g[k] = __ldg(grad + k * C + c);
+    for (int v = 0; v < 5; v++) {
+        V3<R> gv = v3(__ldg(grad + (3 * v) * C + c), __ldg(grad + (3 * v + 1) * C + c),
+                      __ldg(grad + (3 * v + 2) * C + c));
+        if (!FOLD) {
+            R ps = __ldg(psi + v * C + c);
+            gv = v3(gv.x * ps, gv.y * ps, gv.z * ps);
+        }
+        out[v] = qv[v] + dot(gv, off);
     }
 }
 
+// One thread per face. The convective flux comes first (its reconstruction streams the limited
+// gradients), the viscous flux second (its face-averaged gradient re-reads the unlimited gradients,
+// which are still in L1); the register cap keeps 16 warps per SM resident.
 template <typename R, int FK, bool NS, int ORDER, bool FOLD>
-__global__ void __launch_bounds__(BLOCK) k_face(Sizes s, Geometry<R> g, const double *__restrict__ q,
-                                                const R *__restrict__ grad, const R *__restrict__ psi,
-                                                R gamma, R mu, R prandtl, R *__restrict__ G)
+__global__ void __launch_bounds__(BLOCK, 2) k_face(Sizes s, Geometry<R> g, const double *__restrict__ q,
+                                                   const R *__restrict__ grad, const R *__restrict__ psi,
+                                                   R gamma, R mu, R prandtl, R *__restrict__ G)
 {
     int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= s.F) {
@@ -30,110 +43,84 @@ __global__ void __launch_bounds__(BLOCK) k_face(Sizes s, Geometry<R> g, const do
     const int F = s.F, C = s.C, N = s.N;
     const bool boundary = (f >= s.F_in) && (f < s.F_bd);
     int2 c = g.lr[f];
-    Prim<R> ql = load_prim<R>(q, N, c.x);
-    Prim<R> qr = load_prim<R>(q, N, c.y);
-    Basis<R> b = load_basis(g.basis, F, f);
-    R area = __ldg(g.area + f);
 
-    Cons<R> fv{R(0), v3(R(0), R(0), R(0)), R(0)};
+    // convective flux: the basis and the cell states are dead while the flux runs in the face frame
+    // and are re-read afterwards
     Cons<R> fc{R(0), v3(R(0), R(0), R(0)), R(0)};
-
-    if (ORDER == 1) {
-        if (FK != FK_NONE) {
-            fc = convective_flux<FK>(ql, qr, gamma, b);
-        }
-    }
-    else {
-        R gl[15], gr[15];
-        load_grad(grad, C, c.x, gl);
-        if (!boundary) {
-            load_grad(grad, C, c.y, gr);
-        }
-        if (NS) {
-            // face average corrected along the centre-to-centre direction (derivative.c:71-89)
-            R qlv[5] = {ql.rho, ql.u.x, ql.u.y, ql.u.z, ql.p};
-            R qrv[5] = {qr.rho, qr.u.x, qr.u.y, qr.u.z, qr.p};
-            R qm[5], gm[15];
-#pragma unroll
-            for (int v = 0; v < 5; v++) {
-                qm[v] = (qlv[v] + qrv[v]) / R(2);
-            }
-#pragma unroll
-            for (int k = 0; k < 15; k++) {
-                gm[k] = boundary ? gl[k] : (gl[k] + gr[k]) / R(2);
-            }
-            V3<R> unit = load_v3(g.corr, F, f);
-            R norm = __ldg(g.corr + 3 * F + f);
-#pragma unroll
-            for (int v = 0; v < 5; v++) {
-                V3<R> gv = v3(gm[3 * v], gm[3 * v + 1], gm[3 * v + 2]);
-                R adjust = dot(gv, unit) - ((qrv[v] - qlv[v]) / norm);
-                gv = sub(gv, mul(adjust, unit));
-                gm[3 * v] = gv.x;
-                gm[3 * v + 1] = gv.y;
-                gm[3 * v + 2] = gv.z;
-            }
-            Grad<R> gg;
-            gg.rho = v3(gm[0], gm[1], gm[2]);
-            gg.ux = v3(gm[3], gm[4], gm[5]);
-            gg.uy = v3(gm[6], gm[7], gm[8]);
-            gg.uz = v3(gm[9], gm[10], gm[11]);
-            gg.p = v3(gm[12], gm[13], gm[14]);
-            fv = viscous_central(prim_from(qm), gg, gamma, mu, prandtl, b);
-        }
-        if (FK != FK_NONE) {
-            // reconstruct with the limited gradient (derivative.c:158-164, :191-224)
-            V3<R> ol = load_v3(g.offl, F, f);
-            R pl[5], pr[5];
-            R ps[5];
-            if (!FOLD) {
-#pragma unroll
-                for (int v = 0; v < 5; v++) {
-                    ps[v] = __ldg(psi + v * C + c.x);
-                }
-            }
-            R qlv[5] = {ql.rho, ql.u.x, ql.u.y, ql.u.z, ql.p};
-#pragma unroll
-            for (int v = 0; v < 5; v++) {
-                V3<R> gv = v3(gl[3 * v], gl[3 * v + 1], gl[3 * v + 2]);
-                if (!FOLD) {
-                    gv = v3(gv.x * ps[v], gv.y * ps[v], gv.z * ps[v]);
-                }
-                pl[v] = qlv[v] + dot(gv, ol);
-            }
-            R qrv[5] = {qr.rho, qr.u.x, qr.u.y, qr.u.z, qr.p};
-            if (boundary) {
-#pragma unroll
-                for (int v = 0; v < 5; v++) {
-                    pr[v] = qrv[v];
-                }
+    if (FK != FK_NONE) {
+        Local<R> l, r;
+        {
+            Prim<R> ql = load_prim<R>(q, N, c.x);
+            Prim<R> qr = load_prim<R>(q, N, c.y);
+            Basis<R> b = load_basis(g.basis, F, f);
+            if (ORDER == 1) {
+                l = make_local(ql, gamma, b);
+                r = make_local(qr, gamma, b);
             }
             else {
-                V3<R> orr = load_v3(g.offr, F, f);
-                if (!FOLD) {
-#pragma unroll
-                    for (int v = 0; v < 5; v++) {
-                        ps[v] = __ldg(psi + v * C + c.y);
-                    }
+                R pl[5], pr[5];
+                reconstruct<R, FOLD>(ql, grad, psi, C, c.x, load_v3(g.offl, F, f), pl);
+                if (boundary) {  // the ghost state enters unreconstructed (derivative.c:203-211)
+                    pr[0] = qr.rho, pr[1] = qr.u.x, pr[2] = qr.u.y, pr[3] = qr.u.z, pr[4] = qr.p;
                 }
-#pragma unroll
-                for (int v = 0; v < 5; v++) {
-                    V3<R> gv = v3(gr[3 * v], gr[3 * v + 1], gr[3 * v + 2]);
-                    if (!FOLD) {
-                        gv = v3(gv.x * ps[v], gv.y * ps[v], gv.z * ps[v]);
-                    }
-                    pr[v] = qrv[v] + dot(gv, orr);
+                else {
+                    reconstruct<R, FOLD>(qr, grad, psi, C, c.y, load_v3(g.offr, F, f), pr);
                 }
+                l = make_local(prim_from(pl), gamma, b);
+                r = make_local(prim_from(pr), gamma, b);
             }
-            fc = convective_flux<FK>(prim_from(pl), prim_from(pr), gamma, b);
         }
+        fc = convective_flux_local<FK>(l, r, gamma);
+        fc.m = to_global(reload_basis(g.basis, F, f), fc.m);
     }
+    R area = __ldg(g.area + f);
+    R gf[5] = {fc.rho * area, fc.m.x * area, fc.m.y * area, fc.m.z * area, fc.e * area};
 
-    G[f] = (fc.rho * area) - (fv.rho * area);
-    G[F + f] = (fc.m.x * area) - (fv.m.x * area);
-    G[2 * F + f] = (fc.m.y * area) - (fv.m.y * area);
-    G[3 * F + f] = (fc.m.z * area) - (fv.m.z * area);
-    G[4 * F + f] = (fc.e * area) - (fv.e * area);
+    if (NS && ORDER == 2) {
+        // face average corrected along the centre-to-centre direction (derivative.c:71-89)
+        Prim<R> ql = reload_prim<R>(q, N, c.x);
+        Prim<R> qr = reload_prim<R>(q, N, c.y);
+        Basis<R> b = reload_basis(g.basis, F, f);
+        R qlv[5] = {ql.rho, ql.u.x, ql.u.y, ql.u.z, ql.p};
+        R qrv[5] = {qr.rho, qr.u.x, qr.u.y, qr.u.z, qr.p};
+        R qm[5], gm[15];
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+            qm[v] = (qlv[v] + qrv[v]) / R(2);
+        }
+#pragma unroll
+        for (int k = 0; k < 15; k++) {
+            R a = __ldg(grad + k * C + c.x);
+            gm[k] = boundary ? a : (a + __ldg(grad + k * C + c.y)) / R(2);
+        }
+        V3<R> unit = load_v3(g.corr, F, f);
+        R norm = __ldg(g.corr + 3 * F + f);
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+            V3<R> gv = v3(gm[3 * v], gm[3 * v + 1], gm[3 * v + 2]);
+            R adjust = dot(gv, unit) - ((qrv[v] - qlv[v]) / norm);
+            gv = sub(gv, mul(adjust, unit));
+            gm[3 * v] = gv.x;
+            gm[3 * v + 1] = gv.y;
+            gm[3 * v + 2] = gv.z;
+        }
+        Grad<R> gg;
+        gg.rho = v3(gm[0], gm[1], gm[2]);
+        gg.ux = v3(gm[3], gm[4], gm[5]);
+        gg.uy = v3(gm[6], gm[7], gm[8]);
+        gg.uz = v3(gm[9], gm[10], gm[11]);
+        gg.p = v3(gm[12], gm[13], gm[14]);
+        Cons<R> fv = viscous_central(prim_from(qm), gg, gamma, mu, prandtl, b);
+        gf[0] -= fv.rho * area;
+        gf[1] -= fv.m.x * area;
+        gf[2] -= fv.m.y * area;
+        gf[3] -= fv.m.z * area;
+        gf[4] -= fv.e * area;
+    }
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        G[(size_t)v * F + f] = gf[v];
+    }
 }
 
 }  // namespace tg

@@ -29,93 +29,91 @@ __global__ void k_boundary(Sizes s, const int2 *__restrict__ lr, const double *_
 
 // ---- least-squares gradient + limiter (src/equations/gradient.c:7-58, limiter.c:23-113) -------
 //
+// One thread per (cell, variable): a block of GRAD_WARPS x 32 threads covers 32 consecutive cells,
+// warp w handling variable w, so every warp reads one contiguous row of the state and writes
+// contiguous gradient rows; the per-thread state is one variable's gradient, bounds and factor.
+// Each component is summed over the cell's slots in face order, as teal's face loop adds it.
 // FOLD: store the limited gradient (Euler: only the limited one is used); otherwise store the
-// unlimited gradient and the limiter factors psi (Navier–Stokes: the viscous flux needs both).
+// unlimited gradient and the limiter factors psi (Navier-Stokes: the viscous flux needs both).
+constexpr int GRAD_CELLS = 32;
+constexpr int GRAD_THREADS = 5 * GRAD_CELLS;
+
 template <typename R, int LIM, bool FOLD>
-__global__ void __launch_bounds__(BLOCK) k_gradient(Sizes s, Geometry<R> g,
-                                                    const double *__restrict__ eps2,
-                                                    const double *__restrict__ q, R *__restrict__ grad,
-                                                    R *__restrict__ psi_out)
+__global__ void __launch_bounds__(GRAD_THREADS) k_gradient(Sizes s, Geometry<R> g,
+                                                           const double *__restrict__ eps2,
+                                                           const double *__restrict__ q,
+                                                           R *__restrict__ grad, R *__restrict__ psi_out)
 {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int v = threadIdx.x >> 5;  // variable of this warp
+    const int c = blockIdx.x * GRAD_CELLS + (threadIdx.x & 31);
     if (c >= s.C) {
         return;
     }
-    const int C = s.C, N = s.N;
-    double qc[5];
+    const int C = s.C;
+    const double *qv = q + (size_t)v * s.N;
+    const double qc = __ldg(qv + c);
+    const int cnt = g.slot_cnt[c];
+    int nbr[MAX_SLOTS];
+    double qn[MAX_SLOTS];
 #pragma unroll
-    for (int v = 0; v < 5; v++) {
-        qc[v] = __ldg(q + v * N + c);
+    for (int j = 0; j < MAX_SLOTS; j++) {
+        nbr[j] = (j < cnt) ? __ldg(g.slot_nbr + j * C + c) : c;
     }
-    R gr[15];
 #pragma unroll
-    for (int k = 0; k < 15; k++) {
-        gr[k] = R(0);
+    for (int j = 0; j < MAX_SLOTS; j++) {
+        qn[j] = __ldg(qv + nbr[j]);
     }
-    double mn[5], mx[5];
+    R gx = R(0), gy = R(0), gz = R(0);
+    double mn = qc, mx = qc;
 #pragma unroll
-    for (int v = 0; v < 5; v++) {
-        mn[v] = mx[v] = qc[v];
-    }
-    int cnt = g.slot_cnt[c];
-    for (int j = 0; j < cnt; j++) {
-        int n = __ldg(g.slot_nbr + j * C + c);
-        R wx = __ldg(g.slot_w + (0 * MAX_SLOTS + j) * C + c);
-        R wy = __ldg(g.slot_w + (1 * MAX_SLOTS + j) * C + c);
-        R wz = __ldg(g.slot_w + (2 * MAX_SLOTS + j) * C + c);
-#pragma unroll
-        for (int v = 0; v < 5; v++) {
-            double qn = __ldg(q + v * N + n);
-            R d = R(qn - qc[v]);
-            gr[3 * v + 0] += d * wx;
-            gr[3 * v + 1] += d * wy;
-            gr[3 * v + 2] += d * wz;
-            if (LIM != 0) {
-                mn[v] = fmin(mn[v], qn);
-                mx[v] = fmax(mx[v], qn);
-            }
+    for (int j = 0; j < MAX_SLOTS; j++) {
+        if (j < cnt) {
+            R wx = __ldg(g.slot_w + (0 * MAX_SLOTS + j) * C + c);
+            R wy = __ldg(g.slot_w + (1 * MAX_SLOTS + j) * C + c);
+            R wz = __ldg(g.slot_w + (2 * MAX_SLOTS + j) * C + c);
+            R d = R(qn[j] - qc);
+            gx += d * wx;
+            gy += d * wy;
+            gz += d * wz;
+            mn = fmin(mn, qn[j]);
+            mx = fmax(mx, qn[j]);
         }
     }
 
-    R psi[5] = {R(1), R(1), R(1), R(1), R(1)};
+    R psi = R(1);
     if (LIM != 0) {
         R e2 = (LIM == 2) ? R(__ldg(eps2 + c)) : R(0);
-        for (int j = 0; j < cnt; j++) {
-            R ox = __ldg(g.slot_off + (0 * MAX_SLOTS + j) * C + c);
-            R oy = __ldg(g.slot_off + (1 * MAX_SLOTS + j) * C + c);
-            R oz = __ldg(g.slot_off + (2 * MAX_SLOTS + j) * C + c);
 #pragma unroll
-            for (int v = 0; v < 5; v++) {
-                R d2 = ((gr[3 * v] * ox) + (gr[3 * v + 1] * oy)) + (gr[3 * v + 2] * oz);
-                if (is_close_zero(d2)) {
-                    continue;
-                }
-                R d1 = R(((d2 > R(0)) ? mx[v] : mn[v]) - qc[v]);
-                if (LIM == 1) {  // Barth–Jespersen (limiter.c:54-58)
-                    psi[v] = fmin(psi[v], fmin(R(1), d1 / d2));
-                }
-                else {  // Venkatakrishnan (limiter.c:100-106)
-                    R top = (((d1 * d1) + e2) * d2) + ((R(2) * (d2 * d2)) * d1);
-                    R bot = (((d1 * d1) + (R(2) * (d2 * d2))) + (d1 * d2)) + e2;
-                    psi[v] = fmin(psi[v], (top / bot) / d2);
+        for (int j = 0; j < MAX_SLOTS; j++) {
+            if (j < cnt) {
+                R ox = __ldg(g.slot_off + (0 * MAX_SLOTS + j) * C + c);
+                R oy = __ldg(g.slot_off + (1 * MAX_SLOTS + j) * C + c);
+                R oz = __ldg(g.slot_off + (2 * MAX_SLOTS + j) * C + c);
+                R d2 = ((gx * ox) + (gy * oy)) + (gz * oz);
+                if (!is_close_zero(d2)) {
+                    R d1 = R(((d2 > R(0)) ? mx : mn) - qc);
+                    if (LIM == 1) {  // Barth-Jespersen (limiter.c:54-58)
+                        psi = fmin(psi, fmin(R(1), d1 / d2));
+                    }
+                    else {  // Venkatakrishnan (limiter.c:100-106)
+                        R top = (((d1 * d1) + e2) * d2) + ((R(2) * (d2 * d2)) * d1);
+                        R bot = (((d1 * d1) + (R(2) * (d2 * d2))) + (d1 * d2)) + e2;
+                        psi = fmin(psi, (top / bot) / d2);
+                    }
                 }
             }
         }
     }
-
-#pragma unroll
-    for (int v = 0; v < 5; v++) {
-#pragma unroll
-        for (int d = 0; d < 3; d++) {
-            R val = gr[3 * v + d];
-            if (FOLD && LIM != 0) {
-                val *= psi[v];
-            }
-            grad[(3 * v + d) * C + c] = val;
-        }
-        if (!FOLD) {
-            psi_out[v * C + c] = psi[v];
-        }
+    if (FOLD && LIM != 0) {
+        gx *= psi;
+        gy *= psi;
+        gz *= psi;
+    }
+    grad[(3 * v + 0) * C + c] = gx;
+    grad[(3 * v + 1) * C + c] = gy;
+    grad[(3 * v + 2) * C + c] = gz;
+    if (!FOLD) {
+        psi_out[v * C + c] = psi;
     }
 }
 
@@ -157,21 +155,25 @@ __global__ void __launch_bounds__(BLOCK) k_cell(Sizes s, const int *__restrict__
     double r[5] = {0, 0, 0, 0, 0};
     double vol = 1;
     if (active) {
+        // all slot indices first, then every face value in flight at once; sums in slot order
         double acc[5] = {0, 0, 0, 0, 0};
-        int cnt = slot_cnt[c];
-        for (int j = 0; j < cnt; j++) {
-            int sf = __ldg(slot_face + j * C + c);
-            if (sf >= 0) {
+        const int cnt = slot_cnt[c];
+        int sf[MAX_SLOTS];
 #pragma unroll
-                for (int v = 0; v < 5; v++) {
-                    acc[v] += double(__ldg(G + v * F + sf));
-                }
+        for (int j = 0; j < MAX_SLOTS; j++) {
+            sf[j] = (j < cnt) ? __ldg(slot_face + j * C + c) : 0;
+        }
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+            double gv[MAX_SLOTS];
+#pragma unroll
+            for (int j = 0; j < MAX_SLOTS; j++) {
+                gv[j] = (j < cnt) ? double(__ldg(G + (size_t)v * F + (sf[j] >= 0 ? sf[j] : ~sf[j]))) : 0.0;
             }
-            else {
-                int f = ~sf;
 #pragma unroll
-                for (int v = 0; v < 5; v++) {
-                    acc[v] -= double(__ldg(G + v * F + f));
+            for (int j = 0; j < MAX_SLOTS; j++) {
+                if (j < cnt) {
+                    acc[v] = (sf[j] >= 0) ? (acc[v] + gv[j]) : (acc[v] - gv[j]);
                 }
             }
         }

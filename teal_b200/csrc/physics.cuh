@@ -484,13 +484,10 @@ __device__ __forceinline__ Cons<R> flux_central(const Local<R> &l, const Local<R
 // Flux kinds as in the public enum (TG_FLUX_*).
 enum FluxKind { FK_NONE = 0, FK_ROE, FK_HLL, FK_HLLC, FK_HLLE, FK_AUSMD, FK_AUSMDV, FK_LXF, FK_CENTRAL };
 
-// Numerical flux in global coordinates between two primitive states (the `Convective` plugin).
+// Numerical flux in the face frame between two face-frame states.
 template <int FK, typename R>
-__device__ __forceinline__ Cons<R> convective_flux(const Prim<R> &pl, const Prim<R> &pr, R gamma,
-                                                   const Basis<R> &b)
+__device__ __forceinline__ Cons<R> convective_flux_local(const Local<R> &l, const Local<R> &r, R gamma)
 {
-    Local<R> l = make_local(pl, gamma, b);
-    Local<R> r = make_local(pr, gamma, b);
     Cons<R> f;
     if constexpr (FK == FK_ROE) {
         f = flux_roe(l, r, gamma);
@@ -516,6 +513,15 @@ __device__ __forceinline__ Cons<R> convective_flux(const Prim<R> &pl, const Prim
     else {
         f = flux_central(l, r);
     }
+    return f;
+}
+
+// Numerical flux in global coordinates between two primitive states (the `Convective` plugin).
+template <int FK, typename R>
+__device__ __forceinline__ Cons<R> convective_flux(const Prim<R> &pl, const Prim<R> &pr, R gamma,
+                                                   const Basis<R> &b)
+{
+    Cons<R> f = convective_flux_local<FK>(make_local(pl, gamma, b), make_local(pr, gamma, b), gamma);
     f.m = to_global(b, f.m);
     return f;
 }

@@ -55,6 +55,10 @@ def cases():
                     ns=False, flux="hllc", limiter="minmod", coeff=0.0, state="freestream", seed=4,
                     bcs={s: ["farfield", FREE] for s in SIDES[:4]},
                     advance=dict(method="implicit euler", courant=20.0, nk=[0.1, 0.3, 10], steps=1)))
+    out.append(dict(name="implicit_farfield_smooth", n=[10, 8, 2], lo=[0, 0, 0], hi=[1, 1, 0.2], periodic=[0, 0, 1],
+                    ns=False, flux="roe", limiter=None, coeff=0.0, state="freestream", seed=6,
+                    bcs={s: ["farfield", FREE] for s in SIDES[:4]},
+                    advance=dict(method="implicit euler", courant=20.0, nk=[0.1, 0.3, 10], steps=1)))
     return out
 
 

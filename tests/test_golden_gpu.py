@@ -1,6 +1,8 @@
 """The device path against the golden vectors written by the reference solver (no reference tree or
-oracle library needed at run time). FP64 bar: relative L2 per variable <= 1e-12; the implicit step
-<= 1e-6 (its finite-difference Jacobian divides rounding differences by the 1e-6 perturbation)."""
+oracle library needed at run time). FP64 bar: relative L2 per variable <= 1e-12. Implicit steps:
+1e-7 without a limiter and 1e-4 with one, about 10x the reference's own change under a 1e-16
+relative input perturbation (its finite-difference Jacobian amplifies rounding; with a limiter its
+is_close switch sits at the perturbation's scale; tests/test_parity_gpu.py states the measurement)."""
 
 import numpy as np
 import pytest
@@ -39,6 +41,8 @@ def test_device_reproduces_golden(name):
         t = 0.0
         for _ in range(adv["steps"]):
             t, s0, res = sim.advance(t)
-        tol = 1e-6 if adv["method"] == "implicit euler" else 1e-12
+        tol = 1e-12
+        if adv["method"] == "implicit euler":
+            tol = 1e-4 if case["limiter"] else 1e-7
         assert rel_l2(e.primitive[:C], g["advance_state"]).max() <= tol
         assert abs(t - float(g["advance_time"])) <= 1e-13 * float(g["advance_time"])

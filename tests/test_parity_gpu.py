@@ -188,21 +188,26 @@ def test_forward_euler_first_order():
     assert rel_l2(pd, pr).max() <= TOL
 
 
-def test_implicit_euler_newton_gmres():
+@pytest.mark.parametrize("limiter,tol", [(None, 1e-7), ("minmod", 1e-4)])
+def test_implicit_euler_newton_gmres(limiter, tol):
+    """The finite-difference Jacobian (relative perturbation 1e-6) makes the implicit step sensitive
+    to rounding: the reference's own step moves by 3e-9..9e-9 (smooth, no limiter) and by
+    5e-6..1.3e-5 (Barth-Jespersen limiter, whose is_close(delta2, 0) switch sits at the
+    perturbation's scale) when its input is perturbed by 1e-16 relative. The bars are ~10x those."""
     bcs = {s: ("farfield", FREE) for s in SIDES[:4]}
-    rm, re, dm, de = pair((10, 8, 2), (0, 0, 0), (1, 1, 0.2), (0, 0, 1), bcs=bcs)
+    rm, re, dm, de = pair((10, 8, 2), (0, 0, 0), (1, 1, 0.2), (0, 0, 1), bcs=bcs, limiter=limiter)
     prim = np.tile(np.array(FREE), (dm.num_cells, 1))
     rng = np.random.default_rng(4)
     prim[:, 0] *= 1 + 0.05 * rng.random(dm.num_cells)
     # step 1 starts from the same state: same CFL step
     (tr, sr, rr, pr), (td, sd, rd, pd) = run_both(re, de, prim, "implicit euler", 20.0, 1, nk=(0.1, 0.3, 10))
     assert abs(td - tr) <= 1e-13 * tr
-    assert rel_l2(pd, pr).max() <= 1e-6
-    assert np.allclose(rd, rr, rtol=1e-5)
-    # two steps: the second step size follows the (1e-7-close) state of the first
+    assert rel_l2(pd, pr).max() <= tol
+    assert np.allclose(rd, rr, rtol=100 * tol)
+    # two steps: the second step size follows the state of the first
     (tr, sr, rr, pr), (td, sd, rd, pd) = run_both(re, de, prim, "implicit euler", 20.0, 2, nk=(0.1, 0.3, 10))
-    assert abs(td - tr) <= 1e-6 * tr
-    assert rel_l2(pd, pr).max() <= 1e-6
+    assert abs(td - tr) <= tol * tr
+    assert rel_l2(pd, pr).max() <= 10 * tol
 
 
 def test_run_matches_repeated_advance():
