@@ -100,6 +100,59 @@ __device__ __forceinline__ Prim<R> reload_prim(const double *__restrict__ q, int
     return p;
 }
 
+// Per-cell gradient record: (gx, gy, gz, psi) for each of the 5 variables, 20 values per cell,
+// read and written as two 2-vectors per variable (16-byte accesses in FP64).
+template <typename R>
+struct Vec2;
+template <>
+struct Vec2<double> {
+    using T = double2;
+};
+template <>
+struct Vec2<float> {
+    using T = float2;
+};
+
+template <typename R>
+__device__ __forceinline__ void grad_rec_store(R *rec, int c, int v, R gx, R gy, R gz, R psi)
+{
+    using T2 = typename Vec2<R>::T;
+    T2 *p = reinterpret_cast<T2 *>(rec + ((size_t)c * 5 + v) * 4);
+    p[0] = T2{gx, gy};
+    p[1] = T2{gz, psi};
+}
+
+template <typename R>
+__device__ __forceinline__ void grad_rec_load(const R *rec, int c, int v, R &gx, R &gy, R &gz, R &psi)
+{
+    using T2 = typename Vec2<R>::T;
+    const T2 *p = reinterpret_cast<const T2 *>(rec + ((size_t)c * 5 + v) * 4);
+    T2 a = __ldg(p), b = __ldg(p + 1);
+    gx = a.x, gy = a.y, gz = b.x, psi = b.y;
+}
+
+// Per-face flux record: the 5 flux components padded to 6, three 2-vector accesses.
+constexpr int FLUX_REC = 6;
+
+template <typename R>
+__device__ __forceinline__ void flux_rec_store(R *G, int f, const R (&v)[5])
+{
+    using T2 = typename Vec2<R>::T;
+    T2 *p = reinterpret_cast<T2 *>(G + (size_t)f * FLUX_REC);
+    p[0] = T2{v[0], v[1]};
+    p[1] = T2{v[2], v[3]};
+    p[2] = T2{v[4], R(0)};
+}
+
+template <typename R>
+__device__ __forceinline__ void flux_rec_load(const R *G, int f, double (&v)[5])
+{
+    using T2 = typename Vec2<R>::T;
+    const T2 *p = reinterpret_cast<const T2 *>(G + (size_t)f * FLUX_REC);
+    T2 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
+    v[0] = double(a.x), v[1] = double(a.y), v[2] = double(b.x), v[3] = double(b.y), v[4] = double(c.x);
+}
+
 // is_close(x, 0) of src/core/utils.c:29-34 (absolute 1e-8, relative 1e-5)
 template <typename R>
 __device__ __forceinline__ bool is_close_zero(R x)

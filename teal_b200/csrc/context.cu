@@ -184,7 +184,7 @@ struct tg_ctx {
     // state
     double *q = nullptr, *U0 = nullptr, *R = nullptr;
     double *qs = nullptr;  // scratch state for derivatives of host-given states (allocated on use)
-    void *grad = nullptr, *psi = nullptr, *G = nullptr;
+    void *grad = nullptr, *G = nullptr;  // gradient records [C][5][4], face flux records [F][6]
     double *part_dt = nullptr, *part_res = nullptr;
     int nblk = 0;
     StepState *st = nullptr;      // device
@@ -255,7 +255,7 @@ static void free_ctx(tg_ctx *c)
                     c->proj, c->eps2, c->gb.area, c->gb.basis, c->gb.offl, c->gb.offr, c->gb.corr,
                     c->gb.slot_w, c->gb.slot_off, c->gb.area32, c->gb.basis32, c->gb.offl32,
                     c->gb.offr32, c->gb.corr32, c->gb.slot_w32, c->gb.slot_off32, c->q, c->U0, c->R, c->qs,
-                    c->grad, c->psi, c->G, c->part_dt, c->part_res, c->st, c->aos};
+                    c->grad, c->G, c->part_dt, c->part_res, c->st, c->aos};
     for (void *p : ptrs) {
         if (p) cudaFree(p);
     }
@@ -614,10 +614,9 @@ extern "C" int tg_create(const tg_mesh *m, const tg_equations *e, int precision,
         TRY(dalloc(&c->U0, 5 * (size_t)s.C));
         TRY(dalloc(&c->R, 5 * (size_t)s.C));
         if (c->order == 2) {
-            CU(cudaMalloc(&c->grad, 15 * rsz * s.C));
-            CU(cudaMalloc(&c->psi, 5 * rsz * s.C));
+            CU(cudaMalloc(&c->grad, 20 * rsz * s.C));
         }
-        CU(cudaMalloc(&c->G, 5 * rsz * s.F));
+        CU(cudaMalloc(&c->G, FLUX_REC * rsz * s.F));
         c->nblk = grid_of(s.C);
         TRY(dalloc(&c->part_dt, c->nblk));
         TRY(dalloc(&c->part_res, 5 * (size_t)c->nblk));
@@ -766,23 +765,22 @@ template <typename R>
 static void launch_gradient(tg_ctx *c, const Geometry<R> &g, bool fold, const double *q)
 {
     dim3 grid((c->s.C + GRAD_CELLS - 1) / GRAD_CELLS);
-    R *grad = (R *)c->grad;
-    R *psi = (R *)c->psi;
+    R *rec = (R *)c->grad;
     switch (c->limiter) {
         case TG_LIMITER_NONE:
-            k_gradient<R, 0, true><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, grad, psi);
+            k_gradient<R, 0, true><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
             break;
         case TG_LIMITER_BARTH_JESPERSEN:
             if (fold)
-                k_gradient<R, 1, true><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, grad, psi);
+                k_gradient<R, 1, true><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
             else
-                k_gradient<R, 1, false><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, grad, psi);
+                k_gradient<R, 1, false><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
             break;
         default:
             if (fold)
-                k_gradient<R, 2, true><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, grad, psi);
+                k_gradient<R, 2, true><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
             else
-                k_gradient<R, 2, false><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, grad, psi);
+                k_gradient<R, 2, false><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
             break;
     }
 }
@@ -809,8 +807,7 @@ static int run_face(tg_ctx *c, const double *q)
     a.s = c->s;
     a.geom = c->precision == TG_PRECISION_FP64 ? (const void *)&c->g64 : (const void *)&c->g32;
     a.q = q;
-    a.grad = c->grad;
-    a.psi = c->psi;
+    a.rec = c->grad;
     a.gamma = c->prop[0];
     a.mu = c->prop[1];
     a.prandtl = c->prop[2];
@@ -922,14 +919,12 @@ extern "C" int tg_gradient(tg_ctx *c, double time, int limited, double *gradient
     TRY(run_boundary(c, c->q));
     int lim = limited ? c->limiter : TG_LIMITER_NONE;
     TRY(run_gradient(c, c->q, lim));
-    bool fold = limited ? (fold_psi(c) || lim == TG_LIMITER_NONE) : true;
-    // with fold the stored gradient already carries psi
+    // a folded record already carries psi; an unfolded one gets it multiplied in here
+    int limit = (limited && lim != TG_LIMITER_NONE && !fold_psi(c)) ? 1 : 0;
     if (c->precision == TG_PRECISION_FP64)
-        k_grad_to_aos<double><<<grid_of(c->s.C), BLOCK, 0, c->stream>>>(
-            c->s.C, (const double *)c->grad, fold ? nullptr : (const double *)c->psi, c->aos);
+        k_grad_to_aos<double><<<grid_of(c->s.C), BLOCK, 0, c->stream>>>(c->s.C, (const double *)c->grad, limit, c->aos);
     else
-        k_grad_to_aos<float><<<grid_of(c->s.C), BLOCK, 0, c->stream>>>(
-            c->s.C, (const float *)c->grad, fold ? nullptr : (const float *)c->psi, c->aos);
+        k_grad_to_aos<float><<<grid_of(c->s.C), BLOCK, 0, c->stream>>>(c->s.C, (const float *)c->grad, limit, c->aos);
     CU(cudaGetLastError());
     TRY(d2h(c, gradient, c->aos, 15 * (size_t)c->s.C));
     return TG_OK;

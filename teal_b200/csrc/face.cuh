@@ -7,21 +7,23 @@ namespace tg {
 
 // ---- face fluxes (src/equations/derivative.c:18-227) ------------------------------------------
 //
-// Writes G[v][f] = (convective - viscous) flux * area; the cell gather adds G to the left cell and
-// subtracts it from the right one, as teal's face loops do.
+// Writes the flux record G[f] = (convective - viscous) flux * area; the cell gather adds it to the
+// left cell and subtracts it from the right one, as teal's face loops do.
+
 // Reconstructed face state of one side: q + (psi * grad) . offset per variable, streamed one
-// variable at a time so only the result stays live (derivative.c:158-164)
+// variable at a time from the cell's gradient record so only the result stays live
+// (derivative.c:158-164)
 template <typename R, bool FOLD>
-__device__ __forceinline__ void reconstruct(const Prim<R> &q, const R *__restrict__ grad,
-                                            const R *__restrict__ psi, int C, int c, V3<R> off, R (&out)[5])
+__device__ __forceinline__ void reconstruct(const Prim<R> &q, const R *__restrict__ rec, int c, V3<R> off,
+                                            R (&out)[5])
 {
     R qv[5] = {q.rho, q.u.x, q.u.y, q.u.z, q.p};
 #pragma unroll
     for (int v = 0; v < 5; v++) {
-        V3<R> gv = v3(__ldg(grad + (3 * v) * C + c), __ldg(grad + (3 * v + 1) * C + c),
-                      __ldg(grad + (3 * v + 2) * C + c));
+        R gx, gy, gz, ps;
+        grad_rec_load(rec, c, v, gx, gy, gz, ps);
+        V3<R> gv = v3(gx, gy, gz);
         if (!FOLD) {
-            R ps = __ldg(psi + v * C + c);
             gv = v3(gv.x * ps, gv.y * ps, gv.z * ps);
         }
         out[v] = qv[v] + dot(gv, off);
@@ -33,14 +35,14 @@ __device__ __forceinline__ void reconstruct(const Prim<R> &q, const R *__restric
 // which are still in L1); the register cap keeps 16 warps per SM resident.
 template <typename R, int FK, bool NS, int ORDER, bool FOLD>
 __global__ void __launch_bounds__(BLOCK, 2) k_face(Sizes s, Geometry<R> g, const double *__restrict__ q,
-                                                   const R *__restrict__ grad, const R *__restrict__ psi,
-                                                   R gamma, R mu, R prandtl, R *__restrict__ G)
+                                                   const R *__restrict__ rec, R gamma, R mu, R prandtl,
+                                                   R *__restrict__ G)
 {
     int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= s.F) {
         return;
     }
-    const int F = s.F, C = s.C, N = s.N;
+    const int F = s.F, N = s.N;
     const bool boundary = (f >= s.F_in) && (f < s.F_bd);
     int2 c = g.lr[f];
 
@@ -59,12 +61,12 @@ __global__ void __launch_bounds__(BLOCK, 2) k_face(Sizes s, Geometry<R> g, const
             }
             else {
                 R pl[5], pr[5];
-                reconstruct<R, FOLD>(ql, grad, psi, C, c.x, load_v3(g.offl, F, f), pl);
+                reconstruct<R, FOLD>(ql, rec, c.x, load_v3(g.offl, F, f), pl);
                 if (boundary) {  // the ghost state enters unreconstructed (derivative.c:203-211)
                     pr[0] = qr.rho, pr[1] = qr.u.x, pr[2] = qr.u.y, pr[3] = qr.u.z, pr[4] = qr.p;
                 }
                 else {
-                    reconstruct<R, FOLD>(qr, grad, psi, C, c.y, load_v3(g.offr, F, f), pr);
+                    reconstruct<R, FOLD>(qr, rec, c.y, load_v3(g.offr, F, f), pr);
                 }
                 l = make_local(prim_from(pl), gamma, b);
                 r = make_local(prim_from(pr), gamma, b);
@@ -89,9 +91,16 @@ __global__ void __launch_bounds__(BLOCK, 2) k_face(Sizes s, Geometry<R> g, const
             qm[v] = (qlv[v] + qrv[v]) / R(2);
         }
 #pragma unroll
-        for (int k = 0; k < 15; k++) {
-            R a = __ldg(grad + k * C + c.x);
-            gm[k] = boundary ? a : (a + __ldg(grad + k * C + c.y)) / R(2);
+        for (int v = 0; v < 5; v++) {
+            R ax, ay, az, ap, bx, by, bz, bp;
+            grad_rec_load(rec, c.x, v, ax, ay, az, ap);
+            if (boundary) {
+                gm[3 * v] = ax, gm[3 * v + 1] = ay, gm[3 * v + 2] = az;
+            }
+            else {
+                grad_rec_load(rec, c.y, v, bx, by, bz, bp);
+                gm[3 * v] = (ax + bx) / R(2), gm[3 * v + 1] = (ay + by) / R(2), gm[3 * v + 2] = (az + bz) / R(2);
+            }
         }
         V3<R> unit = load_v3(g.corr, F, f);
         R norm = __ldg(g.corr + 3 * F + f);
@@ -117,10 +126,7 @@ __global__ void __launch_bounds__(BLOCK, 2) k_face(Sizes s, Geometry<R> g, const
         gf[3] -= fv.m.z * area;
         gf[4] -= fv.e * area;
     }
-#pragma unroll
-    for (int v = 0; v < 5; v++) {
-        G[(size_t)v * F + f] = gf[v];
-    }
+    flux_rec_store(G, f, gf);
 }
 
 }  // namespace tg

@@ -29,12 +29,14 @@ __global__ void k_boundary(Sizes s, const int2 *__restrict__ lr, const double *_
 
 // ---- least-squares gradient + limiter (src/equations/gradient.c:7-58, limiter.c:23-113) -------
 //
-// One thread per (cell, variable): a block of GRAD_WARPS x 32 threads covers 32 consecutive cells,
-// warp w handling variable w, so every warp reads one contiguous row of the state and writes
-// contiguous gradient rows; the per-thread state is one variable's gradient, bounds and factor.
-// Each component is summed over the cell's slots in face order, as teal's face loop adds it.
-// FOLD: store the limited gradient (Euler: only the limited one is used); otherwise store the
-// unlimited gradient and the limiter factors psi (Navier-Stokes: the viscous flux needs both).
+// One thread per (cell, variable): a block of 5 x 32 threads covers 32 consecutive cells, warp w
+// handling variable w, so each warp reads one contiguous row of the state. The block first stages
+// the slot geometry of its 32 cells (neighbour rows, least-squares weights, face offsets: 312 bytes
+// per cell in FP64) in shared memory with coalesced loads; the five variable warps then read it
+// from there instead of each fetching it from L1/L2. Each gradient component is summed over the
+// cell's slots in face order, as teal's face loop adds it. Output: one gradient record per cell,
+// (gx, gy, gz, psi) per variable (grad_rec_store); FOLD multiplies psi in (Euler: only the limited
+// gradient is used), otherwise the record keeps the unlimited gradient for the viscous flux.
 constexpr int GRAD_CELLS = 32;
 constexpr int GRAD_THREADS = 5 * GRAD_CELLS;
 
@@ -42,39 +44,54 @@ template <typename R, int LIM, bool FOLD>
 __global__ void __launch_bounds__(GRAD_THREADS) k_gradient(Sizes s, Geometry<R> g,
                                                            const double *__restrict__ eps2,
                                                            const double *__restrict__ q,
-                                                           R *__restrict__ grad, R *__restrict__ psi_out)
+                                                           R *__restrict__ rec)
 {
-    const int v = threadIdx.x >> 5;  // variable of this warp
-    const int c = blockIdx.x * GRAD_CELLS + (threadIdx.x & 31);
-    if (c >= s.C) {
+    __shared__ int s_nbr[MAX_SLOTS][GRAD_CELLS];
+    __shared__ int s_cnt[GRAD_CELLS];
+    __shared__ R s_w[3 * MAX_SLOTS][GRAD_CELLS];
+    __shared__ R s_off[(LIM != 0) ? 3 * MAX_SLOTS : 1][GRAD_CELLS];
+    const int C = s.C;
+    const int base = blockIdx.x * GRAD_CELLS;
+    const int ncell = min(GRAD_CELLS, C - base);
+    for (int i = threadIdx.x; i < MAX_SLOTS * GRAD_CELLS; i += GRAD_THREADS) {
+        int j = i / GRAD_CELLS, l = i % GRAD_CELLS;
+        s_nbr[j][l] = (l < ncell) ? __ldg(g.slot_nbr + (size_t)j * C + base + l) : 0;
+    }
+    if (threadIdx.x < GRAD_CELLS) {
+        s_cnt[threadIdx.x] = (threadIdx.x < ncell) ? int(g.slot_cnt[base + threadIdx.x]) : 0;
+    }
+    for (int i = threadIdx.x; i < 3 * MAX_SLOTS * GRAD_CELLS; i += GRAD_THREADS) {
+        int k = i / GRAD_CELLS, l = i % GRAD_CELLS;
+        s_w[k][l] = (l < ncell) ? __ldg(g.slot_w + (size_t)k * C + base + l) : R(0);
+        if (LIM != 0) {
+            s_off[k][l] = (l < ncell) ? __ldg(g.slot_off + (size_t)k * C + base + l) : R(0);
+        }
+    }
+    __syncthreads();
+
+    const int v = threadIdx.x / GRAD_CELLS;  // variable of this warp
+    const int l = threadIdx.x % GRAD_CELLS;
+    if (l >= ncell) {
         return;
     }
-    const int C = s.C;
+    const int c = base + l;
     const double *qv = q + (size_t)v * s.N;
     const double qc = __ldg(qv + c);
-    const int cnt = g.slot_cnt[c];
-    int nbr[MAX_SLOTS];
+    const int cnt = s_cnt[l];
     double qn[MAX_SLOTS];
 #pragma unroll
     for (int j = 0; j < MAX_SLOTS; j++) {
-        nbr[j] = (j < cnt) ? __ldg(g.slot_nbr + j * C + c) : c;
-    }
-#pragma unroll
-    for (int j = 0; j < MAX_SLOTS; j++) {
-        qn[j] = __ldg(qv + nbr[j]);
+        qn[j] = __ldg(qv + ((j < cnt) ? s_nbr[j][l] : c));
     }
     R gx = R(0), gy = R(0), gz = R(0);
     double mn = qc, mx = qc;
 #pragma unroll
     for (int j = 0; j < MAX_SLOTS; j++) {
         if (j < cnt) {
-            R wx = __ldg(g.slot_w + (0 * MAX_SLOTS + j) * C + c);
-            R wy = __ldg(g.slot_w + (1 * MAX_SLOTS + j) * C + c);
-            R wz = __ldg(g.slot_w + (2 * MAX_SLOTS + j) * C + c);
             R d = R(qn[j] - qc);
-            gx += d * wx;
-            gy += d * wy;
-            gz += d * wz;
+            gx += d * s_w[0 * MAX_SLOTS + j][l];
+            gy += d * s_w[1 * MAX_SLOTS + j][l];
+            gz += d * s_w[2 * MAX_SLOTS + j][l];
             mn = fmin(mn, qn[j]);
             mx = fmax(mx, qn[j]);
         }
@@ -86,10 +103,8 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_gradient(Sizes s, Geometry<R> 
 #pragma unroll
         for (int j = 0; j < MAX_SLOTS; j++) {
             if (j < cnt) {
-                R ox = __ldg(g.slot_off + (0 * MAX_SLOTS + j) * C + c);
-                R oy = __ldg(g.slot_off + (1 * MAX_SLOTS + j) * C + c);
-                R oz = __ldg(g.slot_off + (2 * MAX_SLOTS + j) * C + c);
-                R d2 = ((gx * ox) + (gy * oy)) + (gz * oz);
+                R d2 = ((gx * s_off[0 * MAX_SLOTS + j][l]) + (gy * s_off[1 * MAX_SLOTS + j][l])) +
+                       (gz * s_off[2 * MAX_SLOTS + j][l]);
                 if (!is_close_zero(d2)) {
                     R d1 = R(((d2 > R(0)) ? mx : mn) - qc);
                     if (LIM == 1) {  // Barth-Jespersen (limiter.c:54-58)
@@ -109,12 +124,7 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_gradient(Sizes s, Geometry<R> 
         gy *= psi;
         gz *= psi;
     }
-    grad[(3 * v + 0) * C + c] = gx;
-    grad[(3 * v + 1) * C + c] = gy;
-    grad[(3 * v + 2) * C + c] = gz;
-    if (!FOLD) {
-        psi_out[v * C + c] = psi;
-    }
+    grad_rec_store(rec, c, v, gx, gy, gz, psi);
 }
 
 // per-cell time step of the equations' Timestep plugin
@@ -149,7 +159,7 @@ __global__ void __launch_bounds__(BLOCK) k_cell(Sizes s, const int *__restrict__
                                                 double *__restrict__ part_res)
 {
     __shared__ double sh[BLOCK / 32];
-    const int C = s.C, F = s.F, N = s.N;
+    const int C = s.C, N = s.N;
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     bool active = c < C;
     double r[5] = {0, 0, 0, 0, 0};
@@ -163,17 +173,17 @@ __global__ void __launch_bounds__(BLOCK) k_cell(Sizes s, const int *__restrict__
         for (int j = 0; j < MAX_SLOTS; j++) {
             sf[j] = (j < cnt) ? __ldg(slot_face + j * C + c) : 0;
         }
+        double gv[MAX_SLOTS][5];
 #pragma unroll
-        for (int v = 0; v < 5; v++) {
-            double gv[MAX_SLOTS];
+        for (int j = 0; j < MAX_SLOTS; j++) {
+            flux_rec_load(G, (j < cnt) ? (sf[j] >= 0 ? sf[j] : ~sf[j]) : 0, gv[j]);
+        }
 #pragma unroll
-            for (int j = 0; j < MAX_SLOTS; j++) {
-                gv[j] = (j < cnt) ? double(__ldg(G + (size_t)v * F + (sf[j] >= 0 ? sf[j] : ~sf[j]))) : 0.0;
-            }
+        for (int j = 0; j < MAX_SLOTS; j++) {
+            if (j < cnt) {
 #pragma unroll
-            for (int j = 0; j < MAX_SLOTS; j++) {
-                if (j < cnt) {
-                    acc[v] = (sf[j] >= 0) ? (acc[v] + gv[j]) : (acc[v] - gv[j]);
+                for (int v = 0; v < 5; v++) {
+                    acc[v] = (sf[j] >= 0) ? (acc[v] + gv[j][v]) : (acc[v] - gv[j][v]);
                 }
             }
         }
@@ -512,21 +522,23 @@ __global__ void k_aos5_to_soa(int C, const double *__restrict__ aos, double *__r
     }
 }
 
-// gradient [15][C] -> teal's [C][5][3] (limited if psi given)
+// gradient records -> teal's [C][5][3] (limited when `limit` and the record is not folded)
 template <typename R>
-__global__ void k_grad_to_aos(int C, const R *__restrict__ grad, const R *__restrict__ psi,
-                              double *__restrict__ aos)
+__global__ void k_grad_to_aos(int C, const R *__restrict__ rec, int limit, double *__restrict__ aos)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= C) {
         return;
     }
-    for (int k = 0; k < 15; k++) {
-        R g = grad[k * C + i];
-        if (psi) {
-            g *= psi[(k / 3) * C + i];
+    for (int v = 0; v < 5; v++) {
+        R gx, gy, gz, psi;
+        grad_rec_load(rec, i, v, gx, gy, gz, psi);
+        if (limit) {
+            gx *= psi, gy *= psi, gz *= psi;
         }
-        aos[(size_t)i * 15 + k] = double(g);
+        aos[(size_t)i * 15 + 3 * v] = double(gx);
+        aos[(size_t)i * 15 + 3 * v + 1] = double(gy);
+        aos[(size_t)i * 15 + 3 * v + 2] = double(gz);
     }
 }
 

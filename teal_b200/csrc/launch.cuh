@@ -12,8 +12,7 @@ struct FaceLaunch {
     Sizes s;
     const void *geom;  // Geometry<R>*
     const double *q;
-    const void *grad;
-    const void *psi;
+    const void *rec;
     double gamma, mu, prandtl;
     void *G;
 };
@@ -22,22 +21,21 @@ template <int FK, typename R>
 inline cudaError_t launch_face_r(bool ns, int order, bool fold, const FaceLaunch &a, cudaStream_t st)
 {
     const Geometry<R> &g = *static_cast<const Geometry<R> *>(a.geom);
-    const R *grad = static_cast<const R *>(a.grad);
-    const R *psi = static_cast<const R *>(a.psi);
+    const R *rec = static_cast<const R *>(a.rec);
     R *G = static_cast<R *>(a.G);
     dim3 grid((a.s.F + BLOCK - 1) / BLOCK);
     R gm = R(a.gamma), mu = R(a.mu), pr = R(a.prandtl);
     if (order == 1) {
-        k_face<R, FK, false, 1, true><<<grid, BLOCK, 0, st>>>(a.s, g, a.q, grad, psi, gm, mu, pr, G);
+        k_face<R, FK, false, 1, true><<<grid, BLOCK, 0, st>>>(a.s, g, a.q, rec, gm, mu, pr, G);
     }
     else if (!ns) {
-        k_face<R, FK, false, 2, true><<<grid, BLOCK, 0, st>>>(a.s, g, a.q, grad, psi, gm, mu, pr, G);
+        k_face<R, FK, false, 2, true><<<grid, BLOCK, 0, st>>>(a.s, g, a.q, rec, gm, mu, pr, G);
     }
     else if (fold) {
-        k_face<R, FK, true, 2, true><<<grid, BLOCK, 0, st>>>(a.s, g, a.q, grad, psi, gm, mu, pr, G);
+        k_face<R, FK, true, 2, true><<<grid, BLOCK, 0, st>>>(a.s, g, a.q, rec, gm, mu, pr, G);
     }
     else {
-        k_face<R, FK, true, 2, false><<<grid, BLOCK, 0, st>>>(a.s, g, a.q, grad, psi, gm, mu, pr, G);
+        k_face<R, FK, true, 2, false><<<grid, BLOCK, 0, st>>>(a.s, g, a.q, rec, gm, mu, pr, G);
     }
     return cudaGetLastError();
 }

@@ -1,0 +1,87 @@
+"""The FP32-flux form (gradients, limiter and face fluxes in FP32; residual accumulation, RK update
+and norms in FP64) against the FP64 oracle: relative L2 per conserved variable of the residual and
+of the state after explicit steps, plus the kinetic-energy and enstrophy histories of the
+Taylor-Green vortex."""
+
+import numpy as np
+import pytest
+
+import teal_b200 as tb
+from oracle import ref
+from teal_b200 import diagnostics
+from tests.cases import rel_l2, taylor_green, vortex
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not ref.available(), reason="reference oracle not built")]
+
+FP32 = tb.TG_PRECISION_FP32_FLUX
+
+
+def report(name, value):
+    print(f"[fp32] {name}: {value}")
+
+
+def test_fp32_vortex_state_error():
+    n, lo, hi, per = (32, 32, 4), (0, 0, 0), (10, 10, 0.625), (1, 1, 1)
+    rm = ref.RefMesh(lo, hi, n, per)
+    re = ref.RefEquations(rm, False)
+    m = tb.Mesh.create(lo, hi, n, per)
+    e = tb.Equations.euler(m)
+    prim = vortex(m.cell_center)
+    d_err = rel_l2(e.derivative(prim, precision=FP32), re.derivative(prim)).max()
+    report("vortex residual rel L2", d_err)
+    assert d_err < 1e-3
+    re.set_primitive(prim)
+    e.primitive[:] = prim
+    rs = ref.RefSimulation(re, "lserk", 0.5, rk=(3, 3))
+    ds = tb.Simulation(e, precision=FP32)
+    ds.set_advance("lserk", 0.5, (3, 3))
+    t_ref = t_dev = 0.0
+    for _ in range(20):
+        t_ref, _, _ = rs.advance(t_ref)
+        t_dev, _, _ = ds.advance(t_dev)
+    C = m.num_inner_cells
+    err = rel_l2(e.primitive[:C], re.primitive[:C]).max()
+    report("vortex state after 20 RK3 steps rel L2", err)
+    assert err < 1e-6
+
+
+def test_fp32_taylor_green_histories():
+    n, lo, hi, per = (24, 24, 24), (0, 0, 0), (2 * np.pi,) * 3, (1, 1, 1)
+    rm = ref.RefMesh(lo, hi, n, per)
+    re = ref.RefEquations(rm, True)
+    m = tb.Mesh.create(lo, hi, n, per)
+    e = tb.Equations.navierstokes(m)
+    for q in (re, e):
+        q.set_convective_flux("roe")
+        q.set_limiter("venkatakrishnan", 1.0)
+        q.set_property("dynamic viscosity", 1 / 1600)
+    prim = taylor_green(m.cell_center)
+    d_err = rel_l2(e.derivative(prim, precision=FP32), re.derivative(prim)).max()
+    report("tgv residual rel L2", d_err)
+    re.set_primitive(prim)
+    e.primitive[:] = prim
+    rs = ref.RefSimulation(re, "lserk", 0.99, rk=(3, 3))
+    ds = tb.Simulation(e, precision=FP32)
+    ds.set_advance("lserk", 0.99, (3, 3))
+    C = m.num_inner_cells
+    vol = m.cell_volume
+    ke_err, en_err = [], []
+    t_ref = t_dev = 0.0
+    for k in range(4):
+        for _ in range(5):
+            t_ref, _, _ = rs.advance(t_ref)
+            t_dev, _, _ = ds.advance(t_dev)
+        ke_r = diagnostics.kinetic_energy(re.primitive[:C], vol)
+        ke_d = diagnostics.kinetic_energy(e.primitive[:C], vol)
+        en_r = diagnostics.enstrophy(re.primitive[:C], re.gradient(re.primitive)[:C], vol)
+        ctx = e.context(tb.TG_PRECISION_FP64)
+        ctx.set_primitive(e.primitive)
+        en_d = diagnostics.enstrophy(e.primitive[:C], ctx.gradient(), vol)
+        ke_err.append(abs(ke_d - ke_r) / ke_r)
+        en_err.append(abs(en_d - en_r) / en_r)
+    err = rel_l2(e.primitive[:C], re.primitive[:C]).max()
+    report("tgv state after 20 RK3 steps rel L2", err)
+    report("tgv kinetic energy rel error history", ke_err)
+    report("tgv enstrophy rel error history", en_err)
+    assert err < 1e-5
+    assert max(ke_err) < 1e-6 and max(en_err) < 1e-5
