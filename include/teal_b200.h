@@ -207,6 +207,23 @@ int tg_run(tg_ctx *ctx, int method, const void *context, double courant, int max
            double max_time, int variable, double threshold, double *time, int *iter,
            double *residual);
 
+/* ---- batches: several meshes packed into one device arena ---------------------------------------
+ * Instances share the equations, schemes and properties (one "lane"); boundary conditions,
+ * Venkatakrishnan parameters and states differ per instance. The arena keeps all inner cells first
+ * (instance order), then all boundary ghosts; faces likewise, so every kernel runs once over all
+ * instances. Each instance keeps its own time step (CFL over its own cells), time, residual norm
+ * and stop tests, exactly as if it ran alone; the whole batch step replays from one CUDA graph. */
+int tg_batch_create(const tg_mesh *meshes, const tg_equations *eqns, int num, int precision, tg_ctx **ctx);
+int tg_batch_size(tg_ctx *ctx, int *num);
+int tg_batch_set_primitive(tg_ctx *ctx, int instance, const double *primitive);
+int tg_batch_get_primitive(tg_ctx *ctx, int instance, double *primitive);
+/* Run every instance until its own limit: max_iter[i] steps, max_time[i] (null: none), or the
+ * residual of variable[i] (-1: maximum; null: all -1) below threshold[i] (null or <= 0: none).
+ * time[i] is read and updated; iter[i] and residual[i][5] return the end state. Explicit methods. */
+int tg_batch_run(tg_ctx *ctx, int method, const void *context, double courant, const int *max_iter,
+                 const double *max_time, const int *variable, const double *threshold, double *time,
+                 int *iter, double *residual);
+
 /* ---- drop-in Advance methods with teal's signature (src/simulation.h:6-7) ----------------------- */
 
 /* Bind a teal `Equations *` (used only as a lookup key) to a context and to the host primitive

@@ -16,6 +16,7 @@ from ._lib import (  # noqa: F401
     TG_PRECISION_FP64,
 )
 from .api import (  # noqa: F401
+    Batch,
     Context,
     Equations,
     Mesh,

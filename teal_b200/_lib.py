@@ -9,7 +9,8 @@ import ctypes
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libteal_b200.so")
+# TEAL_B200_LIBRARY selects another build of the same library (autotuning variants)
+LIB_PATH = os.environ.get("TEAL_B200_LIBRARY") or os.path.join(_HERE, "libteal_b200.so")
 
 TG_OK = 0
 TG_ERR_INVALID = 1
@@ -118,6 +119,13 @@ SIGNATURES = [
                                   _vp, _dbl_p]),
     ("tg_run", ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_double, ctypes.c_int, ctypes.c_double,
                               ctypes.c_int, ctypes.c_double, _dbl_p, _int_p, _vp]),
+    ("tg_batch_create", ctypes.c_int, [ctypes.POINTER(TgMesh), ctypes.POINTER(TgEquations), ctypes.c_int,
+                                       ctypes.c_int, ctypes.POINTER(_vp)]),
+    ("tg_batch_size", ctypes.c_int, [_vp, _int_p]),
+    ("tg_batch_set_primitive", ctypes.c_int, [_vp, ctypes.c_int, _vp]),
+    ("tg_batch_get_primitive", ctypes.c_int, [_vp, ctypes.c_int, _vp]),
+    ("tg_batch_run", ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_double, _vp, _vp, _vp, _vp, _vp, _vp,
+                                    _vp]),
     ("tg_bind", ctypes.c_int, [_vp, _vp, _vp]),
     ("tg_unbind", ctypes.c_int, [_vp]),
     ("tg_teal_euler", ctypes.c_double, [_vp, _dbl_p, _vp, ctypes.c_double, ctypes.c_double, _vp]),

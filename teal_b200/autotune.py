@@ -1,0 +1,129 @@
+"""Autotuner of the hot kernels' launch shapes.
+
+Builds the library once per candidate of (face-flux block size, face-flux blocks resident per SM,
+cell-gather block size) into a scratch directory, times a fixed number of RK steps of a workload on
+the current GPU with each build (a fresh process per build, selected with TEAL_B200_LIBRARY), and
+writes the fastest shape to teal_b200/csrc/tuned.h (and to --out when given).
+
+    python -m teal_b200.autotune [--n 96] [--steps 10] [--precision fp64] [--out gpurun_out/tuned.h]
+
+Needs nvcc and a GPU. Every candidate computes the same results; only speed differs.
+"""
+
+import argparse
+import concurrent.futures
+import itertools
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+ROOT = os.path.dirname(HERE)
+
+# face-flux block size x resident face threads per SM (65536 registers / threads = the cap per
+# thread: 512 -> 128, 768 -> 85, 1024 -> 64) x cell-gather block size
+FACE_BLOCKS = [128, 256]
+FACE_THREADS = [512, 768, 1024]
+CELL_BLOCKS = [128, 256]
+
+TIMER = r"""
+import json, math, sys, time
+import torch
+import teal_b200 as tb
+n, steps, prec = int(sys.argv[1]), int(sys.argv[2]), sys.argv[3]
+def tgv(c, gamma=1.4, mach=0.1):
+    import numpy as np
+    x, y, z = c[:, 0], c[:, 1], c[:, 2]
+    p0 = 1 / (gamma * mach**2)
+    out = np.zeros((c.shape[0], 5))
+    out[:, 1] = np.sin(x) * np.cos(y) * np.cos(z)
+    out[:, 2] = -np.cos(x) * np.sin(y) * np.cos(z)
+    out[:, 4] = p0 + (np.cos(2 * x) + np.cos(2 * y)) * (np.cos(2 * z) + 2) / 16
+    out[:, 0] = out[:, 4] / p0
+    return out
+m = tb.Mesh.create((0, 0, 0), (2 * math.pi,) * 3, (n, n, n), (1, 1, 1))
+e = tb.Equations.navierstokes(m)
+e.set_convective_flux("roe"); e.set_limiter("venkatakrishnan", 1.0); e.set_property("dynamic viscosity", 1 / 1600)
+e.set_initial_condition("domain", tgv)
+ctx = e.context(tb.TG_PRECISION_FP64 if prec == "fp64" else tb.TG_PRECISION_FP32_FLUX)
+s = torch.cuda.Stream(); ctx.set_stream(s.cuda_stream)
+ctx.run(tb.TG_ADVANCE_LSERK, 0.99, 3, context=(3, 3)); torch.cuda.synchronize()
+best = float("inf")
+for _ in range(3):
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(s); ctx.run(tb.TG_ADVANCE_LSERK, 0.99, steps, context=(3, 3)); b.record(s); torch.cuda.synchronize()
+    best = min(best, a.elapsed_time(b) / steps)
+print(json.dumps({"ms_per_step": best}))
+"""
+
+
+def build(variant, workdir, jobs):
+    name = "_".join(f"{k[3:].lower()}{v}" for k, v in variant.items())
+    out = os.path.join(workdir, f"lib_{name}.so")
+    tune = " ".join(f"-D{k}={v}" for k, v in variant.items())
+    cmd = ["make", "-C", CSRC, f"-j{jobs}", f"OUT={out}", f"BUILD={os.path.join(workdir, 'build_' + name)}",
+           f"TUNE={tune}"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"build of {name} failed:\n{r.stderr[-2000:]}")
+    return name, out
+
+
+def time_variant(lib, n, steps, precision):
+    env = dict(os.environ, TEAL_B200_LIBRARY=lib, PYTHONPATH=ROOT + os.pathsep + os.environ.get("PYTHONPATH", ""))
+    r = subprocess.run([sys.executable, "-c", TIMER, str(n), str(steps), precision], capture_output=True,
+                       text=True, env=env, timeout=600)
+    if r.returncode != 0:
+        raise RuntimeError(r.stderr[-2000:])
+    return json.loads(r.stdout.strip().splitlines()[-1])["ms_per_step"]
+
+
+def write_header(path, best):
+    lines = ["// Launch shapes of the hot kernels, chosen by teal_b200/autotune.py on a B200 (fastest",
+             "// measured RK step); a value given with -D at build time wins.", "#pragma once", ""]
+    notes = {"TG_FACE_BLOCK": "threads per face-flux block",
+             "TG_FACE_MINB": "face-flux blocks kept resident per SM (caps registers per thread)",
+             "TG_CELL_BLOCK": "threads per cell-gather block"}
+    for k, v in best.items():
+        lines += [f"#ifndef {k}", f"#define {k} {v}  // {notes[k]}", "#endif"]
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, default=96)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--out", default=None, help="also write the chosen header here")
+    ap.add_argument("--jobs", type=int, default=os.cpu_count() or 8)
+    args = ap.parse_args()
+    variants = [{"TG_FACE_BLOCK": fb, "TG_FACE_MINB": ft // fb, "TG_CELL_BLOCK": cb}
+                for fb, ft, cb in itertools.product(FACE_BLOCKS, FACE_THREADS, CELL_BLOCKS)]
+    results = []
+    with tempfile.TemporaryDirectory() as work:
+        per = max(2, args.jobs // 4)
+        with concurrent.futures.ThreadPoolExecutor(max_workers=4) as pool:
+            built = list(pool.map(lambda v: (v,) + build(v, work, per), variants))
+        for v, name, lib in built:
+            try:
+                ms = time_variant(lib, args.n, args.steps, args.precision)
+            except Exception as exc:  # a variant that fails is reported and skipped
+                print(json.dumps({"variant": v, "error": str(exc)[-300:]}), flush=True)
+                continue
+            results.append((ms, v))
+            print(json.dumps({"variant": v, "ms_per_step": ms}), flush=True)
+    if not results:
+        raise SystemExit("no variant ran")
+    ms, best = min(results, key=lambda r: r[0])
+    write_header(os.path.join(CSRC, "tuned.h"), best)
+    if args.out:
+        write_header(args.out, best)
+    print(json.dumps({"best": best, "ms_per_step": ms, "workload": f"tgv {args.n}^3 {args.precision}"}))
+
+
+if __name__ == "__main__":
+    main()

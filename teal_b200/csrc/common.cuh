@@ -5,10 +5,14 @@
 #include <cfloat>
 
 #include "device.cuh"
+#include "tuned.h"
 
 namespace tg {
 
 constexpr int BLOCK = 256;
+constexpr int FACE_BLOCK = TG_FACE_BLOCK;
+constexpr int FACE_MINB = TG_FACE_MINB;
+constexpr int CELL_BLOCK = TG_CELL_BLOCK;
 constexpr int REDUCE_BLOCK = 1024;
 
 // ---- small helpers ---------------------------------------------------------------------------

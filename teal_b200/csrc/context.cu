@@ -141,17 +141,23 @@ struct GeomBuf {
 // workspace of the Jacobian-free Newton-GMRES implicit step
 struct Gmres {
     int dim = 0;
-    double *U = nullptr;     // [5][C] Newton iterate (conserved)
+    double *U = nullptr;      // [5][C] Newton iterate (conserved)
     double *Ustart = nullptr; // [5][C] conserved state at the start of the step
-    double *r = nullptr;     // [5][C] Newton residual
-    double *delta = nullptr; // [5][C] increment
-    double *V = nullptr;     // [dim + 1][5][C] Krylov basis
-    double *w = nullptr;     // [5][C]
-    double *q1 = nullptr;    // [5][N] perturbed primitive state
-    double *R1 = nullptr;    // [5][C] derivative of the perturbed state
-    double *part = nullptr;  // block partials
-    double *sc = nullptr;    // device scalars (see GmresScalars)
+    double *r = nullptr;      // [5][C] Newton residual
+    double *delta = nullptr;  // [5][C] increment
+    double *V = nullptr;      // [dim + 1][5][C] Krylov basis
+    double *w = nullptr;      // [5][C]
+    double *q1 = nullptr;     // [5][N] perturbed primitive state
+    double *R1 = nullptr;     // [5][C] derivative of the perturbed state
+    double *part = nullptr;   // block partials
+    double *sc = nullptr;     // device scalars (GmresScalar)
 };
+
+// Host mirror of the per-instance step arrays (pinned; one copy per direction moves all of them):
+// doubles: time, step, step0, max_step, max_time, threshold, residual[5]; ints: variable, iter,
+// max_iter, active, then num_active and error.
+enum { SD_TIME, SD_STEP, SD_STEP0, SD_MAX_STEP, SD_MAX_TIME, SD_THRESHOLD, SD_RESIDUAL, SD_COUNT = SD_RESIDUAL + 5 };
+enum { SI_VARIABLE, SI_ITER, SI_MAX_ITER, SI_ACTIVE, SI_COUNT };
 
 struct tg_ctx {
     int device = 0;
@@ -160,15 +166,21 @@ struct tg_ctx {
 
     // sizes
     Sizes s{};
-    int num_cells = 0;          // teal's cells.num
-    int off_boundary_cells = 0; // first periodic ghost
-    int num_periodic = 0;
+    int num_periodic = 0;  // periodic ghosts of the arena (redirected to their owners)
 
-    // equations
+    // equations (shared by every instance of the arena)
     int physics = 0, order = 2, flux = 0, viscous = 0, limiter = 0, precision = 0;
     double prop[3] = {1.4, 0, 0.71};
-    double sum_volume = 0;
-    BoundaryTable bt{};
+
+    // instances
+    int ninst = 1;
+    std::vector<int> inst_row_off;  // teal rows of each instance in the row map
+    int *rowmap = nullptr;          // teal row of an instance -> arena state row (periodic: owner)
+    std::vector<int> h_inst_cell_off;
+    int *cell_inst = nullptr, *inst_cell_off = nullptr, *piece_beg = nullptr, *inst_piece_off = nullptr;
+    double *sum_volume = nullptr;
+    int npieces = 0;
+    Segments seg{};
 
     // device mesh
     int2 *lr = nullptr;
@@ -176,6 +188,8 @@ struct tg_ctx {
     uint8_t *slot_cnt = nullptr;
     int *owner = nullptr;      // periodic ghost -> owner cell
     int *bface_ent = nullptr;  // boundary face -> boundary index
+    int *bkind = nullptr;      // boundary index -> TG_BC_*
+    double *bctx = nullptr;    // boundary index -> primitive context [5]
     double *volume = nullptr, *proj = nullptr, *eps2 = nullptr;
     GeomBuf gb;
     Geometry<double> g64{};
@@ -185,15 +199,18 @@ struct tg_ctx {
     double *q = nullptr, *U0 = nullptr, *R = nullptr;
     double *qs = nullptr;  // scratch state for derivatives of host-given states (allocated on use)
     void *grad = nullptr, *G = nullptr;  // gradient records [C][5][4], face flux records [F][6]
-    double *part_dt = nullptr, *part_res = nullptr;
-    int nblk = 0;
-    StepState *st = nullptr;      // device
-    StepState *st_host = nullptr; // pinned mirror
-    double *aos = nullptr;        // device scratch for teal-layout transfers
+    double *dtc = nullptr;               // per-cell stable step
+    double *part_min = nullptr, *part_sum = nullptr;
+    double *sd = nullptr;  // device step doubles [SD_COUNT][ninst]
+    int *si = nullptr;     // device step ints [SI_COUNT][ninst] + num_active + error
+    double *hd = nullptr;  // pinned mirrors
+    int *hi = nullptr;
+    Steps st{};
+    double *aos = nullptr;     // device scratch for teal-layout transfers
     size_t aos_len = 0;
-    double *pinned = nullptr;     // pinned host staging buffer
+    double *pinned = nullptr;  // pinned host staging buffer
     size_t pinned_len = 0;
-    bool prepared = false;        // U0 and part_dt valid for the resident state
+    bool prepared = false;     // U0, dtc and the piece minima valid for the resident state
 
     // implicit solver workspace (allocated on first use)
     Gmres gm{};
@@ -209,10 +226,15 @@ struct tg_ctx {
 
     // step graph cache
     cudaGraphExec_t graph = nullptr;
-    int graph_method = -1, graph_stages = 0, graph_order = 0;
+    int graph_method = -1, graph_stages = 0;
     double graph_courant = 0;
     int graph_use_max_time = -1;
 };
+
+static double &hd_at(tg_ctx *c, int field, int i) { return c->hd[(size_t)field * c->ninst + i]; }
+static int &hi_at(tg_ctx *c, int field, int i) { return c->hi[(size_t)field * c->ninst + i]; }
+static int &hi_num_active(tg_ctx *c) { return c->hi[(size_t)SI_COUNT * c->ninst]; }
+static int &hi_error(tg_ctx *c) { return c->hi[(size_t)SI_COUNT * c->ninst + 1]; }
 
 static const double LSERK_ALPHA[3][6][7] = {
     // tabulated low-storage RK coefficients, teal's table (src/simulation/advance.c:50-75)
@@ -251,11 +273,12 @@ static void free_ctx(tg_ctx *c)
         cudaEventDestroy(p.second.second);
     }
     if (c->graph) cudaGraphExecDestroy(c->graph);
-    void *ptrs[] = {c->lr, c->slot_nbr, c->slot_face, c->slot_cnt, c->owner, c->bface_ent, c->volume,
-                    c->proj, c->eps2, c->gb.area, c->gb.basis, c->gb.offl, c->gb.offr, c->gb.corr,
-                    c->gb.slot_w, c->gb.slot_off, c->gb.area32, c->gb.basis32, c->gb.offl32,
-                    c->gb.offr32, c->gb.corr32, c->gb.slot_w32, c->gb.slot_off32, c->q, c->U0, c->R, c->qs,
-                    c->grad, c->G, c->part_dt, c->part_res, c->st, c->aos};
+    void *ptrs[] = {c->lr, c->slot_nbr, c->slot_face, c->slot_cnt, c->owner, c->bface_ent, c->bkind, c->bctx,
+                    c->volume, c->proj, c->eps2, c->gb.area, c->gb.basis, c->gb.offl, c->gb.offr, c->gb.corr,
+                    c->gb.slot_w, c->gb.slot_off, c->gb.area32, c->gb.basis32, c->gb.offl32, c->gb.offr32,
+                    c->gb.corr32, c->gb.slot_w32, c->gb.slot_off32, c->q, c->U0, c->R, c->qs, c->grad, c->G,
+                    c->dtc, c->part_min, c->part_sum, c->sd, c->si, c->aos, c->rowmap, c->cell_inst,
+                    c->inst_cell_off, c->piece_beg, c->inst_piece_off, c->sum_volume};
     for (void *p : ptrs) {
         if (p) cudaFree(p);
     }
@@ -264,7 +287,8 @@ static void free_ctx(tg_ctx *c)
     for (void *p : gp) {
         if (p) cudaFree(p);
     }
-    if (c->st_host) cudaFreeHost(c->st_host);
+    if (c->hd) cudaFreeHost(c->hd);
+    if (c->hi) cudaFreeHost(c->hi);
     if (c->pinned) cudaFreeHost(c->pinned);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
@@ -310,6 +334,24 @@ struct Launch {
     }
 };
 
+// ---- mesh input: one teal mesh, or several packed into one arena -------------------------------
+
+// Arena arrays in teal's layouts plus what the device upload needs beyond them.
+struct MeshInput {
+    tg_mesh m{};                    // views into the vectors below, or the caller's arrays
+    std::vector<int> face_cell;     // merged arrays (batches only)
+    std::vector<double> area, basis, weight, offset, correction, volume, projection;
+    std::vector<int> owner;         // periodic ghost (row - off_boundary_cells) -> inner owner
+    std::vector<int> bent;          // boundary face (f - F_in) -> boundary index
+    std::vector<int> bkind;         // boundary index -> TG_BC_*
+    std::vector<double> bctx;       // boundary index -> [5]
+    std::vector<double> eps2;       // Venkatakrishnan parameter per inner cell (empty: none)
+    std::vector<int> inst_cell_off; // inner cells per instance
+    std::vector<double> sum_volume; // per instance
+    std::vector<int> inst_row_off;  // teal rows per instance
+    std::vector<int> rowmap;        // teal row -> arena row (periodic ghosts: the owner's row)
+};
+
 // periodic ghost -> owner cell, by matching each receive tag with the send posted under it
 // (the single-process halo exchange of src/equations/exchange.c:8-36 and src/mesh/create.c:351-440)
 static int build_owner_map(const tg_mesh *m, std::vector<int> &owner)
@@ -353,14 +395,6 @@ static int build_owner_map(const tg_mesh *m, std::vector<int> &owner)
     return TG_OK;
 }
 
-template <typename T>
-static int upload(T **dst, const T *src, size_t n, cudaStream_t st)
-{
-    TRY(dalloc(dst, n));
-    if (n) CU(cudaMemcpyAsync(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice, st));
-    return TG_OK;
-}
-
 static int validate(const tg_mesh *m, const tg_equations *e)
 {
     if (!m || !e) return fail(TG_ERR_INVALID, "null mesh or equations");
@@ -392,7 +426,6 @@ static int validate(const tg_mesh *m, const tg_equations *e)
     int nb = m->off_boundary_entities - m->num_inner_entities;
     if (nb != e->num_boundaries)
         return fail(TG_ERR_INVALID, "boundary count %d does not match the mesh (%d)", e->num_boundaries, nb);
-    if (nb > MAX_BOUNDARIES) return fail(TG_ERR_INVALID, "more than %d boundaries", MAX_BOUNDARIES);
     for (int i = 0; i < nb; i++) {
         int k = e->boundary_kind ? e->boundary_kind[i] : 0;
         if (k < TG_BC_SYMMETRY || k > TG_BC_ADIABATIC_WALL)
@@ -400,6 +433,197 @@ static int validate(const tg_mesh *m, const tg_equations *e)
         if (k == TG_BC_ADIABATIC_WALL && e->physics != TG_NAVIERSTOKES)
             return fail(TG_ERR_INVALID, "adiabatic wall needs the Navier-Stokes equations");
     }
+    return TG_OK;
+}
+
+// boundary faces of one mesh -> its boundary index; boundary kinds and contexts
+static int boundary_tables(const tg_mesh *m, const tg_equations *e, std::vector<int> &bent, std::vector<int> &bkind,
+                           std::vector<double> &bctx)
+{
+    int F_in = m->num_inner_faces, F_bd = m->off_boundary_faces;
+    bent.assign(F_bd - F_in, -1);
+    bkind.resize(e->num_boundaries);
+    bctx.assign(5 * (size_t)e->num_boundaries, 0.0);
+    for (int i = 0; i < e->num_boundaries; i++) {
+        bkind[i] = e->boundary_kind[i];
+        for (int v = 0; v < 5; v++) bctx[5 * i + v] = e->boundary_context ? e->boundary_context[5 * i + v] : 0.0;
+        int ent = m->num_inner_entities + i;
+        int beg = m->entity_face_off[ent], end = m->entity_face_off[ent + 1];
+        if (beg < F_in || end > F_bd || beg > end)
+            return fail(TG_ERR_INVALID, "boundary entity %d face range [%d, %d) invalid", i, beg, end);
+        for (int f = beg; f < end; f++) bent[f - F_in] = i;
+    }
+    for (size_t i = 0; i < bent.size(); i++) {
+        if (bent[i] < 0) return fail(TG_ERR_INVALID, "boundary face %zu belongs to no boundary", i + F_in);
+        int r = m->face_cell[2 * (F_in + i) + 1];
+        if (r < m->num_inner_cells || r >= m->off_boundary_cells)
+            return fail(TG_ERR_INVALID, "boundary face right cell out of range");
+    }
+    return TG_OK;
+}
+
+static void limiter_parameter(const tg_mesh *m, const tg_equations *e, double *eps2)
+{
+    for (int i = 0; i < m->num_inner_cells; i++) {
+        if (e->limiter_parameter) {
+            eps2[i] = e->limiter_parameter[i];
+        }
+        else {  // eps^2 = (K * V^(1/3))^3, src/equations/limiter.c:8-21
+            double x = e->limiter_coefficient * cbrt(m->cell_volume[i]);
+            eps2[i] = (x * x) * x;
+        }
+    }
+}
+
+static int single_input(const tg_mesh *m, const tg_equations *e, MeshInput &in)
+{
+    TRY(validate(m, e));
+    in.m = *m;
+    TRY(build_owner_map(m, in.owner));
+    TRY(boundary_tables(m, e, in.bent, in.bkind, in.bctx));
+    if (e->limiter == TG_LIMITER_VENKATAKRISHNAN) {
+        in.eps2.resize(m->num_inner_cells);
+        limiter_parameter(m, e, in.eps2.data());
+    }
+    in.inst_cell_off = {0, m->num_inner_cells};
+    in.sum_volume = {m->sum_volume};
+    in.inst_row_off = {0, m->num_cells};
+    in.rowmap.resize(m->num_cells);
+    for (int r = 0; r < m->num_cells; r++) {
+        in.rowmap[r] = r < m->off_boundary_cells ? r : in.owner[r - m->off_boundary_cells];
+    }
+    return TG_OK;
+}
+
+// Pack several meshes into one arena: all inner cells (instance order), then all boundary ghosts,
+// then all periodic ghosts; faces likewise (inner, boundary, periodic). Every kernel then runs over
+// the arena as over one mesh whose instances are disconnected pieces.
+static int merged_input(const tg_mesh *ms, const tg_equations *es, int num, MeshInput &in)
+{
+    if (num <= 0) return fail(TG_ERR_INVALID, "a batch needs at least one instance");
+    const tg_equations &e0 = es[0];
+    for (int i = 0; i < num; i++) {
+        TRY(validate(&ms[i], &es[i]));
+        const tg_equations &e = es[i];
+        if (e.physics != e0.physics || e.space_order != e0.space_order || e.convective != e0.convective ||
+            e.viscous != e0.viscous || e.limiter != e0.limiter || e.property[0] != e0.property[0] ||
+            e.property[1] != e0.property[1] || e.property[2] != e0.property[2])
+            return fail(TG_ERR_INVALID, "batch instance %d differs in equations, schemes or properties", i);
+    }
+    long C = 0, NB = 0, NP = 0, Fi = 0, Fb = 0, Fp = 0, nbnd = 0, rows = 0;
+    for (int i = 0; i < num; i++) {
+        const tg_mesh &m = ms[i];
+        C += m.num_inner_cells;
+        NB += m.off_boundary_cells - m.num_inner_cells;
+        NP += m.num_cells - m.off_boundary_cells;
+        Fi += m.num_inner_faces;
+        Fb += m.off_boundary_faces - m.num_inner_faces;
+        Fp += m.num_faces - m.off_boundary_faces;
+        nbnd += es[i].num_boundaries;
+        rows += m.num_cells;
+    }
+    if (C + NB + NP > 2000000000L || Fi + Fb + Fp > 2000000000L)
+        return fail(TG_ERR_INVALID, "batch exceeds 2^31 cells or faces");
+    const long F = Fi + Fb + Fp;
+    in.face_cell.resize(2 * F);
+    in.area.resize(F);
+    in.basis.resize(9 * F);
+    in.weight.resize(6 * F);
+    in.offset.resize(6 * F);
+    bool visc = e0.viscous == TG_VISCOUS_CENTRAL;
+    if (visc) in.correction.resize(4 * F);
+    in.volume.assign(C + NB + NP, 0.0);
+    in.projection.assign(3 * (C + NB + NP), 0.0);
+    in.owner.resize(NP);
+    in.bent.resize(Fb);
+    in.bkind.clear();
+    in.bctx.clear();
+    if (e0.limiter == TG_LIMITER_VENKATAKRISHNAN) in.eps2.resize(C);
+    in.inst_cell_off.assign(1, 0);
+    in.sum_volume.clear();
+    in.inst_row_off.assign(1, 0);
+    in.rowmap.resize(rows);
+
+    long c0 = 0, b0 = 0, p0 = 0, fi0 = 0, fb0 = 0, fp0 = 0, bnd0 = 0, row0 = 0;
+    for (int i = 0; i < num; i++) {
+        const tg_mesh &m = ms[i];
+        const tg_equations &e = es[i];
+        std::vector<int> owner, bent, bkind;
+        std::vector<double> bctx;
+        TRY(build_owner_map(&m, owner));
+        TRY(boundary_tables(&m, &e, bent, bkind, bctx));
+        const int Ci = m.num_inner_cells, OBi = m.off_boundary_cells;
+        auto cell = [&](int r) -> long {
+            if (r < Ci) return c0 + r;
+            if (r < OBi) return C + b0 + (r - Ci);
+            return C + NB + p0 + (r - OBi);
+        };
+        auto copy_face = [&](int f, long g) {
+            in.face_cell[2 * g] = (int)cell(m.face_cell[2 * f]);
+            in.face_cell[2 * g + 1] = (int)cell(m.face_cell[2 * f + 1]);
+            in.area[g] = m.face_area[f];
+            memcpy(&in.basis[9 * g], m.face_basis + 9 * (size_t)f, 9 * sizeof(double));
+            memcpy(&in.weight[6 * g], m.face_weight + 6 * (size_t)f, 6 * sizeof(double));
+            memcpy(&in.offset[6 * g], m.face_offset + 6 * (size_t)f, 6 * sizeof(double));
+            if (visc) memcpy(&in.correction[4 * g], m.face_correction + 4 * (size_t)f, 4 * sizeof(double));
+        };
+        for (int f = 0; f < m.num_inner_faces; f++) copy_face(f, fi0 + f);
+        for (int f = m.num_inner_faces; f < m.off_boundary_faces; f++) {
+            copy_face(f, Fi + fb0 + (f - m.num_inner_faces));
+            in.bent[fb0 + (f - m.num_inner_faces)] = (int)(bnd0 + bent[f - m.num_inner_faces]);
+        }
+        for (int f = m.off_boundary_faces; f < m.num_faces; f++) copy_face(f, Fi + Fb + fp0 + (f - m.off_boundary_faces));
+        for (int r = 0; r < m.num_cells; r++) {
+            long a = cell(r);
+            in.volume[a] = m.cell_volume[r];
+            memcpy(&in.projection[3 * a], m.cell_projection + 3 * (size_t)r, 3 * sizeof(double));
+        }
+        for (int p = 0; p < m.num_cells - OBi; p++) in.owner[p0 + p] = (int)(c0 + owner[p]);
+        in.bkind.insert(in.bkind.end(), bkind.begin(), bkind.end());
+        in.bctx.insert(in.bctx.end(), bctx.begin(), bctx.end());
+        if (!in.eps2.empty()) limiter_parameter(&m, &e, &in.eps2[c0]);
+        for (int r = 0; r < m.num_cells; r++) {
+            in.rowmap[row0 + r] = (int)(r < OBi ? cell(r) : c0 + owner[r - OBi]);
+        }
+        c0 += Ci;
+        b0 += OBi - Ci;
+        p0 += m.num_cells - OBi;
+        fi0 += m.num_inner_faces;
+        fb0 += m.off_boundary_faces - m.num_inner_faces;
+        fp0 += m.num_faces - m.off_boundary_faces;
+        bnd0 += e.num_boundaries;
+        row0 += m.num_cells;
+        in.inst_cell_off.push_back((int)c0);
+        in.sum_volume.push_back(m.sum_volume);
+        in.inst_row_off.push_back((int)row0);
+    }
+    tg_mesh &v = in.m;
+    memset(&v, 0, sizeof(v));
+    v.num_cells = (int)(C + NB + NP);
+    v.num_inner_cells = (int)C;
+    v.off_boundary_cells = (int)(C + NB);
+    v.off_periodic_cells = v.num_cells;
+    v.cell_volume = in.volume.data();
+    v.cell_projection = in.projection.data();
+    v.num_faces = (int)F;
+    v.num_inner_faces = (int)Fi;
+    v.off_boundary_faces = (int)(Fi + Fb);
+    v.face_cell = in.face_cell.data();
+    v.face_area = in.area.data();
+    v.face_basis = in.basis.data();
+    v.face_weight = in.weight.data();
+    v.face_offset = in.offset.data();
+    v.face_correction = visc ? in.correction.data() : nullptr;
+    return TG_OK;
+}
+
+// ---- device upload ------------------------------------------------------------------------------
+
+template <typename T>
+static int upload(T **dst, const T *src, size_t n, cudaStream_t st)
+{
+    TRY(dalloc(dst, n));
+    if (n) CU(cudaMemcpyAsync(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice, st));
     return TG_OK;
 }
 
@@ -430,19 +654,27 @@ static int to_float(const double *a, float *b, size_t n, cudaStream_t st)
     return TG_OK;
 }
 
-extern "C" int tg_create(const tg_mesh *m, const tg_equations *e, int precision, tg_ctx **out)
+// AoS host array [n][k] -> device SoA [k][n] through a device temporary
+static int upload_soa(double **dst, const double *src, size_t n, int k, double *tmp, cudaStream_t st)
 {
-    if (!out) return fail(TG_ERR_INVALID, "null output pointer");
+    TRY(dalloc(dst, (size_t)k * n));
+    if (!n) return TG_OK;
+    CU(cudaMemcpyAsync(tmp, src, (size_t)k * n * sizeof(double), cudaMemcpyHostToDevice, st));
+    k_transpose<double><<<grid_of((long)n), BLOCK, 0, st>>>((int)n, k, tmp, *dst);
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(st));  // tmp is reused by the next upload
+    return TG_OK;
+}
+
+static int create_ctx(MeshInput &in, const tg_equations *e, int precision, tg_ctx **out)
+{
     *out = nullptr;
-    TRY(validate(m, e));
     if (precision != TG_PRECISION_FP64 && precision != TG_PRECISION_FP32_FLUX)
         return fail(TG_ERR_INVALID, "invalid precision %d", precision);
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
         return fail(TG_ERR_NO_DEVICE, "no CUDA device available");
-
-    std::vector<int> owner;
-    TRY(build_owner_map(m, owner));
+    const tg_mesh *m = &in.m;
 
     tg_ctx *c = new tg_ctx();
     int rc = [&]() -> int {
@@ -457,8 +689,6 @@ extern "C" int tg_create(const tg_mesh *m, const tg_equations *e, int precision,
         s.F = m->num_faces;
         s.F_in = m->num_inner_faces;
         s.F_bd = m->off_boundary_faces;
-        c->num_cells = m->num_cells;
-        c->off_boundary_cells = m->off_boundary_cells;
         c->num_periodic = m->num_cells - m->off_boundary_cells;
         c->physics = e->physics;
         c->order = e->space_order;
@@ -467,32 +697,33 @@ extern "C" int tg_create(const tg_mesh *m, const tg_equations *e, int precision,
         c->limiter = e->limiter;
         c->precision = precision;
         for (int i = 0; i < 3; i++) c->prop[i] = e->property[i];
-        c->sum_volume = m->sum_volume;
 
-        // boundary table and boundary face -> boundary index
-        c->bt.num = e->num_boundaries;
-        std::vector<int> bent(s.F_bd - s.F_in, -1);
-        for (int i = 0; i < e->num_boundaries; i++) {
-            c->bt.kind[i] = e->boundary_kind[i];
-            for (int v = 0; v < 5; v++) c->bt.ctx[i][v] = e->boundary_context ? e->boundary_context[5 * i + v] : 0.0;
-            int ent = m->num_inner_entities + i;
-            int beg = m->entity_face_off[ent], end = m->entity_face_off[ent + 1];
-            if (beg < s.F_in || end > s.F_bd || beg > end)
-                return fail(TG_ERR_INVALID, "boundary entity %d face range [%d, %d) invalid", i, beg, end);
-            for (int f = beg; f < end; f++) bent[f - s.F_in] = i;
+        // instances and reduction pieces
+        c->ninst = (int)in.inst_cell_off.size() - 1;
+        c->inst_row_off = in.inst_row_off;
+        c->h_inst_cell_off = in.inst_cell_off;
+        std::vector<int> cell_inst(s.C), piece_beg, inst_piece_off(1, 0);
+        for (int i = 0; i < c->ninst; i++) {
+            for (int x = in.inst_cell_off[i]; x < in.inst_cell_off[i + 1]; x++) cell_inst[x] = i;
+            for (int x = in.inst_cell_off[i]; x < in.inst_cell_off[i + 1]; x += PIECE) piece_beg.push_back(x);
+            inst_piece_off.push_back((int)piece_beg.size());
         }
-        for (size_t i = 0; i < bent.size(); i++) {
-            if (bent[i] < 0) return fail(TG_ERR_INVALID, "boundary face %zu belongs to no boundary", i + s.F_in);
-            int r = m->face_cell[2 * (s.F_in + i) + 1];
-            if (r < s.C || r >= s.N) return fail(TG_ERR_INVALID, "boundary face right cell out of range");
-        }
+        c->npieces = (int)piece_beg.size();
+        piece_beg.push_back(s.C);
+        TRY(upload(&c->cell_inst, cell_inst.data(), cell_inst.size(), st));
+        TRY(upload(&c->inst_cell_off, in.inst_cell_off.data(), in.inst_cell_off.size(), st));
+        TRY(upload(&c->piece_beg, piece_beg.data(), piece_beg.size(), st));
+        TRY(upload(&c->inst_piece_off, inst_piece_off.data(), inst_piece_off.size(), st));
+        TRY(upload(&c->sum_volume, in.sum_volume.data(), in.sum_volume.size(), st));
+        TRY(upload(&c->rowmap, in.rowmap.data(), in.rowmap.size(), st));
+        c->seg = Segments{c->ninst, c->npieces, c->cell_inst, c->inst_cell_off, c->piece_beg, c->inst_piece_off,
+                          c->sum_volume};
 
         // raw teal arrays -> device temporaries
-        int *d_face_cell = nullptr, *d_owner_tmp = nullptr, *d_err = nullptr, *d_cnt = nullptr;
+        int *d_face_cell = nullptr, *d_err = nullptr, *d_cnt = nullptr;
         double *d_weight = nullptr, *d_offset = nullptr, *d_tmp = nullptr;
         auto cleanup = [&]() {
             cudaFree(d_face_cell);
-            cudaFree(d_owner_tmp);
             cudaFree(d_err);
             cudaFree(d_cnt);
             cudaFree(d_weight);
@@ -501,15 +732,15 @@ extern "C" int tg_create(const tg_mesh *m, const tg_equations *e, int precision,
         };
         int r2 = [&]() -> int {
             TRY(upload(&d_face_cell, m->face_cell, 2 * (size_t)s.F, st));
-            TRY(upload(&c->owner, owner.data(), owner.size(), st));
+            TRY(upload(&c->owner, in.owner.data(), in.owner.size(), st));
             TRY(dalloc(&d_err, 1));
             CU(cudaMemsetAsync(d_err, 0, sizeof(int), st));
             TRY(dalloc(&c->lr, s.F));
-            k_redirect<<<grid_of(s.F), BLOCK, 0, st>>>(s.F, s.F_bd, m->off_boundary_cells, d_face_cell,
-                                                       c->owner, (int)owner.size(), c->lr, d_err);
+            k_redirect<<<grid_of(s.F), BLOCK, 0, st>>>(s.F, s.F_bd, m->off_boundary_cells, d_face_cell, c->owner,
+                                                       (int)in.owner.size(), c->lr, d_err);
             CU(cudaGetLastError());
 
-            // slots
+            // per-cell slot lists: count, scatter, sort by face (integer work on the device)
             TRY(dalloc(&d_cnt, 2 * (size_t)s.C));
             CU(cudaMemsetAsync(d_cnt, 0, 2 * sizeof(int) * s.C, st));
             TRY(dalloc(&c->slot_face, MAX_SLOTS * (size_t)s.C));
@@ -528,13 +759,8 @@ extern "C" int tg_create(const tg_mesh *m, const tg_equations *e, int precision,
 
             // face geometry, structure of arrays
             TRY(upload(&c->gb.area, m->face_area, s.F, st));
-            TRY(dalloc(&c->gb.basis, 9 * (size_t)s.F));
-            TRY(dalloc(&c->gb.offl, 3 * (size_t)s.F));
-            TRY(dalloc(&c->gb.offr, 3 * (size_t)s.F));
-            TRY(dalloc(&d_tmp, 9 * (size_t)s.F));
-            CU(cudaMemcpyAsync(d_tmp, m->face_basis, 9 * sizeof(double) * s.F, cudaMemcpyHostToDevice, st));
-            k_transpose<double><<<grid_of(s.F), BLOCK, 0, st>>>(s.F, 9, d_tmp, c->gb.basis);
-            // offsets: AoS [F][2][3] -> left [3][F], right [3][F]
+            TRY(dalloc(&d_tmp, 9 * (size_t)s.F > 3 * (size_t)s.C ? 9 * (size_t)s.F : 3 * (size_t)s.C));
+            TRY(upload_soa(&c->gb.basis, m->face_basis, s.F, 9, d_tmp, st));
             std::vector<double> ol(3 * (size_t)s.F), orr(3 * (size_t)s.F);
             for (int f = 0; f < s.F; f++) {
                 for (int d = 0; d < 3; d++) {
@@ -542,42 +768,21 @@ extern "C" int tg_create(const tg_mesh *m, const tg_equations *e, int precision,
                     orr[(size_t)f * 3 + d] = m->face_offset[(size_t)f * 6 + 3 + d];
                 }
             }
-            CU(cudaStreamSynchronize(st));  // d_tmp reuse
-            CU(cudaMemcpyAsync(d_tmp, ol.data(), 3 * sizeof(double) * s.F, cudaMemcpyHostToDevice, st));
-            k_transpose<double><<<grid_of(s.F), BLOCK, 0, st>>>(s.F, 3, d_tmp, c->gb.offl);
-            CU(cudaStreamSynchronize(st));
-            CU(cudaMemcpyAsync(d_tmp, orr.data(), 3 * sizeof(double) * s.F, cudaMemcpyHostToDevice, st));
-            k_transpose<double><<<grid_of(s.F), BLOCK, 0, st>>>(s.F, 3, d_tmp, c->gb.offr);
+            TRY(upload_soa(&c->gb.offl, ol.data(), s.F, 3, d_tmp, st));
+            TRY(upload_soa(&c->gb.offr, orr.data(), s.F, 3, d_tmp, st));
             if (e->viscous == TG_VISCOUS_CENTRAL) {
-                TRY(dalloc(&c->gb.corr, 4 * (size_t)s.F));
-                CU(cudaStreamSynchronize(st));
-                CU(cudaMemcpyAsync(d_tmp, m->face_correction, 4 * sizeof(double) * s.F,
-                                   cudaMemcpyHostToDevice, st));
-                k_transpose<double><<<grid_of(s.F), BLOCK, 0, st>>>(s.F, 4, d_tmp, c->gb.corr);
+                TRY(upload_soa(&c->gb.corr, m->face_correction, s.F, 4, d_tmp, st));
             }
-            CU(cudaGetLastError());
 
-            // cells
+            // cells and boundaries
             TRY(upload(&c->volume, m->cell_volume, s.C, st));
-            TRY(dalloc(&c->proj, 3 * (size_t)s.C));
-            CU(cudaStreamSynchronize(st));
-            CU(cudaMemcpyAsync(d_tmp, m->cell_projection, 3 * sizeof(double) * s.C, cudaMemcpyHostToDevice, st));
-            k_transpose<double><<<grid_of(s.C), BLOCK, 0, st>>>(s.C, 3, d_tmp, c->proj);
-            if (e->limiter == TG_LIMITER_VENKATAKRISHNAN) {
-                std::vector<double> eps2(s.C);
-                for (int i = 0; i < s.C; i++) {
-                    if (e->limiter_parameter) {
-                        eps2[i] = e->limiter_parameter[i];
-                    }
-                    else {  // eps^2 = (K * V^(1/3))^3, src/equations/limiter.c:8-21
-                        double x = e->limiter_coefficient * cbrt(m->cell_volume[i]);
-                        eps2[i] = (x * x) * x;
-                    }
-                }
-                TRY(upload(&c->eps2, eps2.data(), s.C, st));
-                CU(cudaStreamSynchronize(st));
+            TRY(upload_soa(&c->proj, m->cell_projection, s.C, 3, d_tmp, st));
+            if (!in.eps2.empty()) TRY(upload(&c->eps2, in.eps2.data(), s.C, st));
+            if (s.F_bd > s.F_in) {
+                TRY(upload(&c->bface_ent, in.bent.data(), in.bent.size(), st));
+                TRY(upload(&c->bkind, in.bkind.data(), in.bkind.size(), st));
+                TRY(upload(&c->bctx, in.bctx.data(), in.bctx.size(), st));
             }
-            if (s.F_bd > s.F_in) TRY(upload(&c->bface_ent, bent.data(), bent.size(), st));
             CU(cudaGetLastError());
 
             int h_err = 0;
@@ -601,10 +806,10 @@ extern "C" int tg_create(const tg_mesh *m, const tg_equations *e, int precision,
             TRY(to_float(c->gb.slot_w, c->gb.slot_w32, 3 * MAX_SLOTS * (size_t)s.C, st));
             TRY(to_float(c->gb.slot_off, c->gb.slot_off32, 3 * MAX_SLOTS * (size_t)s.C, st));
         }
-        c->g64 = Geometry<double>{c->lr,       c->gb.area, c->gb.basis, c->gb.offl,   c->gb.offr,   c->gb.corr,
+        c->g64 = Geometry<double>{c->lr,       c->gb.area,  c->gb.basis,   c->gb.offl,   c->gb.offr,   c->gb.corr,
                                   c->slot_nbr, c->slot_face, c->slot_cnt, c->gb.slot_w, c->gb.slot_off};
-        c->g32 = Geometry<float>{c->lr,       c->gb.area32, c->gb.basis32, c->gb.offl32,   c->gb.offr32,
-                                 c->gb.corr32, c->slot_nbr, c->slot_face, c->slot_cnt, c->gb.slot_w32,
+        c->g32 = Geometry<float>{c->lr,         c->gb.area32, c->gb.basis32, c->gb.offl32,   c->gb.offr32,
+                                 c->gb.corr32, c->slot_nbr,  c->slot_face,  c->slot_cnt, c->gb.slot_w32,
                                  c->gb.slot_off32};
 
         // state
@@ -613,20 +818,36 @@ extern "C" int tg_create(const tg_mesh *m, const tg_equations *e, int precision,
         CU(cudaMemsetAsync(c->q, 0, 5 * sizeof(double) * s.N, st));
         TRY(dalloc(&c->U0, 5 * (size_t)s.C));
         TRY(dalloc(&c->R, 5 * (size_t)s.C));
+        CU(cudaMemsetAsync(c->R, 0, 5 * sizeof(double) * s.C, st));
         if (c->order == 2) {
             CU(cudaMalloc(&c->grad, 20 * rsz * s.C));
         }
         CU(cudaMalloc(&c->G, FLUX_REC * rsz * s.F));
-        c->nblk = grid_of(s.C);
-        TRY(dalloc(&c->part_dt, c->nblk));
-        TRY(dalloc(&c->part_res, 5 * (size_t)c->nblk));
-        TRY(dalloc(&c->st, 1));
-        CU(cudaMallocHost(&c->st_host, sizeof(StepState)));
-        memset(c->st_host, 0, sizeof(StepState));
-        c->st_host->max_step = DBL_MAX;
-        c->st_host->max_time = DBL_MAX;
-        CU(cudaMemcpyAsync(c->st, c->st_host, sizeof(StepState), cudaMemcpyHostToDevice, st));
-        c->aos_len = (size_t)15 * (c->num_cells > s.F ? c->num_cells : s.F);
+        TRY(dalloc(&c->dtc, s.C));
+        CU(cudaMemsetAsync(c->dtc, 0, sizeof(double) * s.C, st));
+        TRY(dalloc(&c->part_min, c->npieces));
+        TRY(dalloc(&c->part_sum, 5 * (size_t)c->npieces));
+        TRY(dalloc(&c->sd, (size_t)SD_COUNT * c->ninst));
+        TRY(dalloc(&c->si, (size_t)SI_COUNT * c->ninst + 2));
+        CU(cudaMallocHost(&c->hd, sizeof(double) * SD_COUNT * c->ninst));
+        CU(cudaMallocHost(&c->hi, sizeof(int) * (SI_COUNT * c->ninst + 2)));
+        memset(c->hd, 0, sizeof(double) * SD_COUNT * c->ninst);
+        memset(c->hi, 0, sizeof(int) * (SI_COUNT * c->ninst + 2));
+        for (int i = 0; i < c->ninst; i++) {
+            hd_at(c, SD_MAX_STEP, i) = DBL_MAX;
+            hd_at(c, SD_MAX_TIME, i) = DBL_MAX;
+            hi_at(c, SI_VARIABLE, i) = -1;
+            hi_at(c, SI_MAX_ITER, i) = 0x7fffffff;
+            hi_at(c, SI_ACTIVE, i) = 1;
+        }
+        int n = c->ninst;
+        c->st = Steps{c->sd + SD_TIME * n,     c->sd + SD_STEP * n,      c->sd + SD_STEP0 * n,
+                      c->sd + SD_MAX_STEP * n, c->sd + SD_MAX_TIME * n,  c->sd + SD_THRESHOLD * n,
+                      c->sd + SD_RESIDUAL * n, c->si + SI_VARIABLE * n,  c->si + SI_ITER * n,
+                      c->si + SI_MAX_ITER * n, c->si + SI_ACTIVE * n,    c->si + SI_COUNT * n,
+                      c->si + SI_COUNT * n + 1, 0};
+        // the residual block is [ninst][5] inside the doubles: SD_RESIDUAL * n .. + 5 n
+        c->aos_len = (size_t)15 * ((size_t)m->num_cells > (size_t)s.F ? (size_t)m->num_cells : (size_t)s.F);
         TRY(dalloc(&c->aos, c->aos_len));
         CU(cudaStreamSynchronize(st));
         return TG_OK;
@@ -639,6 +860,32 @@ extern "C" int tg_create(const tg_mesh *m, const tg_equations *e, int precision,
         return rc;
     }
     *out = c;
+    return TG_OK;
+}
+
+extern "C" int tg_create(const tg_mesh *m, const tg_equations *e, int precision, tg_ctx **out)
+{
+    if (!out) return fail(TG_ERR_INVALID, "null output pointer");
+    *out = nullptr;
+    MeshInput in;
+    TRY(single_input(m, e, in));
+    return create_ctx(in, e, precision, out);
+}
+
+extern "C" int tg_batch_create(const tg_mesh *meshes, const tg_equations *eqns, int num, int precision,
+                               tg_ctx **out)
+{
+    if (!out || !meshes || !eqns) return fail(TG_ERR_INVALID, "null argument");
+    *out = nullptr;
+    MeshInput in;
+    TRY(merged_input(meshes, eqns, num, in));
+    return create_ctx(in, &eqns[0], precision, out);
+}
+
+extern "C" int tg_batch_size(tg_ctx *c, int *num)
+{
+    if (!c || !num) return fail(TG_ERR_INVALID, "null argument");
+    *num = c->ninst;
     return TG_OK;
 }
 
@@ -710,24 +957,47 @@ static int d2h(tg_ctx *c, double *dst, const double *src, size_t n)
     return TG_OK;
 }
 
-extern "C" int tg_set_primitive(tg_ctx *c, const double *prim)
+static int set_rows(tg_ctx *c, int inst, const double *prim, double *q)
+{
+    if (inst < 0 || inst >= c->ninst) return fail(TG_ERR_INVALID, "invalid instance %d", inst);
+    int row0 = c->h_inst_cell_off[inst];
+    int n = c->h_inst_cell_off[inst + 1] - row0;
+    TRY(h2d(c, c->aos, prim, 5 * (size_t)n));
+    k_rows_aos_to_soa<<<grid_of(n), BLOCK, 0, c->stream>>>(n, row0, c->s.N, c->aos, q);
+    CU(cudaGetLastError());
+    return TG_OK;
+}
+
+extern "C" int tg_batch_set_primitive(tg_ctx *c, int inst, const double *prim)
 {
     if (!c || !prim) return fail(TG_ERR_INVALID, "null argument");
-    TRY(h2d(c, c->aos, prim, 5 * (size_t)c->s.C));
-    k_prim_aos_to_soa<<<grid_of(c->s.C), BLOCK, 0, c->stream>>>(c->s.C, c->s.N, c->aos, c->q);
-    CU(cudaGetLastError());
+    TRY(set_rows(c, inst, prim, c->q));
     c->prepared = false;
     return TG_OK;
 }
 
-extern "C" int tg_get_primitive(tg_ctx *c, double *prim)
+extern "C" int tg_batch_get_primitive(tg_ctx *c, int inst, double *prim)
 {
     if (!c || !prim) return fail(TG_ERR_INVALID, "null argument");
-    k_prim_soa_to_aos<<<grid_of(c->num_cells), BLOCK, 0, c->stream>>>(c->s.N, c->num_cells, c->s.N, c->owner,
-                                                                        c->q, c->aos);
+    if (inst < 0 || inst >= c->ninst) return fail(TG_ERR_INVALID, "invalid instance %d", inst);
+    int r0 = c->inst_row_off[inst];
+    int n = c->inst_row_off[inst + 1] - r0;
+    k_rows_gather<<<grid_of(n), BLOCK, 0, c->stream>>>(n, c->rowmap + r0, c->s.N, c->q, c->aos);
     CU(cudaGetLastError());
-    TRY(d2h(c, prim, c->aos, 5 * (size_t)c->num_cells));
+    TRY(d2h(c, prim, c->aos, 5 * (size_t)n));
     return TG_OK;
+}
+
+extern "C" int tg_set_primitive(tg_ctx *c, const double *prim)
+{
+    if (c && c->ninst != 1) return fail(TG_ERR_INVALID, "a batch takes its state per instance");
+    return tg_batch_set_primitive(c, 0, prim);
+}
+
+extern "C" int tg_get_primitive(tg_ctx *c, double *prim)
+{
+    if (c && c->ninst != 1) return fail(TG_ERR_INVALID, "a batch gives its state per instance");
+    return tg_batch_get_primitive(c, 0, prim);
 }
 
 // ---- kernel sequencing -----------------------------------------------------------------------
@@ -755,7 +1025,7 @@ static int run_boundary(tg_ctx *c, double *q)
     int nbf = c->s.F_bd - c->s.F_in;
     if (nbf <= 0) return TG_OK;
     Launch l(c, TG_PROF_BOUNDARY);
-    k_boundary<<<grid_of(nbf), BLOCK, 0, c->stream>>>(c->s, c->lr, c->gb.basis, c->bface_ent, c->bt, q,
+    k_boundary<<<grid_of(nbf), BLOCK, 0, c->stream>>>(c->s, c->lr, c->gb.basis, c->bface_ent, c->bkind, c->bctx, q,
                                                       c->prop[0]);
     CU(cudaGetLastError());
     return TG_OK;
@@ -831,35 +1101,31 @@ static int run_face(tg_ctx *c, const double *q)
     return TG_OK;
 }
 
+template <int MODE, bool NS, typename GT>
+static void launch_cell_t(tg_ctx *c, double alpha, int last, double *q, double *Rout)
+{
+    CellData cd{c->volume, c->proj, c->eps2};
+    k_cell<MODE, NS, GT><<<(c->s.C + CELL_BLOCK - 1) / CELL_BLOCK, CELL_BLOCK, 0, c->stream>>>(c->s, c->slot_face, c->slot_cnt, cd,
+                                                                  (const GT *)c->G, c->U0, q, Rout, c->seg,
+                                                                  c->st, alpha, last, props_of(c), c->dtc);
+}
+
 template <int MODE>
 static int launch_cell(tg_ctx *c, double alpha, int last, double *q, double *Rout)
 {
-    CellData cd{c->volume, c->proj, c->eps2};
-    dim3 grid(c->nblk);
-    Props p = props_of(c);
-    bool ns = is_ns(c);
     Launch l(c, TG_PROF_CELL);
+    bool ns = is_ns(c);
     if (c->precision == TG_PRECISION_FP64) {
-        const double *G = (const double *)c->G;
         if (ns)
-            k_cell<MODE, true, double><<<grid, BLOCK, 0, c->stream>>>(c->s, c->slot_face, c->slot_cnt, cd, G, c->U0,
-                                                                       q, Rout, c->st, alpha, last, p,
-                                                                       c->part_dt, c->part_res);
+            launch_cell_t<MODE, true, double>(c, alpha, last, q, Rout);
         else
-            k_cell<MODE, false, double><<<grid, BLOCK, 0, c->stream>>>(c->s, c->slot_face, c->slot_cnt, cd, G, c->U0,
-                                                                        q, Rout, c->st, alpha, last, p,
-                                                                        c->part_dt, c->part_res);
+            launch_cell_t<MODE, false, double>(c, alpha, last, q, Rout);
     }
     else {
-        const float *G = (const float *)c->G;
         if (ns)
-            k_cell<MODE, true, float><<<grid, BLOCK, 0, c->stream>>>(c->s, c->slot_face, c->slot_cnt, cd, G, c->U0,
-                                                                      q, Rout, c->st, alpha, last, p,
-                                                                      c->part_dt, c->part_res);
+            launch_cell_t<MODE, true, float>(c, alpha, last, q, Rout);
         else
-            k_cell<MODE, false, float><<<grid, BLOCK, 0, c->stream>>>(c->s, c->slot_face, c->slot_cnt, cd, G, c->U0,
-                                                                       q, Rout, c->st, alpha, last, p,
-                                                                       c->part_dt, c->part_res);
+            launch_cell_t<MODE, false, float>(c, alpha, last, q, Rout);
     }
     CU(cudaGetLastError());
     return TG_OK;
@@ -874,16 +1140,60 @@ static int run_fluxes(tg_ctx *c, double *q)
     return TG_OK;
 }
 
+// per-piece reductions of the cell steps (and of V R^2 with `res`)
+static int run_pieces(tg_ctx *c, int res)
+{
+    Launch l(c, TG_PROF_REDUCE);
+    k_piece_reduce<<<c->npieces, BLOCK, 0, c->stream>>>(c->seg, c->s.C, c->dtc, c->R, c->volume, res, c->part_min,
+                                                        c->part_sum);
+    CU(cudaGetLastError());
+    return TG_OK;
+}
+
 static int run_prepare(tg_ctx *c)
 {
     CellData cd{c->volume, c->proj, c->eps2};
     if (is_ns(c))
-        k_prepare<true><<<c->nblk, BLOCK, 0, c->stream>>>(c->s, cd, c->q, c->U0, props_of(c), c->part_dt);
+        k_prepare<true><<<grid_of(c->s.C), BLOCK, 0, c->stream>>>(c->s, cd, c->q, c->U0, props_of(c), c->dtc);
     else
-        k_prepare<false><<<c->nblk, BLOCK, 0, c->stream>>>(c->s, cd, c->q, c->U0, props_of(c), c->part_dt);
+        k_prepare<false><<<grid_of(c->s.C), BLOCK, 0, c->stream>>>(c->s, cd, c->q, c->U0, props_of(c), c->dtc);
     CU(cudaGetLastError());
+    TRY(run_pieces(c, 0));
     c->prepared = true;
     return TG_OK;
+}
+
+// ---- step bookkeeping transfers ---------------------------------------------------------------
+
+static int read_steps(tg_ctx *c)
+{
+    CU(cudaMemcpyAsync(c->hd, c->sd, sizeof(double) * SD_COUNT * c->ninst, cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaMemcpyAsync(c->hi, c->si, sizeof(int) * (SI_COUNT * c->ninst + 2), cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    return TG_OK;
+}
+
+static int write_steps(tg_ctx *c)
+{
+    CU(cudaMemcpyAsync(c->sd, c->hd, sizeof(double) * SD_COUNT * c->ninst, cudaMemcpyHostToDevice, c->stream));
+    CU(cudaMemcpyAsync(c->si, c->hi, sizeof(int) * (SI_COUNT * c->ninst + 2), cudaMemcpyHostToDevice, c->stream));
+    return TG_OK;
+}
+
+static int check_error(tg_ctx *c)
+{
+    if (hi_error(c)) {
+        hi_error(c) = 0;
+        write_steps(c);
+        return fail(TG_ERR_NONFINITE, "non-finite time step or residual");
+    }
+    return TG_OK;
+}
+
+// residual[5] of instance i from the host mirror
+static void residual_of(tg_ctx *c, int i, double *out)
+{
+    for (int v = 0; v < 5; v++) out[v] = c->hd[(size_t)SD_RESIDUAL * c->ninst + 5 * i + v];
 }
 
 // ---- public single-evaluation entry points ----------------------------------------------------
@@ -892,6 +1202,7 @@ extern "C" int tg_derivative(tg_ctx *c, const double *prim, double *deriv, doubl
 {
     (void)time;  // device boundary conditions do not depend on time
     if (!c || !deriv) return fail(TG_ERR_INVALID, "null argument");
+    if (c->ninst != 1) return fail(TG_ERR_INVALID, "tg_derivative takes a single-mesh context");
     double *q = c->q;
     if (prim) {  // evaluate a host-given state in scratch memory; the resident state stays as it is
         if (!c->qs) {
@@ -899,9 +1210,7 @@ extern "C" int tg_derivative(tg_ctx *c, const double *prim, double *deriv, doubl
             CU(cudaMemsetAsync(c->qs, 0, 5 * sizeof(double) * c->s.N, c->stream));
         }
         q = c->qs;
-        TRY(h2d(c, c->aos, prim, 5 * (size_t)c->s.C));
-        k_prim_aos_to_soa<<<grid_of(c->s.C), BLOCK, 0, c->stream>>>(c->s.C, c->s.N, c->aos, q);
-        CU(cudaGetLastError());
+        TRY(set_rows(c, 0, prim, q));
     }
     TRY(run_fluxes(c, q));
     TRY(launch_cell<0>(c, 0.0, 0, q, c->R));
@@ -930,44 +1239,37 @@ extern "C" int tg_gradient(tg_ctx *c, double time, int limited, double *gradient
     return TG_OK;
 }
 
-static int read_state(tg_ctx *c)
-{
-    CU(cudaMemcpyAsync(c->st_host, c->st, sizeof(StepState), cudaMemcpyDeviceToHost, c->stream));
-    CU(cudaStreamSynchronize(c->stream));
-    return TG_OK;
-}
-
-static int write_state(tg_ctx *c)
-{
-    CU(cudaMemcpyAsync(c->st, c->st_host, sizeof(StepState), cudaMemcpyHostToDevice, c->stream));
-    return TG_OK;
-}
-
 extern "C" int tg_timestep(tg_ctx *c, double *step)
 {
     if (!c || !step) return fail(TG_ERR_INVALID, "null argument");
     TRY(run_prepare(c));
-    TRY(read_state(c));
-    c->st_host->use_max_time = 0;
-    c->st_host->max_step = DBL_MAX;
-    TRY(write_state(c));
-    k_step_begin<<<1, REDUCE_BLOCK, 0, c->stream>>>(c->part_dt, c->nblk, 1.0, c->st);
+    TRY(read_steps(c));
+    for (int i = 0; i < c->ninst; i++) {
+        hd_at(c, SD_MAX_STEP, i) = DBL_MAX;
+        hi_at(c, SI_ACTIVE, i) = 1;
+    }
+    c->st.use_max_time = 0;
+    TRY(write_steps(c));
+    k_inst_begin<<<c->ninst, INST_BLOCK, 0, c->stream>>>(c->seg, c->part_min, 1.0, c->st);
     CU(cudaGetLastError());
-    TRY(read_state(c));
-    *step = c->st_host->step0;
+    TRY(read_steps(c));
+    *step = hd_at(c, SD_STEP0, 0);
     return TG_OK;
 }
 
 extern "C" int tg_residual(tg_ctx *c, const double *deriv, double *residual)
 {
     if (!c || !deriv || !residual) return fail(TG_ERR_INVALID, "null argument");
+    if (c->ninst != 1) return fail(TG_ERR_INVALID, "tg_residual takes a single-mesh context");
     TRY(h2d(c, c->aos, deriv, 5 * (size_t)c->s.C));
     k_aos5_to_soa<<<grid_of(c->s.C), BLOCK, 0, c->stream>>>(c->s.C, c->aos, c->R);
-    k_residual_part<<<c->nblk, BLOCK, 0, c->stream>>>(c->s, c->volume, c->R, c->part_res);
-    k_step_end<<<1, REDUCE_BLOCK, 0, c->stream>>>(c->part_res, c->nblk, c->sum_volume, 0, c->st);
     CU(cudaGetLastError());
-    TRY(read_state(c));
-    for (int v = 0; v < 5; v++) residual[v] = c->st_host->residual[v];
+    TRY(run_pieces(c, 1));
+    k_inst_end<<<c->ninst, INST_BLOCK, 0, c->stream>>>(c->seg, c->part_sum, 0, c->st);
+    CU(cudaGetLastError());
+    TRY(read_steps(c));
+    residual_of(c, 0, residual);
+    c->prepared = false;  // the piece minima were recomputed from stale cell steps
     return TG_OK;
 }
 
@@ -994,21 +1296,26 @@ static int rk_params(const tg_ctx *c, int method, const void *context, int *stag
     return TG_OK;
 }
 
-// one explicit step on the resident state (U0 and the time-step partials must be current)
+// one explicit step of every active instance (U0 and the piece minima must be current)
 static int enqueue_explicit_step(tg_ctx *c, int stages, const double *alpha, double courant)
 {
     {
         Launch l(c, TG_PROF_REDUCE);
-        k_step_begin<<<1, REDUCE_BLOCK, 0, c->stream>>>(c->part_dt, c->nblk, courant, c->st);
+        k_inst_begin<<<c->ninst, INST_BLOCK, 0, c->stream>>>(c->seg, c->part_min, courant, c->st);
     }
     CU(cudaGetLastError());
     for (int i = 0; i < stages; i++) {
         TRY(run_fluxes(c, c->q));
         TRY(launch_cell<1>(c, alpha[i + 1], i == stages - 1, c->q, c->R));
     }
+    TRY(run_pieces(c, 1));
     {
         Launch l(c, TG_PROF_REDUCE);
-        k_step_end<<<1, REDUCE_BLOCK, 0, c->stream>>>(c->part_res, c->nblk, c->sum_volume, 1, c->st);
+        k_inst_end<<<c->ninst, INST_BLOCK, 0, c->stream>>>(c->seg, c->part_sum, 1, c->st);
+    }
+    {
+        Launch l(c, TG_PROF_REDUCE);
+        k_count_active<<<1, 256, 0, c->stream>>>(c->ninst, c->st);
     }
     CU(cudaGetLastError());
     return TG_OK;
@@ -1025,8 +1332,9 @@ static int launch_step(tg_ctx *c, int stages, const double *alpha, double couran
 
 static int step_graph(tg_ctx *c, int method, int stages, const double *alpha, double courant, int use_max_time)
 {
+    c->st.use_max_time = use_max_time;
     if (c->graph && c->graph_method == method && c->graph_stages == stages && c->graph_courant == courant &&
-        c->graph_use_max_time == use_max_time && c->graph_order == c->order) {
+        c->graph_use_max_time == use_max_time) {
         return TG_OK;
     }
     if (c->graph) {
@@ -1055,17 +1363,6 @@ static int step_graph(tg_ctx *c, int method, int stages, const double *alpha, do
     c->graph_stages = stages;
     c->graph_courant = courant;
     c->graph_use_max_time = use_max_time;
-    c->graph_order = c->order;
-    return TG_OK;
-}
-
-static int check_error(tg_ctx *c)
-{
-    if (c->st_host->error) {
-        c->st_host->error = 0;
-        write_state(c);
-        return fail(TG_ERR_NONFINITE, "non-finite time step or residual");
-    }
     return TG_OK;
 }
 
@@ -1076,6 +1373,7 @@ extern "C" int tg_advance(tg_ctx *c, int method, const void *context, double cou
                           double max_step, double *residual, double *step0)
 {
     if (!c || !time) return fail(TG_ERR_INVALID, "null argument");
+    if (c->ninst != 1) return fail(TG_ERR_INVALID, "tg_advance takes a single-mesh context (batches: tg_batch_run)");
     if (!(courant > 0)) return fail(TG_ERR_INVALID, "invalid courant number (%g)", courant);
     if (method == TG_ADVANCE_IMPLICIT_EULER) {
         return implicit_euler_step(c, context, courant, time, max_step, residual, step0);
@@ -1086,19 +1384,45 @@ extern "C" int tg_advance(tg_ctx *c, int method, const void *context, double cou
     const double *alpha;
     TRY(rk_params(c, method, context, &stages, &alpha));
     if (!c->prepared) TRY(run_prepare(c));
-    c->st_host->time = *time;
-    c->st_host->max_step = max_step;
-    c->st_host->use_max_time = 0;
-    c->st_host->error = 0;
-    TRY(write_state(c));
+    hd_at(c, SD_TIME, 0) = *time;
+    hd_at(c, SD_MAX_STEP, 0) = max_step;
+    hd_at(c, SD_THRESHOLD, 0) = 0;
+    hi_at(c, SI_ITER, 0) = 0;
+    hi_at(c, SI_MAX_ITER, 0) = 0x7fffffff;
+    hi_at(c, SI_ACTIVE, 0) = 1;
+    hi_error(c) = 0;
+    TRY(write_steps(c));
     TRY(step_graph(c, method, stages, alpha, courant, 0));
     TRY(launch_step(c, stages, alpha, courant));
-    TRY(read_state(c));
+    TRY(read_steps(c));
     TRY(check_error(c));
-    *time = c->st_host->time;
-    if (residual)
-        for (int v = 0; v < 5; v++) residual[v] = c->st_host->residual[v];
-    if (step0) *step0 = c->st_host->step0;
+    *time = hd_at(c, SD_TIME, 0);
+    if (residual) residual_of(c, 0, residual);
+    if (step0) *step0 = hd_at(c, SD_STEP0, 0);
+    return TG_OK;
+}
+
+// run loop over every instance: each stops on its own limits; the host replays the step graph
+// and checks the number of active instances every `every` steps
+static int run_instances(tg_ctx *c, int method, const void *context, double courant, int max_launch, int every)
+{
+    int stages;
+    const double *alpha;
+    TRY(rk_params(c, method, context, &stages, &alpha));
+    if (!c->prepared) TRY(run_prepare(c));
+    TRY(write_steps(c));
+    TRY(step_graph(c, method, stages, alpha, courant, 1));
+    for (int it = 0; it < max_launch;) {
+        int n = (max_launch - it < every) ? max_launch - it : every;
+        for (int k = 0; k < n; k++) TRY(launch_step(c, stages, alpha, courant));
+        it += n;
+        TRY(read_steps(c));
+        TRY(check_error(c));
+        if (hi_num_active(c) == 0) break;
+    }
+    TRY(read_steps(c));
+    TRY(check_error(c));
+    c->prepared = false;  // cells of stopped instances carry no current step estimate
     return TG_OK;
 }
 
@@ -1107,7 +1431,9 @@ extern "C" int tg_run(tg_ctx *c, int method, const void *context, double courant
                       double *residual)
 {
     if (!c || !time || !iter) return fail(TG_ERR_INVALID, "null argument");
+    if (c->ninst != 1) return fail(TG_ERR_INVALID, "tg_run takes a single-mesh context (batches: tg_batch_run)");
     if (variable < -1 || variable > 4) return fail(TG_ERR_INVALID, "invalid termination variable");
+    if (!(courant > 0)) return fail(TG_ERR_INVALID, "invalid courant number (%g)", courant);
     if (method == TG_ADVANCE_IMPLICIT_EULER) {
         // implicit steps synchronise inside the Newton loop; run them one by one
         int it = 0;
@@ -1129,42 +1455,57 @@ extern "C" int tg_run(tg_ctx *c, int method, const void *context, double courant
     }
     if (method != TG_ADVANCE_EULER && method != TG_ADVANCE_LSERK)
         return fail(TG_ERR_INVALID, "invalid advance method (%d)", method);
-    int stages;
-    const double *alpha;
-    TRY(rk_params(c, method, context, &stages, &alpha));
-    if (!c->prepared) TRY(run_prepare(c));
-    c->st_host->time = *time;
-    c->st_host->max_time = max_time;
-    c->st_host->use_max_time = 1;
-    c->st_host->error = 0;
-    TRY(write_state(c));
-    TRY(step_graph(c, method, stages, alpha, courant, 1));
-    bool check_each = threshold > 0 || max_time < DBL_MAX;
-    int it = 0;
-    while (it < max_iter) {
-        TRY(launch_step(c, stages, alpha, courant));
-        it++;
-        if (check_each) {
-            TRY(read_state(c));
-            TRY(check_error(c));
-            const double *res = c->st_host->residual;
-            if (threshold > 0) {
-                double m = 0;
-                for (int v = 0; v < 5; v++) m = res[v] > m ? res[v] : m;
-                if (((variable >= 0) ? res[variable] : m) < threshold) break;
-            }
-            // teal's loop condition is_less(time, max_time) (src/simulation/run.c:68)
-            double t = c->st_host->time;
-            bool close = fabs(t - max_time) <= fmax(1e-8, 1e-5 * fmax(fabs(t), fabs(max_time)));
-            if (!(t < max_time) || close) break;
-        }
+    if (max_iter <= 0) {
+        *iter = 0;
+        return TG_OK;
     }
-    TRY(read_state(c));
-    TRY(check_error(c));
-    *time = c->st_host->time;
-    *iter = it;
-    if (residual)
-        for (int v = 0; v < 5; v++) residual[v] = c->st_host->residual[v];
+    hd_at(c, SD_TIME, 0) = *time;
+    hd_at(c, SD_MAX_TIME, 0) = max_time;
+    hd_at(c, SD_THRESHOLD, 0) = threshold;
+    hi_at(c, SI_VARIABLE, 0) = variable;
+    hi_at(c, SI_ITER, 0) = 0;
+    hi_at(c, SI_MAX_ITER, 0) = max_iter;
+    hi_at(c, SI_ACTIVE, 0) = 1;
+    hi_error(c) = 0;
+    // stop tests that can end the run early are polled every step, a fixed count only at the end
+    int every = (threshold > 0 || max_time < DBL_MAX) ? 1 : max_iter;
+    TRY(run_instances(c, method, context, courant, max_iter, every));
+    *time = hd_at(c, SD_TIME, 0);
+    *iter = hi_at(c, SI_ITER, 0);
+    if (residual) residual_of(c, 0, residual);
+    return TG_OK;
+}
+
+extern "C" int tg_batch_run(tg_ctx *c, int method, const void *context, double courant, const int *max_iter,
+                            const double *max_time, const int *variable, const double *threshold, double *time,
+                            int *iter, double *residual)
+{
+    if (!c || !max_iter || !time || !iter) return fail(TG_ERR_INVALID, "null argument");
+    if (method != TG_ADVANCE_EULER && method != TG_ADVANCE_LSERK)
+        return fail(TG_ERR_INVALID, "batches run the explicit methods (euler, lserk)");
+    if (!(courant > 0)) return fail(TG_ERR_INVALID, "invalid courant number (%g)", courant);
+    int most = 0;
+    bool early = false;
+    for (int i = 0; i < c->ninst; i++) {
+        int var = variable ? variable[i] : -1;
+        if (var < -1 || var > 4) return fail(TG_ERR_INVALID, "invalid termination variable of instance %d", i);
+        hd_at(c, SD_TIME, i) = time[i];
+        hd_at(c, SD_MAX_TIME, i) = max_time ? max_time[i] : DBL_MAX;
+        hd_at(c, SD_THRESHOLD, i) = threshold ? threshold[i] : 0.0;
+        hi_at(c, SI_VARIABLE, i) = var;
+        hi_at(c, SI_ITER, i) = 0;
+        hi_at(c, SI_MAX_ITER, i) = max_iter[i];
+        hi_at(c, SI_ACTIVE, i) = max_iter[i] > 0;
+        most = max_iter[i] > most ? max_iter[i] : most;
+        early = early || hd_at(c, SD_THRESHOLD, i) > 0 || hd_at(c, SD_MAX_TIME, i) < DBL_MAX;
+    }
+    hi_error(c) = 0;
+    if (most > 0) TRY(run_instances(c, method, context, courant, most, early ? 8 : most));
+    for (int i = 0; i < c->ninst; i++) {
+        time[i] = hd_at(c, SD_TIME, i);
+        iter[i] = hi_at(c, SI_ITER, i);
+        if (residual) residual_of(c, i, residual + 5 * i);
+    }
     return TG_OK;
 }
 
@@ -1294,19 +1635,20 @@ static int implicit_euler_step(tg_ctx *c, const void *context, double courant, d
 
     // step from the CFL condition; U = cons(q) (advance.c:136-143)
     TRY(run_prepare(c));
-    c->st_host->time = *time;
-    c->st_host->max_step = max_step;
-    c->st_host->use_max_time = 0;
-    c->st_host->error = 0;
-    TRY(write_state(c));
-    k_step_begin<<<1, REDUCE_BLOCK, 0, c->stream>>>(c->part_dt, c->nblk, courant, c->st);
+    hd_at(c, SD_TIME, 0) = *time;
+    hd_at(c, SD_MAX_STEP, 0) = max_step;
+    hi_at(c, SI_ACTIVE, 0) = 1;
+    hi_error(c) = 0;
+    c->st.use_max_time = 0;
+    TRY(write_steps(c));
+    k_inst_begin<<<1, INST_BLOCK, 0, c->stream>>>(c->seg, c->part_min, courant, c->st);
     CU(cudaGetLastError());
-    TRY(read_state(c));
+    TRY(read_steps(c));
     TRY(check_error(c));
-    double step = c->st_host->step;
+    double step = hd_at(c, SD_STEP, 0);
     CU(cudaMemcpyAsync(g.U, c->U0, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     CU(cudaMemcpyAsync(g.Ustart, c->U0, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-    CU(cudaMemcpyAsync(sc + GS_STEP, &c->st_host->step, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CU(cudaMemcpyAsync(sc + GS_STEP, c->st.step, sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     c->prepared = false;
 
     double t = *time + step;
@@ -1334,15 +1676,14 @@ static int implicit_euler_step(tg_ctx *c, const void *context, double courant, d
         if (!std::isfinite(norm)) return fail(TG_ERR_NONFINITE, "non-finite Newton residual");
     }
     // residual of the last derivative (advance.c:188)
-    k_residual_part<<<c->nblk, BLOCK, 0, c->stream>>>(c->s, c->volume, c->R, c->part_res);
-    k_step_end<<<1, REDUCE_BLOCK, 0, c->stream>>>(c->part_res, c->nblk, c->sum_volume, 0, c->st);
+    TRY(run_pieces(c, 1));
+    k_inst_end<<<1, INST_BLOCK, 0, c->stream>>>(c->seg, c->part_sum, 0, c->st);
     CU(cudaGetLastError());
-    TRY(read_state(c));
+    TRY(read_steps(c));
     TRY(check_error(c));
     *time = t;
-    if (residual)
-        for (int v = 0; v < 5; v++) residual[v] = c->st_host->residual[v];
-    if (step0) *step0 = c->st_host->step0;
+    if (residual) residual_of(c, 0, residual);
+    if (step0) *step0 = hd_at(c, SD_STEP0, 0);
     return TG_OK;
 }
 

@@ -17,7 +17,6 @@
 namespace tg {
 
 constexpr int MAX_SLOTS = 6;  // teal's MAX_CELL_FACES (src/mesh.h:7-11)
-constexpr int MAX_BOUNDARIES = 16;
 
 // geometry and connectivity; `G` is the geometry element type (double, or float for the FP32
 // flux form, which keeps its own copies)
@@ -42,26 +41,42 @@ struct CellData {
     const double *eps2;       // [C] Venkatakrishnan parameter (or null)
 };
 
-struct BoundaryTable {
-    int num;
-    int kind[MAX_BOUNDARIES];
-    double ctx[MAX_BOUNDARIES][5];
-};
-
 struct Sizes {
     int C, N, F, F_in, F_bd;
 };
 
-// step bookkeeping kept on the device so a whole step can be replayed from a CUDA graph
-struct StepState {
-    double time;
-    double step;       // step of the current / last step (after clipping)
-    double step0;      // unclipped step of the current / last step
-    double max_step;   // clip for the next step (tg_advance)
-    double max_time;   // clip time for the next step (tg_run)
-    double residual[5];
-    int use_max_time;
-    int error;         // nonzero once a non-finite norm or step was seen
+// Instances packed in one arena (a single mesh is one instance). Inner cells of instance i are
+// [inst_cell_off[i], inst_cell_off[i+1]); reductions run over "pieces", cell ranges of at most
+// PIECE cells that never straddle two instances, first per piece, then per instance in piece order.
+constexpr int PIECE = 4096;
+
+struct Segments {
+    int ninst;
+    int npieces;
+    const int *cell_inst;      // [C]
+    const int *inst_cell_off;  // [ninst + 1]
+    const int *piece_beg;      // [npieces + 1]
+    const int *inst_piece_off; // [ninst + 1]
+    const double *sum_volume;  // [ninst]
+};
+
+// Per-instance step bookkeeping in device memory, so whole steps replay from a CUDA graph and
+// instances stop on their own (max iterations, residual threshold, end time).
+struct Steps {
+    double *time;
+    double *step;      // step of the current / last step (after clipping)
+    double *step0;     // unclipped step of the current / last step
+    double *max_step;  // clip of the next step (one Advance call)
+    double *max_time;  // end time (run loops)
+    double *threshold; // residual threshold (<= 0: none)
+    double *residual;  // [ninst][5]
+    int *variable;     // residual variable tested (-1: the maximum)
+    int *iter;
+    int *max_iter;
+    int *active;       // updates and clocks of an inactive instance stand still
+    int *num_active;   // active instances after the last step
+    int *error;        // nonzero once a non-finite step or norm was seen
+    int use_max_time;  // clip by max_time - time instead of max_step
 };
 
 }  // namespace tg

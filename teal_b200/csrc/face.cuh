@@ -32,9 +32,9 @@ __device__ __forceinline__ void reconstruct(const Prim<R> &q, const R *__restric
 
 // One thread per face. The convective flux comes first (its reconstruction streams the limited
 // gradients), the viscous flux second (its face-averaged gradient re-reads the unlimited gradients,
-// which are still in L1); the register cap keeps 16 warps per SM resident.
+// which are still in L1); FACE_MINB caps the registers so that many blocks stay resident per SM.
 template <typename R, int FK, bool NS, int ORDER, bool FOLD>
-__global__ void __launch_bounds__(BLOCK, 2) k_face(Sizes s, Geometry<R> g, const double *__restrict__ q,
+__global__ void __launch_bounds__(FACE_BLOCK, FACE_MINB) k_face(Sizes s, Geometry<R> g, const double *__restrict__ q,
                                                    const R *__restrict__ rec, R gamma, R mu, R prandtl,
                                                    R *__restrict__ G)
 {

@@ -10,8 +10,8 @@ namespace tg {
 // ---- boundary pass (src/equations/boundary.c:5-43) -------------------------------------------
 
 __global__ void k_boundary(Sizes s, const int2 *__restrict__ lr, const double *__restrict__ basis,
-                           const int *__restrict__ bface_ent, BoundaryTable bt, double *q,
-                           double gamma)
+                           const int *__restrict__ bface_ent, const int *__restrict__ bkind,
+                           const double *__restrict__ bctx, double *q, double gamma)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int f = s.F_in + i;
@@ -22,8 +22,8 @@ __global__ void k_boundary(Sizes s, const int2 *__restrict__ lr, const double *_
     int e = bface_ent[i];
     Prim<double> in = load_prim<double>(q, s.N, c.x);
     Basis<double> b = load_basis(basis, s.F, f);
-    Prim<double> ctx = prim_from(bt.ctx[e]);
-    Prim<double> out = boundary_state(bt.kind[e], in, ctx, gamma, b);
+    Prim<double> ctx = prim_from(bctx + 5 * e);
+    Prim<double> out = boundary_state(bkind[e], in, ctx, gamma, b);
     store_prim(q, s.N, c.y, out);
 }
 
@@ -97,9 +97,15 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_gradient(Sizes s, Geometry<R> 
         }
     }
 
+    // limiter factor: the minimum over the cell's faces of teal's candidate ratios. In FP64 the
+    // running minimum is kept as a fraction (numerator, positive denominator), compared by cross
+    // multiplication, and divided once: one division per thread instead of one or two per face,
+    // within two ulps of teal's per-face quotients. FP32 divides per face (its products could
+    // underflow).
     R psi = R(1);
     if (LIM != 0) {
         R e2 = (LIM == 2) ? R(__ldg(eps2 + c)) : R(0);
+        R best_n = R(1), best_d = R(1);
 #pragma unroll
         for (int j = 0; j < MAX_SLOTS; j++) {
             if (j < cnt) {
@@ -107,16 +113,35 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_gradient(Sizes s, Geometry<R> 
                        (gz * s_off[2 * MAX_SLOTS + j][l]);
                 if (!is_close_zero(d2)) {
                     R d1 = R(((d2 > R(0)) ? mx : mn) - qc);
-                    if (LIM == 1) {  // Barth-Jespersen (limiter.c:54-58)
-                        psi = fmin(psi, fmin(R(1), d1 / d2));
+                    R num, den;
+                    if (LIM == 1) {  // Barth-Jespersen: min(1, d1 / d2) (limiter.c:54-58)
+                        num = d1;
+                        den = d2;
                     }
-                    else {  // Venkatakrishnan (limiter.c:100-106)
+                    else {  // Venkatakrishnan: top / bot / d2 (limiter.c:100-106); bot > 0
                         R top = (((d1 * d1) + e2) * d2) + ((R(2) * (d2 * d2)) * d1);
                         R bot = (((d1 * d1) + (R(2) * (d2 * d2))) + (d1 * d2)) + e2;
-                        psi = fmin(psi, (top / bot) / d2);
+                        num = top;
+                        den = bot * d2;
+                    }
+                    if constexpr (sizeof(R) == sizeof(double)) {
+                        if (den < R(0)) {
+                            num = -num;
+                            den = -den;
+                        }
+                        if (num * best_d < best_n * den) {
+                            best_n = num;
+                            best_d = den;
+                        }
+                    }
+                    else {
+                        psi = fmin(psi, (LIM == 1) ? fmin(R(1), num / den) : num / den);
                     }
                 }
             }
+        }
+        if constexpr (sizeof(R) == sizeof(double)) {
+            psi = best_n / best_d;
         }
     }
     if (FOLD && LIM != 0) {
@@ -147,25 +172,25 @@ struct Props {
 // ---- cell gather, finalize and stage update (derivative.c:229-267, advance.c:96-108) ---------
 //
 // MODE 0: R = -sum / V (equations_derivative); MODE 1: one low-storage RK stage
-// U = U0 + R * alpha * step, q = prim(U). With `last`, also: R kept, U0 <- cons(q) for the next
-// step, per-block minimum time step and per-block volume-weighted sums of R^2.
+// U = U0 + R * alpha * step, q = prim(U), with the step of the cell's instance (cells of inactive
+// instances keep their state). With `last`, also: R kept, U0 <- cons(q) for the next step and the
+// cell's stable time step of the new state.
 template <int MODE, bool NS, typename GT>
-__global__ void __launch_bounds__(BLOCK) k_cell(Sizes s, const int *__restrict__ slot_face,
+__global__ void __launch_bounds__(CELL_BLOCK) k_cell(Sizes s, const int *__restrict__ slot_face,
                                                 const uint8_t *__restrict__ slot_cnt, CellData cd,
                                                 const GT *__restrict__ G, double *__restrict__ U0,
                                                 double *__restrict__ q, double *__restrict__ Rout,
-                                                const StepState *__restrict__ st, double alpha,
-                                                int last, Props prop, double *__restrict__ part_dt,
-                                                double *__restrict__ part_res)
+                                                Segments seg, Steps st, double alpha, int last, Props prop,
+                                                double *__restrict__ dtc)
 {
-    __shared__ double sh[BLOCK / 32];
     const int C = s.C, N = s.N;
     int c = blockIdx.x * blockDim.x + threadIdx.x;
-    bool active = c < C;
-    double r[5] = {0, 0, 0, 0, 0};
-    double vol = 1;
-    if (active) {
-        // all slot indices first, then every face value in flight at once; sums in slot order
+    if (c >= C) {
+        return;
+    }
+    double r[5];
+    {
+        // all slot indices first, then every face record in flight at once; sums in slot order
         double acc[5] = {0, 0, 0, 0, 0};
         const int cnt = slot_cnt[c];
         int sf[MAX_SLOTS];
@@ -187,153 +212,204 @@ __global__ void __launch_bounds__(BLOCK) k_cell(Sizes s, const int *__restrict__
                 }
             }
         }
-        vol = __ldg(cd.volume + c);
+        double vol = __ldg(cd.volume + c);
 #pragma unroll
         for (int v = 0; v < 5; v++) {
             r[v] = -acc[v] / vol;
         }
     }
-    if (MODE == 0) {
-        if (active) {
+    if (MODE == 0 || last) {
 #pragma unroll
-            for (int v = 0; v < 5; v++) {
-                Rout[v * C + c] = r[v];
-            }
+        for (int v = 0; v < 5; v++) {
+            Rout[v * C + c] = r[v];
+        }
+    }
+    if (MODE == 0) {
+        return;
+    }
+    const int inst = __ldg(seg.cell_inst + c);
+    if (!st.active[inst]) {
+        if (last) {
+            dtc[c] = DBL_MAX;
         }
         return;
     }
-
-    double step = st->step;
-    double dt_cell = DBL_MAX;
-    if (active) {
-        Cons<double> u;
-        u.rho = __ldg(U0 + c) + ((r[0] * alpha) * step);
-        u.m.x = __ldg(U0 + C + c) + ((r[1] * alpha) * step);
-        u.m.y = __ldg(U0 + 2 * C + c) + ((r[2] * alpha) * step);
-        u.m.z = __ldg(U0 + 3 * C + c) + ((r[3] * alpha) * step);
-        u.e = __ldg(U0 + 4 * C + c) + ((r[4] * alpha) * step);
-        Prim<double> p = cons_to_prim(u, prop.v[0]);
-        store_prim(q, N, c, p);
-        if (last) {
-#pragma unroll
-            for (int v = 0; v < 5; v++) {
-                Rout[v * C + c] = r[v];
-            }
-            Cons<double> u0 = prim_to_cons(p, prop.v[0]);
-            U0[c] = u0.rho;
-            U0[C + c] = u0.m.x;
-            U0[2 * C + c] = u0.m.y;
-            U0[3 * C + c] = u0.m.z;
-            U0[4 * C + c] = u0.e;
-            dt_cell = cell_timestep<NS>(p, prop.v, cd, C, c);
-        }
-    }
+    const double step = st.step[inst];
+    Cons<double> u;
+    u.rho = __ldg(U0 + c) + ((r[0] * alpha) * step);
+    u.m.x = __ldg(U0 + C + c) + ((r[1] * alpha) * step);
+    u.m.y = __ldg(U0 + 2 * C + c) + ((r[2] * alpha) * step);
+    u.m.z = __ldg(U0 + 3 * C + c) + ((r[3] * alpha) * step);
+    u.e = __ldg(U0 + 4 * C + c) + ((r[4] * alpha) * step);
+    Prim<double> p = cons_to_prim(u, prop.v[0]);
+    store_prim(q, N, c, p);
     if (last) {
-        double m = block_min<BLOCK>(dt_cell, sh);
-        if (threadIdx.x == 0) {
-            part_dt[blockIdx.x] = m;
-        }
-#pragma unroll
-        for (int v = 0; v < 5; v++) {
-            double t = active ? vol * (r[v] * r[v]) : 0.0;
-            double sum = block_sum<BLOCK>(t, sh);
-            if (threadIdx.x == 0) {
-                part_res[v * gridDim.x + blockIdx.x] = sum;
-            }
-        }
-    }
-}
-
-// U0 = cons(q) and per-block minimum time step of the current state (start of a run / after the
-// host changed the state)
-template <bool NS>
-__global__ void __launch_bounds__(BLOCK) k_prepare(Sizes s, CellData cd, const double *__restrict__ q,
-                                                   double *__restrict__ U0, Props prop,
-                                                   double *__restrict__ part_dt)
-{
-    __shared__ double sh[BLOCK / 32];
-    const int C = s.C;
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    double dt_cell = DBL_MAX;
-    if (c < C) {
-        Prim<double> p = load_prim<double>(q, s.N, c);
         Cons<double> u0 = prim_to_cons(p, prop.v[0]);
         U0[c] = u0.rho;
         U0[C + c] = u0.m.x;
         U0[2 * C + c] = u0.m.y;
         U0[3 * C + c] = u0.m.z;
         U0[4 * C + c] = u0.e;
-        dt_cell = cell_timestep<NS>(p, prop.v, cd, C, c);
-    }
-    double m = block_min<BLOCK>(dt_cell, sh);
-    if (threadIdx.x == 0) {
-        part_dt[blockIdx.x] = m;
+        dtc[c] = cell_timestep<NS>(p, prop.v, cd, C, c);
     }
 }
 
-// per-block sums of V * R^2 of a derivative (equations_residual, residual.c:8-33)
-__global__ void __launch_bounds__(BLOCK) k_residual_part(Sizes s, const double *__restrict__ volume,
-                                                         const double *__restrict__ Rin,
-                                                         double *__restrict__ part_res)
+// U0 = cons(q) and the stable time step of every cell (start of a run / after the host changed
+// the state)
+template <bool NS>
+__global__ void __launch_bounds__(BLOCK) k_prepare(Sizes s, CellData cd, const double *__restrict__ q,
+                                                   double *__restrict__ U0, Props prop, double *__restrict__ dtc)
+{
+    const int C = s.C;
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= C) {
+        return;
+    }
+    Prim<double> p = load_prim<double>(q, s.N, c);
+    Cons<double> u0 = prim_to_cons(p, prop.v[0]);
+    U0[c] = u0.rho;
+    U0[C + c] = u0.m.x;
+    U0[2 * C + c] = u0.m.y;
+    U0[3 * C + c] = u0.m.z;
+    U0[4 * C + c] = u0.e;
+    dtc[c] = cell_timestep<NS>(p, prop.v, cd, C, c);
+}
+
+// ---- per-instance reductions (deterministic: fixed pieces, fixed order) ---------------------
+
+// per piece: minimum cell time step and (with `res`) the sums of V * R^2 per variable
+__global__ void __launch_bounds__(BLOCK) k_piece_reduce(Segments seg, int C, const double *__restrict__ dtc,
+                                                        const double *__restrict__ R,
+                                                        const double *__restrict__ volume, int res,
+                                                        double *__restrict__ part_min,
+                                                        double *__restrict__ part_sum)
 {
     __shared__ double sh[BLOCK / 32];
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    bool active = c < s.C;
-    double vol = active ? volume[c] : 0.0;
-#pragma unroll
-    for (int v = 0; v < 5; v++) {
-        double r = active ? Rin[v * s.C + c] : 0.0;
-        double sum = block_sum<BLOCK>(active ? vol * (r * r) : 0.0, sh);
-        if (threadIdx.x == 0) {
-            part_res[v * gridDim.x + blockIdx.x] = sum;
-        }
-    }
-}
-
-// start of a step: step0 = courant * min(partials), step = min(step0, max step)
-__global__ void __launch_bounds__(REDUCE_BLOCK) k_step_begin(const double *__restrict__ part_dt,
-                                                             int nparts, double courant, StepState *st)
-{
-    __shared__ double sh[REDUCE_BLOCK / 32];
+    const int beg = seg.piece_beg[blockIdx.x], end = seg.piece_beg[blockIdx.x + 1];
     double m = DBL_MAX;
-    for (int i = threadIdx.x; i < nparts; i += REDUCE_BLOCK) {
-        m = fmin(m, part_dt[i]);
-    }
-    m = block_min<REDUCE_BLOCK>(m, sh);
-    if (threadIdx.x == 0) {
-        double step0 = courant * m;
-        double max_step = st->use_max_time ? (st->max_time - st->time) : st->max_step;
-        st->step0 = step0;
-        st->step = fmin(step0, max_step);
-        if (!isfinite(step0) || !(step0 > 0)) {
-            st->error = 1;
-        }
-    }
-}
-
-// end of a step: time += step, residual = sqrt(sum / sum_volume)
-__global__ void __launch_bounds__(REDUCE_BLOCK) k_step_end(const double *__restrict__ part_res,
-                                                           int nparts, double sum_volume, int advance,
-                                                           StepState *st)
-{
-    __shared__ double sh[REDUCE_BLOCK / 32];
-    for (int v = 0; v < 5; v++) {
-        double t = 0;
-        // fixed-order strided partial sums, then a fixed tree
-        for (int i = threadIdx.x; i < nparts; i += REDUCE_BLOCK) {
-            t += part_res[v * nparts + i];
-        }
-        double sum = block_sum<REDUCE_BLOCK>(t, sh);
-        if (threadIdx.x == 0) {
-            double res = sqrt(sum / sum_volume);
-            st->residual[v] = res;
-            if (!isfinite(res)) {
-                st->error = 1;
+    double t[5] = {0, 0, 0, 0, 0};
+    for (int c = beg + threadIdx.x; c < end; c += BLOCK) {
+        m = fmin(m, dtc[c]);
+        if (res) {
+            double v = volume[c];
+#pragma unroll
+            for (int k = 0; k < 5; k++) {
+                double r = R[k * C + c];
+                t[k] += v * (r * r);
             }
         }
     }
-    if (threadIdx.x == 0 && advance) {
-        st->time += st->step;
+    m = block_min<BLOCK>(m, sh);
+    if (threadIdx.x == 0) {
+        part_min[blockIdx.x] = m;
+    }
+    if (res) {
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+            double sum = block_sum<BLOCK>(t[k], sh);
+            if (threadIdx.x == 0) {
+                part_sum[5 * blockIdx.x + k] = sum;
+            }
+        }
+    }
+}
+
+constexpr int INST_BLOCK = 128;
+
+// start of a step, one block per instance: step0 = courant * min, step = min(step0, clip)
+__global__ void __launch_bounds__(INST_BLOCK) k_inst_begin(Segments seg, const double *__restrict__ part_min,
+                                                           double courant, Steps st)
+{
+    __shared__ double sh[INST_BLOCK / 32];
+    const int i = blockIdx.x;
+    double m = DBL_MAX;
+    for (int p = seg.inst_piece_off[i] + threadIdx.x; p < seg.inst_piece_off[i + 1]; p += INST_BLOCK) {
+        m = fmin(m, part_min[p]);
+    }
+    m = block_min<INST_BLOCK>(m, sh);
+    if (threadIdx.x == 0 && st.active[i]) {
+        double step0 = courant * m;
+        double clip = st.use_max_time ? (st.max_time[i] - st.time[i]) : st.max_step[i];
+        st.step0[i] = step0;
+        st.step[i] = fmin(step0, clip);
+        if (!isfinite(step0) || !(step0 > 0)) {
+            atomicExch(st.error, 1);
+        }
+    }
+}
+
+// is_close of src/core/utils.c:29-34
+__device__ __forceinline__ bool is_close(double a, double b)
+{
+    return fabs(a - b) <= fmax(1e-8, 1e-5 * fmax(fabs(a), fabs(b)));
+}
+
+// end of a step (or a bare residual), one block per instance: residual = sqrt(sum / sum_volume);
+// with `advance`: time += step, iteration count, and the run loop's stop tests
+// (src/simulation/run.c:68-83): iterations, residual threshold, end time
+__global__ void __launch_bounds__(INST_BLOCK) k_inst_end(Segments seg, const double *__restrict__ part_sum,
+                                                         int advance, Steps st)
+{
+    __shared__ double sh[INST_BLOCK / 32];
+    const int i = blockIdx.x;
+    const bool was_active = st.active[i] != 0;
+    double res[5];
+    for (int k = 0; k < 5; k++) {
+        double t = 0;
+        for (int p = seg.inst_piece_off[i] + threadIdx.x; p < seg.inst_piece_off[i + 1]; p += INST_BLOCK) {
+            t += part_sum[5 * p + k];
+        }
+        res[k] = block_sum<INST_BLOCK>(t, sh);
+    }
+    if (threadIdx.x != 0 || (advance && !was_active)) {
+        return;
+    }
+    double mx = 0;
+    for (int k = 0; k < 5; k++) {
+        res[k] = sqrt(res[k] / seg.sum_volume[i]);
+        st.residual[5 * i + k] = res[k];
+        mx = (res[k] > mx) ? res[k] : mx;
+        if (!isfinite(res[k])) {
+            atomicExch(st.error, 1);
+        }
+    }
+    if (!advance) {
+        return;
+    }
+    double t = st.time[i] + st.step[i];
+    st.time[i] = t;
+    int it = st.iter[i] + 1;
+    st.iter[i] = it;
+    bool stop = it >= st.max_iter[i];
+    if (st.threshold[i] > 0) {
+        int v = st.variable[i];
+        stop = stop || (((v >= 0) ? res[v] : mx) < st.threshold[i]);
+    }
+    if (st.use_max_time) {
+        double tm = st.max_time[i];
+        stop = stop || !((t < tm) && !is_close(t, tm));
+    }
+    if (stop) {
+        st.active[i] = 0;
+    }
+}
+
+// number of active instances after a step
+__global__ void k_count_active(int ninst, Steps st)
+{
+    __shared__ int sh;
+    if (threadIdx.x == 0) {
+        sh = 0;
+    }
+    __syncthreads();
+    int n = 0;
+    for (int i = threadIdx.x; i < ninst; i += blockDim.x) {
+        n += st.active[i] != 0;
+    }
+    atomicAdd(&sh, n);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        *st.num_active = sh;
     }
 }
 
@@ -469,8 +545,8 @@ __global__ void k_redirect(int F, int F_bd, int off_periodic_ghost, const int *_
     lr[f] = make_int2(l, r);
 }
 
-// SoA state rows <-> teal's AoS [cells][5]
-__global__ void k_prim_aos_to_soa(int n, int N, const double *__restrict__ aos, double *__restrict__ q)
+// teal AoS rows [n][5] -> state rows [row0, row0 + n) of the SoA state
+__global__ void k_rows_aos_to_soa(int n, int row0, int N, const double *__restrict__ aos, double *__restrict__ q)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) {
@@ -478,22 +554,22 @@ __global__ void k_prim_aos_to_soa(int n, int N, const double *__restrict__ aos, 
     }
 #pragma unroll
     for (int v = 0; v < 5; v++) {
-        q[v * N + i] = aos[(size_t)i * 5 + v];
+        q[(size_t)v * N + row0 + i] = aos[(size_t)i * 5 + v];
     }
 }
 
-// rows [0, n): direct; rows of periodic ghosts: copied from the owner
-__global__ void k_prim_soa_to_aos(int n_direct, int n_total, int N, const int *__restrict__ owner,
-                                  const double *__restrict__ q, double *__restrict__ aos)
+// teal AoS rows [n][5] gathered from the state rows `rowmap` (periodic ghosts map to their owners)
+__global__ void k_rows_gather(int n, const int *__restrict__ rowmap, int N, const double *__restrict__ q,
+                              double *__restrict__ aos)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n_total) {
+    if (i >= n) {
         return;
     }
-    int src = i < n_direct ? i : owner[i - n_direct];
+    int src = rowmap[i];
 #pragma unroll
     for (int v = 0; v < 5; v++) {
-        aos[(size_t)i * 5 + v] = q[v * N + src];
+        aos[(size_t)i * 5 + v] = q[(size_t)v * N + src];
     }
 }
 

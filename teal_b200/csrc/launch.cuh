@@ -23,19 +23,19 @@ inline cudaError_t launch_face_r(bool ns, int order, bool fold, const FaceLaunch
     const Geometry<R> &g = *static_cast<const Geometry<R> *>(a.geom);
     const R *rec = static_cast<const R *>(a.rec);
     R *G = static_cast<R *>(a.G);
-    dim3 grid((a.s.F + BLOCK - 1) / BLOCK);
+    dim3 grid((a.s.F + FACE_BLOCK - 1) / FACE_BLOCK);
     R gm = R(a.gamma), mu = R(a.mu), pr = R(a.prandtl);
     if (order == 1) {
-        k_face<R, FK, false, 1, true><<<grid, BLOCK, 0, st>>>(a.s, g, a.q, rec, gm, mu, pr, G);
+        k_face<R, FK, false, 1, true><<<grid, FACE_BLOCK, 0, st>>>(a.s, g, a.q, rec, gm, mu, pr, G);
     }
     else if (!ns) {
-        k_face<R, FK, false, 2, true><<<grid, BLOCK, 0, st>>>(a.s, g, a.q, rec, gm, mu, pr, G);
+        k_face<R, FK, false, 2, true><<<grid, FACE_BLOCK, 0, st>>>(a.s, g, a.q, rec, gm, mu, pr, G);
     }
     else if (fold) {
-        k_face<R, FK, true, 2, true><<<grid, BLOCK, 0, st>>>(a.s, g, a.q, rec, gm, mu, pr, G);
+        k_face<R, FK, true, 2, true><<<grid, FACE_BLOCK, 0, st>>>(a.s, g, a.q, rec, gm, mu, pr, G);
     }
     else {
-        k_face<R, FK, true, 2, false><<<grid, BLOCK, 0, st>>>(a.s, g, a.q, rec, gm, mu, pr, G);
+        k_face<R, FK, true, 2, false><<<grid, FACE_BLOCK, 0, st>>>(a.s, g, a.q, rec, gm, mu, pr, G);
     }
     return cudaGetLastError();
 }

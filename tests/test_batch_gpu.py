@@ -1,0 +1,105 @@
+"""The batched form: several meshes packed into one arena. Every instance must give the same bits
+it gives alone (same face order inside each face class, reduction pieces aligned to instance
+starts), stop on its own limits, and match the reference solver."""
+
+import numpy as np
+import pytest
+
+import teal_b200 as tb
+from oracle import ref
+from tests.cases import rel_l2, vortex
+
+pytestmark = pytest.mark.gpu
+
+FREE = (1.0, 0.6, 0.1, -0.05, 1.0 / 1.4)
+
+
+def vortex_problem(n):
+    m = tb.Mesh.create((0, 0, 0), (10, 10, 0.625), (n, n, 4), (1, 1, 1))
+    e = tb.Equations.euler(m)
+    e.set_initial_condition("domain", vortex)
+    return e
+
+
+def channel_problem(nx, ny, mach, seed):
+    m = tb.Mesh.create((0, 0, 0), (2, 1, 0.25), (nx, ny, 2), (0, 0, 1))
+    e = tb.Equations.euler(m)
+    free = np.array([1.0, mach * 1.183216, 0.1 * mach, 0.0, 1.0])
+    for side in ("left", "right", "bottom", "top"):
+        e.set_boundary_condition(side, "farfield", free)
+    rng = np.random.default_rng(seed)
+    prim = np.tile(free, (m.num_cells, 1))
+    prim[:, 0] *= 1 + 0.05 * rng.random(m.num_cells)
+    e.primitive[:] = prim
+    return e
+
+
+def problems():
+    return [vortex_problem(16), channel_problem(12, 7, 0.5, 1), vortex_problem(24), channel_problem(9, 9, 2.0, 2)]
+
+
+def alone(e, steps, courant=0.5):
+    ctx = tb.Context(e.mesh, e)
+    ctx.set_primitive(e.primitive)
+    t, it, res = ctx.run(tb.TG_ADVANCE_LSERK, courant, steps, context=(3, 3))
+    return t, it, res, ctx.get_primitive()
+
+
+def test_batch_instances_are_bit_identical_to_solo_runs():
+    ps = problems()
+    steps = [7, 5, 9, 3]
+    b = tb.Batch(ps)
+    t, it, res = b.run(tb.TG_ADVANCE_LSERK, 0.5, steps, context=(3, 3))
+    assert list(it) == steps
+    for i, e in enumerate(ps):
+        t1, it1, res1, p1 = alone(e, steps[i])
+        C = e.mesh.num_inner_cells
+        got = b.get_primitive(i)
+        assert it1 == steps[i]
+        assert t[i] == t1
+        assert np.array_equal(res[i], res1)
+        assert np.array_equal(got[:C], p1[:C])
+        assert np.array_equal(got, p1)  # ghost rows too
+
+
+def test_batch_stops_each_instance_on_its_own_limits():
+    ps = problems()
+    b = tb.Batch(ps)
+    # instance 0: time limit; 1: residual threshold; 2, 3: iteration limits
+    t, it, res = b.run(tb.TG_ADVANCE_LSERK, 0.5, [1000, 1000, 4, 6], max_time=[0.05, 1e300, 1e300, 1e300],
+                       threshold=[0, 0.5 * 1e9, 0, 0], context=(3, 3))
+    assert abs(t[0] - 0.05) <= 1e-12
+    assert it[1] == 1  # the first residual is already below the (huge) threshold
+    assert it[2] == 4 and it[3] == 6
+
+
+def test_batch_matches_reference():
+    sizes = [(12, 12, 4), (20, 14, 4)]
+    ps, refs = [], []
+    for n in sizes:
+        m = tb.Mesh.create((0, 0, 0), (10, 10, 0.625), n, (1, 1, 1))
+        e = tb.Equations.euler(m)
+        e.set_initial_condition("domain", vortex)
+        ps.append(e)
+        rm = ref.RefMesh((0, 0, 0), (10, 10, 0.625), n, (1, 1, 1))
+        re = ref.RefEquations(rm, False)
+        re.set_primitive(e.primitive)
+        refs.append(re)
+    b = tb.Batch(ps)
+    t, it, res = b.run(tb.TG_ADVANCE_LSERK, 0.5, 5, context=(3, 3))
+    for i, re in enumerate(refs):
+        rs = ref.RefSimulation(re, "lserk", 0.5, rk=(3, 3))
+        tr = 0.0
+        for _ in range(5):
+            tr, _, rr = rs.advance(tr)
+        C = ps[i].mesh.num_inner_cells
+        assert rel_l2(b.get_primitive(i)[:C], re.primitive[:C]).max() <= 1e-12
+        assert abs(t[i] - tr) <= 1e-13 * tr
+
+
+def test_batch_rejects_mixed_lanes():
+    a = vortex_problem(8)
+    c = vortex_problem(8)
+    c.set_convective_flux("roe")
+    with pytest.raises(tb.TealError, match="differs"):
+        tb.Batch([a, c])
