@@ -1020,13 +1020,14 @@ static bool fold_psi(const tg_ctx *c)
     return !(c->viscous == TG_VISCOUS_CENTRAL) || c->limiter == TG_LIMITER_NONE;
 }
 
-static int run_boundary(tg_ctx *c, double *q)
+// `masked`: inside a step sequence, where instances that have stopped keep their ghost rows
+static int run_boundary(tg_ctx *c, double *q, bool masked = false)
 {
     int nbf = c->s.F_bd - c->s.F_in;
     if (nbf <= 0) return TG_OK;
     Launch l(c, TG_PROF_BOUNDARY);
     k_boundary<<<grid_of(nbf), BLOCK, 0, c->stream>>>(c->s, c->lr, c->gb.basis, c->bface_ent, c->bkind, c->bctx, q,
-                                                      c->prop[0]);
+                                                      c->prop[0], c->cell_inst, masked ? c->st.active : nullptr);
     CU(cudaGetLastError());
     return TG_OK;
 }
@@ -1132,9 +1133,9 @@ static int launch_cell(tg_ctx *c, double alpha, int last, double *q, double *Rou
 }
 
 // boundary pass, gradient + limiter, face fluxes: everything of a residual before the gather
-static int run_fluxes(tg_ctx *c, double *q)
+static int run_fluxes(tg_ctx *c, double *q, bool masked = false)
 {
-    TRY(run_boundary(c, q));
+    TRY(run_boundary(c, q, masked));
     if (c->order == 2) TRY(run_gradient(c, q));
     TRY(run_face(c, q));
     return TG_OK;
@@ -1305,7 +1306,7 @@ static int enqueue_explicit_step(tg_ctx *c, int stages, const double *alpha, dou
     }
     CU(cudaGetLastError());
     for (int i = 0; i < stages; i++) {
-        TRY(run_fluxes(c, c->q));
+        TRY(run_fluxes(c, c->q, true));
         TRY(launch_cell<1>(c, alpha[i + 1], i == stages - 1, c->q, c->R));
     }
     TRY(run_pieces(c, 1));

@@ -9,9 +9,12 @@ namespace tg {
 
 // ---- boundary pass (src/equations/boundary.c:5-43) -------------------------------------------
 
+// With `active` (inside a step sequence), faces of instances that have stopped keep their ghost
+// rows: a stopped instance's state, ghosts included, is what it was when it stopped.
 __global__ void k_boundary(Sizes s, const int2 *__restrict__ lr, const double *__restrict__ basis,
                            const int *__restrict__ bface_ent, const int *__restrict__ bkind,
-                           const double *__restrict__ bctx, double *q, double gamma)
+                           const double *__restrict__ bctx, double *q, double gamma,
+                           const int *__restrict__ cell_inst, const int *__restrict__ active)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int f = s.F_in + i;
@@ -19,6 +22,9 @@ __global__ void k_boundary(Sizes s, const int2 *__restrict__ lr, const double *_
         return;
     }
     int2 c = lr[f];
+    if (active && !active[cell_inst[c.x]]) {
+        return;
+    }
     int e = bface_ent[i];
     Prim<double> in = load_prim<double>(q, s.N, c.x);
     Basis<double> b = load_basis(basis, s.F, f);
