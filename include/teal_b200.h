@@ -283,6 +283,28 @@ int tg_launch_count(tg_ctx *ctx, long *count);
  * Returns TG_ERR_INVALID for an unknown name or a count that does not match. */
 int tg_layout(tg_ctx *ctx, const char *name, void *out, long count);
 
+/* ---- residual norm with no device allocation -----------------------------------------------------
+ * No counterpart in the reference. It computes what equations_residual does (equations/residual.c:8),
+ * residual[k] = sqrt(sum_c volume[c] * derivative[c][k]^2 / sum_volume), for a derivative that is
+ * already on the device, without a context and without allocating device memory. It is meant for
+ * callers that cannot allocate while they solve: a server that committed its whole HBM budget to
+ * state arenas up front, or a host loop that must not stall the device (cudaMalloc and cudaFree
+ * can synchronise it).
+ *   derivative  device double[num_cells][5] (teal's row layout)
+ *   volume      device double[num_cells]
+ *   sum_volume  the divisor (teal's mesh->cell.sum_volume)
+ *   residual    device double[5], written on `stream` (a cudaStream_t; null = legacy default)
+ * All three buffers must be 8-byte aligned device or managed memory, else TG_ERR_INVALID.
+ * The partial sums go to a fixed 640 KiB array compiled into the library, one per device, which
+ * limits num_cells to TG_NOALLOC_MAX_CELLS; a larger num_cells returns TG_ERR_INVALID.
+ * The first call on each device does a set-up (it looks up that array's device address, which can
+ * initialise the device's CUDA context); make that first call before any stream capture.
+ * Calls that overlap in time on the same device (other streams, other host threads) share the
+ * array and race: serialise them. The result equals tg_residual's on the same derivative. */
+#define TG_NOALLOC_MAX_CELLS 67108864
+int tg_residual_noalloc(const double *derivative, const double *volume, int num_cells, double sum_volume,
+                        double *residual, void *stream);
+
 /* ---- version / build info ---------------------------------------------------------------------- */
 const char *tg_build_info(void);
 

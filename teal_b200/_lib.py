@@ -25,6 +25,7 @@ TG_VISCOUS_NONE, TG_VISCOUS_CENTRAL = 0, 1
 TG_LIMITER_NONE, TG_LIMITER_BARTH_JESPERSEN, TG_LIMITER_VENKATAKRISHNAN = 0, 1, 2
 TG_ADVANCE_EULER, TG_ADVANCE_LSERK, TG_ADVANCE_IMPLICIT_EULER = 0, 1, 2
 TG_PRECISION_FP64, TG_PRECISION_FP32_FLUX = 0, 1
+TG_NOALLOC_MAX_CELLS = 67108864  # cell limit of tg_residual_noalloc (its fixed scratch array)
 
 _int_p = ctypes.POINTER(ctypes.c_int)
 _dbl_p = ctypes.POINTER(ctypes.c_double)
@@ -141,6 +142,7 @@ SIGNATURES = [
     ("tg_profile_read", ctypes.c_int, [_vp, _vp, _vp]),
     ("tg_launch_count", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_long)]),
     ("tg_layout", ctypes.c_int, [_vp, ctypes.c_char_p, _vp, ctypes.c_long]),
+    ("tg_residual_noalloc", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_double, _vp, _vp]),
     ("tg_build_info", ctypes.c_char_p, []),
 ]
 

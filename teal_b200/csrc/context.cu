@@ -56,6 +56,12 @@ extern "C" const char *tg_last_error(void)
     return g_error.c_str();
 }
 
+// lets the library's other translation units report through tg_last_error
+int tg_record_error(int code, const char *msg)
+{
+    return fail(code, "%s", msg);
+}
+
 extern "C" const char *tg_build_info(void)
 {
     return "teal_b200 sm_100a " __DATE__;
