@@ -7,6 +7,11 @@ limiter (K = 1), low-storage RK {time order 3, 3 stages}, CFL 0.99, FP64. A step
 (3 residual evaluations + update). Metric: cell-updates/s = inner cells x steps / device seconds.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--n 128] [--precision fp64]
+                  [--workload tgv|ramp]
+
+--workload ramp measures the unstructured case instead: a compression ramp on an 80^3 jittered grid
+split into tetrahedra, prisms, hexahedra and pyramid transitions (about 2.4 M cells), Euler, Mach 2.5,
+ausmd flux, Barth-Jespersen limiter, supersonic inflow / outflow and slip walls, lserk {3,3}.
 
 With --gpus N (launched by torchrun) every rank advances its own replica of the workload (the path is
 one mesh per GPU; there is no exchange), timed on the device, max over ranks; `value` is the
@@ -31,6 +36,13 @@ sys.path.insert(0, ROOT)
 
 METRIC = "cell-updates/s"
 WORKLOAD = "taylor-green vortex 128^3 periodic hex, navier-stokes, roe + ls gradient + venkatakrishnan(1), lserk{3,3}, cfl 0.99"
+RAMP_WORKLOAD = ("compression ramp 80^3 jittered hex grid split into tetrahedra / prisms / hexahedra / pyramid "
+                 "transitions, 15 deg ramp, Mach 2.5, euler, ausmd + ls gradient + barth-jespersen, "
+                 "supersonic inflow / outflow + slip walls, lserk{3,3}, cfl 0.99")
+M25 = (1.0, 2.5, 0.0, 0.0, 1.0 / 1.4)
+RAMP_BCS = {"left": ("supersonic inflow", M25), "right": ("supersonic outflow", None),
+            "bottom": ("slipwall", None), "top": ("slipwall", None), "back": ("slipwall", None),
+            "front": ("slipwall", None)}
 
 
 def tgv_state(center, gamma=1.4, mach=0.1):
@@ -144,18 +156,41 @@ def dist_setup():
     return world, rank, local
 
 
-def reference_cpu(n, steps, warmup=0):
-    """Time the reference solver's own lserk step (oracle/_ref, one core) on a TGV mesh of n^3 cells.
-    Returns (cell-updates/s, seconds, steps)."""
+def ramp_state(center):
+    return np.tile(np.array(M25), (center.shape[0], 1))
+
+
+def configure(eqns, workload):
+    """The plugin settings of a workload on teal_b200 or reference equations (same setter names)."""
+    if workload == "tgv":
+        eqns.set_convective_flux("roe")
+        eqns.set_limiter("venkatakrishnan", 1.0)
+        eqns.set_property("dynamic viscosity", 1 / 1600)
+    else:
+        eqns.set_convective_flux("ausmd")
+        eqns.set_limiter("minmod", 0.0)
+        for entity, (name, ctx) in RAMP_BCS.items():
+            eqns.set_boundary_condition(entity, name, ctx)
+
+
+def reference_cpu(n, steps, warmup=0, workload="tgv"):
+    """Time the reference solver's own lserk step (oracle/_ref, one core) on the workload at mesh size
+    n (TGV n^3; ramp n^3 grid cells before splitting). Returns (cell-updates/s, seconds, steps)."""
     from oracle import ref
 
-    m = ref.RefMesh((0, 0, 0), (2 * math.pi,) * 3, (n, n, n), (1, 1, 1))
-    e = ref.RefEquations(m, navierstokes=True)
-    e.set_convective_flux("roe")
-    e.set_limiter("venkatakrishnan", 1.0)
-    e.set_property("dynamic viscosity", 1 / 1600)
+    if workload == "tgv":
+        m = ref.RefMesh((0, 0, 0), (2 * math.pi,) * 3, (n, n, n), (1, 1, 1))
+        e = ref.RefEquations(m, navierstokes=True)
+        init = tgv_state
+    else:
+        from teal_b200 import meshes
+
+        m = ref.RefMesh.from_cells(meshes.ramp_mesh(n=(n, n, n)))
+        e = ref.RefEquations(m, navierstokes=False)
+        init = ramp_state
+    configure(e, workload)
     c = m.arrays()["cells.center"]
-    e.set_primitive(tgv_state(c))
+    e.set_primitive(init(c))
     sim = ref.RefSimulation(e, "lserk", 0.99, rk=(3, 3))
     t = 0.0
     for _ in range(warmup):
@@ -177,15 +212,16 @@ def run_reference_arm(args, world, rank):
         print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref not built"}))
         return
     n_sample = args.ref_n
-    value, secs, steps = reference_cpu(n_sample, args.steps, warmup=min(args.warmup, 1))
+    value, secs, steps = reference_cpu(n_sample, args.steps, warmup=min(args.warmup, 1), workload=args.workload)
     line = {
         "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000 * secs / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample_mesh": f"{n_sample}^3", "parallelism": "1 core"},
+        "config": {"workload": WORKLOAD if args.workload == "tgv" else RAMP_WORKLOAD,
+                   "sample_mesh": f"{n_sample}^3", "parallelism": "1 core"},
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
-                         "sample": f"{steps} lserk steps of the same TGV case on a {n_sample}^3 mesh, one core "
+                         "sample": f"{steps} lserk steps of the same case on a {n_sample}^3 mesh, one core "
                                    "(single-process build of the reference)"},
         "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -198,11 +234,18 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="teal_b200")
-    ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--workload", default="tgv", choices=["tgv", "ramp"],
+                    help="tgv: Taylor-Green 128^3 (the headline); ramp: the unstructured compression ramp")
+    ap.add_argument("--n", type=int, default=None, help="mesh cells per axis (tgv 128, ramp 80)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
-    ap.add_argument("--ref-n", type=int, default=48, help="mesh size of the CPU reference sample")
+    ap.add_argument("--ref-n", type=int, default=None, help="mesh size of the CPU reference sample (tgv 48, ramp 32)")
+    ap.add_argument("--ref-steps", type=int, default=20, help="steps of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    if args.n is None:
+        args.n = 128 if args.workload == "tgv" else 80
+    if args.ref_n is None:
+        args.ref_n = 48 if args.workload == "tgv" else 32
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()
 
@@ -225,14 +268,20 @@ def main():
     import teal_b200 as tb
 
     n = args.n
+    ns = args.workload == "tgv"
     t0 = time.perf_counter()
-    mesh = tb.Mesh.create((0, 0, 0), (2 * math.pi,) * 3, (n, n, n), (1, 1, 1))
+    if ns:
+        mesh = tb.Mesh.create((0, 0, 0), (2 * math.pi,) * 3, (n, n, n), (1, 1, 1))
+        eqns = tb.Equations.navierstokes(mesh)
+    else:
+        from teal_b200 import meshes
+
+        cells = meshes.ramp_mesh(n=(n, n, n))
+        mesh = tb.Mesh.from_cells(cells)
+        eqns = tb.Equations.euler(mesh)
     t_mesh = time.perf_counter() - t0
-    eqns = tb.Equations.navierstokes(mesh)
-    eqns.set_convective_flux("roe")
-    eqns.set_limiter("venkatakrishnan", 1.0)
-    eqns.set_property("dynamic viscosity", 1 / 1600)
-    eqns.set_initial_condition("domain", tgv_state)
+    configure(eqns, args.workload)
+    eqns.set_initial_condition("domain", tgv_state if ns else ramp_state)
     precision = tb.TG_PRECISION_FP64 if args.precision == "fp64" else tb.TG_PRECISION_FP32_FLUX
     t0 = time.perf_counter()
     ctx = eqns.context(precision)
@@ -308,9 +357,9 @@ def main():
     peak, peak_kind = read_peaks()
     stages = ksteps * rk[1]
     stage_ms = sum(prof[k][0] for k in ("boundary", "gradient", "face", "cell")) / stages
-    b_stage = stage_bytes(C, F, ns=True)
+    b_stage = stage_bytes(C, F, ns=ns)
     achieved = b_stage / (stage_ms / 1000.0) / 1e9
-    kb = kernel_bytes(C, F, S, NB, ns=True, fold=False)
+    kb = kernel_bytes(C, F, S, NB, ns=ns, fold=not ns)
     kernels = {}
     for k in ("gradient", "face", "cell"):
         kms, kn = prof[k]
@@ -322,7 +371,7 @@ def main():
 
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "stage_traffic.json")
-    if os.path.exists(tpath):
+    if ns and os.path.exists(tpath):
         with open(tpath) as f:
             tr = json.load(f)
         if tr.get("n") and tr.get("bytes_per_stage"):
@@ -333,9 +382,9 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32-flux/f64-accumulate",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "cells": C, "faces": F, "mesh": f"{n}^3", "global_batch": world,
-                   "parallelism": f"replicas x{world}" if world > 1 else "1 gpu",
-                   "l2": "inputs larger than L2 (state + geometry ~3 GB per stage)"},
+        "config": {"workload": WORKLOAD if ns else RAMP_WORKLOAD, "cells": C, "faces": F, "mesh": f"{n}^3",
+                   "global_batch": world, "parallelism": f"replicas x{world}" if world > 1 else "1 gpu",
+                   "l2": f"inputs larger than L2 (state + geometry ~{b_stage / 1e9:.1f} GB per stage)"},
         "roofline": {"bound": "hbm", "kernel": "rk stage (boundary+gradient+face+cell)", "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "peak_kind": peak_kind, "algorithmic_bytes_per_launch": b_stage,
@@ -353,9 +402,9 @@ def main():
             from oracle import ref
 
             if ref.available():
-                v, secs, st = reference_cpu(args.ref_n, 2)
+                v, secs, st = reference_cpu(args.ref_n, args.ref_steps, workload=args.workload)
                 line["cpu_baseline"] = {"value": v, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
-                                        "sample": f"{st} lserk steps of the same TGV case on a {args.ref_n}^3 mesh "
+                                        "sample": f"{st} lserk steps of the same case on a {args.ref_n}^3 mesh "
                                                   f"({secs:.1f} s), one core"}
         except Exception as exc:  # the baseline is reported, never required
             line["cpu_baseline"] = {"error": str(exc)}

@@ -249,6 +249,15 @@ typedef struct tg_host_mesh tg_host_mesh;
  * geometry is generated, as mesh_modify would. */
 int tg_host_mesh_cartesian(const double *min_coord, const double *max_coord, const int *num_cells,
                            const int *periodic, const double *displacement, tg_host_mesh **mesh);
+/* Generate a single-process mesh given as nodes, cells and entities, as teal holds it between
+ * mesh_read (src/mesh/read.c) and mesh_generate: coord [num_nodes][3]; cells as node lists in CSR
+ * (node_off [num_cells + 1], node_idx), first num_inner_cells volume cells (tetrahedron 4,
+ * pyramid 5, prism 6, hexahedron 8 nodes, Gmsh order), then boundary face cells (3 or 4 nodes);
+ * entities as names and cell ranges (entity_cell_off [num_entities + 1]): the inner entities
+ * first, then one entity per boundary. No periodic entities. */
+int tg_host_mesh_cells(int num_nodes, const double *coord, int num_cells, int num_inner_cells,
+                       const int *node_off, const int *node_idx, int num_entities,
+                       const char *const *entity_names, const int *entity_cell_off, tg_host_mesh **mesh);
 /* View of the generated arrays (pointers stay owned by the host mesh). */
 int tg_host_mesh_view(const tg_host_mesh *mesh, tg_mesh *view);
 /* Entity names (teal's: "domain", "left", "right", ...) and their cell ranges. */

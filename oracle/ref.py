@@ -33,6 +33,8 @@ def lib():
             "ref_set_quiet": (None, [ctypes.c_int]),
             "ref_mesh_cartesian": (vp, [dp, dp, ip, ip]),
             "ref_mesh_displace": (None, [vp, dp, ctypes.c_int]),
+            "ref_mesh_cells": (vp, [ctypes.c_int, dp, ctypes.c_int, ctypes.c_int, ip, ip, ctypes.c_int,
+                                    ctypes.POINTER(ctypes.c_char_p), ip]),
             "ref_mesh_split": (None, [vp, ctypes.c_char_p, dp, dp]),
             "ref_mesh_generate": (None, [vp]),
             "ref_mesh_validate": (None, [vp]),
@@ -98,6 +100,26 @@ class RefMesh:
             L.ref_mesh_displace(self.ptr, _d(self._disp), self._disp.shape[0])
         if generate:
             L.ref_mesh_generate(self.ptr)
+
+    @classmethod
+    def from_cells(cls, mesh, generate=True):
+        """A one-rank mesh from nodes / cells / entities (the dict of teal_b200.meshes), then
+        mesh_generate."""
+        L = lib()
+        self = cls.__new__(cls)
+        coord = np.ascontiguousarray(mesh["coord"], np.float64)
+        off = np.ascontiguousarray(mesh["node_off"], np.int32)
+        idx = np.ascontiguousarray(mesh["node_idx"], np.int32)
+        ents = mesh["entities"]
+        names = (ctypes.c_char_p * len(ents))(*[e[0].encode() for e in ents])
+        eoff = np.array([e[1] for e in ents] + [ents[-1][2]], np.int32)
+        ip = ctypes.POINTER(ctypes.c_int)
+        self.ptr = ctypes.c_void_p(L.ref_mesh_cells(coord.shape[0], _d(coord), off.size - 1, mesh["num_inner"],
+                                                    off.ctypes.data_as(ip), idx.ctypes.data_as(ip), len(ents),
+                                                    names, eoff.ctypes.data_as(ip)))
+        if generate:
+            L.ref_mesh_generate(self.ptr)
+        return self
 
     def validate(self):
         lib().ref_mesh_validate(self.ptr)

@@ -36,9 +36,6 @@ void ref_set_quiet(int quiet)
 
 /* ---- mesh ----------------------------------------------------------------------------------- */
 
-static void (*modify_fn)(Vector *) = 0;
-static double jitter_amp = 0;
-
 void *ref_mesh_cartesian(const double *min, const double *max, const int *num, const int *periodic)
 {
     Vector lo = {min[0], min[1], min[2]};
@@ -46,6 +43,56 @@ void *ref_mesh_cartesian(const double *min, const double *max, const int *num, c
     Triple n = {num[0], num[1], num[2]};
     Triple p = {periodic[0], periodic[1], periodic[2]};
     Mesh *mesh = mesh_create(lo, hi, n, p);
+    return mesh;
+}
+
+/* A one-rank mesh from nodes, cells (node lists: inner cells, then boundary face cells) and entity
+ * cell ranges, in the state mesh_read leaves it before mesh_generate (src/mesh/read.c): all nodes
+ * and cells local, no periodic entities, no neighbour ranks (as create_neighbors leaves a rank
+ * without neighbours, src/mesh/create.c:388-440). Entities whose range ends within the inner cells
+ * are inner entities. */
+void *ref_mesh_cells(int num_nodes, const double *coord, int num_cells, int num_inner, const int *node_off,
+                     const int *node_idx, int num_entities, const char *const *names, const int *cell_off)
+{
+    Mesh *mesh = teal_calloc(1, sizeof(*mesh));
+    mesh->nodes.num = num_nodes;
+    mesh->nodes.num_inner = num_nodes;
+    mesh->nodes.global = teal_calloc(num_nodes, sizeof(*mesh->nodes.global));
+    mesh->nodes.coord = teal_calloc(num_nodes, sizeof(*mesh->nodes.coord));
+    for (int i = 0; i < num_nodes; i++) {
+        mesh->nodes.global[i] = i;
+        mesh->nodes.coord[i] = (Vector){coord[(3 * i) + 0], coord[(3 * i) + 1], coord[(3 * i) + 2]};
+    }
+    mesh->cells.num = num_cells;
+    mesh->cells.num_inner = num_inner;
+    mesh->cells.off_boundary = num_cells;
+    mesh->cells.off_periodic = num_cells;
+    mesh->cells.node.off = teal_calloc(num_cells + 1, sizeof(int));
+    mesh->cells.node.idx = teal_calloc(node_off[num_cells], sizeof(int));
+    memcpy(mesh->cells.node.off, node_off, (num_cells + 1) * sizeof(int));
+    memcpy(mesh->cells.node.idx, node_idx, node_off[num_cells] * sizeof(int));
+    int num_inner_entities = 0;
+    for (int i = 0; i < num_entities; i++) {
+        if (cell_off[i + 1] <= num_inner) num_inner_entities = i + 1;
+    }
+    mesh->entities.num = num_entities;
+    mesh->entities.num_inner = num_inner_entities;
+    mesh->entities.off_boundary = num_entities;
+    mesh->entities.name = teal_calloc(num_entities, sizeof(*mesh->entities.name));
+    mesh->entities.cell_off = teal_calloc(num_entities + 1, sizeof(int));
+    mesh->entities.rotation = teal_calloc(num_entities, sizeof(*mesh->entities.rotation));
+    mesh->entities.translation = teal_calloc(num_entities, sizeof(*mesh->entities.translation));
+    for (int i = 0; i < num_entities; i++) {
+        strncpy(mesh->entities.name[i], names[i], sizeof(mesh->entities.name[i]) - 1);
+    }
+    memcpy(mesh->entities.cell_off, cell_off, (num_entities + 1) * sizeof(int));
+    mesh->neighbors.num = 0;
+    mesh->neighbors.tag = teal_calloc(1, sizeof(*mesh->neighbors.tag));
+    mesh->neighbors.rank = teal_calloc(1, sizeof(int));
+    mesh->neighbors.recv_off = teal_calloc(1, sizeof(int));
+    mesh->neighbors.recv_off[0] = num_cells;
+    mesh->neighbors.send.off = teal_calloc(1, sizeof(int));
+    mesh->neighbors.send.idx = teal_calloc(1, sizeof(int));
     return mesh;
 }
 
@@ -70,8 +117,6 @@ void ref_mesh_displace(void *mesh, const double *disp, int num)
     displacement_cur = 0;
     mesh_modify(mesh, displace);
     displacement = 0;
-    (void)modify_fn;
-    (void)jitter_amp;
 }
 
 void ref_mesh_split(void *mesh, const char *entity, const double *root, const double *normal)

@@ -134,6 +134,9 @@ SIGNATURES = [
     ("tg_teal_implicit_euler", ctypes.c_double, [_vp, _dbl_p, _vp, ctypes.c_double, ctypes.c_double,
                                                  _vp]),
     ("tg_host_mesh_cartesian", ctypes.c_int, [_dbl_p, _dbl_p, _int_p, _int_p, _dbl_p, ctypes.POINTER(_vp)]),
+    ("tg_host_mesh_cells", ctypes.c_int, [ctypes.c_int, _dbl_p, ctypes.c_int, ctypes.c_int, _int_p, _int_p,
+                                          ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), _int_p,
+                                          ctypes.POINTER(_vp)]),
     ("tg_host_mesh_view", ctypes.c_int, [_vp, ctypes.POINTER(TgMesh)]),
     ("tg_host_mesh_entity", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), _int_p,
                                            _int_p]),

@@ -408,16 +408,18 @@ struct Face {
     int node[4];
 };
 
-void correct_face_node_order(Face &f, const tg_host_mesh &m)  // generate.c:227-264
+// a quad's nodes put in cyclic order (generate.c:227-264); false when no order is valid
+bool correct_face_node_order(Face &f, const tg_host_mesh &m)
 {
-    if (f.num_nodes != 4) return;
+    if (f.num_nodes != 4) return true;
     for (int i = 0; i < 3; i++) {
         Vec c[4];
         for (int j = 0; j < 4; j++) c[j] = m.coord[f.node[j]];
         Vec a2b = vsub(c[1], c[0]), a2c = vsub(c[2], c[0]), a2d = vsub(c[3], c[0]);
-        if (vdot(vcross(a2b, a2c), vcross(a2c, a2d)) > 0) return;
+        if (vdot(vcross(a2b, a2c), vcross(a2c, a2d)) > 0) return true;
         if (i + 2 < f.num_nodes) std::swap(f.node[i + 1], f.node[i + 2]);
     }
+    return false;
 }
 
 int create_faces(tg_host_mesh &m)  // generate.c:267-321
@@ -439,7 +441,7 @@ int create_faces(tg_host_mesh &m)  // generate.c:267-321
                             f.node[f.num_nodes++] = m.node_idx[a];
                         }
                 if (f.num_nodes < 3) return TG_ERR_INVALID;
-                correct_face_node_order(f, m);
+                if (!correct_face_node_order(f, m)) return TG_ERR_INVALID;
                 faces.push_back(f);
             }
         }
@@ -797,6 +799,63 @@ extern "C" int tg_host_mesh_cartesian(const double *min_coord, const double *max
     tg_host_mesh *m = new tg_host_mesh();
     int rc = cartesian(*m, min_coord, max_coord, num_cells, periodic, displacement);
     if (rc == TG_OK) rc = generate(*m);
+    if (rc != TG_OK) {
+        delete m;
+        return rc;
+    }
+    *out = m;
+    return TG_OK;
+}
+
+// One process's mesh given as teal holds it before generation (mesh_read's output, src/mesh/read.c,
+// without partitioning or neighbours): nodes, cells as node lists (inner cells with 4, 5, 6 or 8
+// nodes in Gmsh order, then boundary face cells with 3 or 4 nodes), and entities as cell ranges.
+extern "C" int tg_host_mesh_cells(int num_nodes, const double *coord, int num_cells, int num_inner_cells,
+                                  const int *node_off, const int *node_idx, int num_entities,
+                                  const char *const *entity_names, const int *entity_cell_off,
+                                  tg_host_mesh **out)
+{
+    if (!coord || !node_off || !node_idx || !entity_names || !entity_cell_off || !out) return TG_ERR_INVALID;
+    *out = nullptr;
+    if (num_nodes <= 0 || num_inner_cells <= 0 || num_cells < num_inner_cells || num_entities < 1) {
+        return TG_ERR_INVALID;
+    }
+    if (node_off[0] != 0 || entity_cell_off[0] != 0 || entity_cell_off[num_entities] != num_cells) {
+        return TG_ERR_INVALID;
+    }
+    for (int i = 0; i < num_cells; i++) {
+        int len = node_off[i + 1] - node_off[i];
+        bool ok = (i < num_inner_cells) ? (len == 4 || len == 5 || len == 6 || len == 8) : (len == 3 || len == 4);
+        if (!ok) return TG_ERR_INVALID;
+        for (int j = node_off[i]; j < node_off[i + 1]; j++) {
+            if (node_idx[j] < 0 || node_idx[j] >= num_nodes) return TG_ERR_INVALID;
+        }
+    }
+    int num_inner_entities = 0;
+    for (int e = 0; e < num_entities; e++) {
+        if (entity_cell_off[e + 1] < entity_cell_off[e] || !entity_names[e]) return TG_ERR_INVALID;
+        if (entity_cell_off[e + 1] <= num_inner_cells) num_inner_entities = e + 1;
+    }
+    if (entity_cell_off[num_inner_entities] != num_inner_cells) return TG_ERR_INVALID;
+    tg_host_mesh *m = new tg_host_mesh();
+    m->coord.resize(num_nodes);
+    for (int v = 0; v < num_nodes; v++) m->coord[v] = {coord[3 * v], coord[3 * v + 1], coord[3 * v + 2]};
+    m->num_cells = num_cells;
+    m->num_inner = num_inner_cells;
+    m->off_boundary = m->off_periodic = num_cells;
+    m->node_off.assign(node_off, node_off + num_cells + 1);
+    m->node_idx.assign(node_idx, node_idx + node_off[num_cells]);
+    m->num_inner_entities = num_inner_entities;
+    m->off_boundary_entities = num_entities;
+    for (int e = 0; e < num_entities; e++) {
+        Entity en{};
+        en.name = entity_names[e];
+        m->entities.push_back(en);
+    }
+    m->ent_cell_off.assign(entity_cell_off, entity_cell_off + num_entities + 1);
+    m->recv_off.assign(1, num_cells);
+    m->send_off.assign(1, 0);
+    int rc = generate(*m);
     if (rc != TG_OK) {
         delete m;
         return rc;

@@ -23,6 +23,10 @@ from oracle import ref  # noqa: E402
 from tests.cases import random_state, taylor_green, vortex  # noqa: E402
 
 FREE = [1.0, 0.6, 0.1, -0.05, 1.0 / 1.4]
+FREE_M25 = [1.0, 2.5, 0.0, 0.0, 1.0 / 1.4]  # Mach 2.5 (sound speed 1)
+RAMP_BCS = {"left": ["supersonic inflow", FREE_M25], "right": ["supersonic outflow", None],
+            "bottom": ["slipwall", None], "top": ["slipwall", None], "back": ["slipwall", None],
+            "front": ["slipwall", None]}
 SIDES = ["left", "right", "bottom", "top", "back", "front"]
 
 
@@ -59,7 +63,22 @@ def cases():
                     ns=False, flux="roe", limiter=None, coeff=0.0, state="freestream", seed=6,
                     bcs={s: ["farfield", FREE] for s in SIDES[:4]},
                     advance=dict(method="implicit euler", courant=20.0, nk=[0.1, 0.3, 10], steps=1)))
+    # the unstructured compression ramp (tetrahedra, prisms, hexahedra, pyramid transitions)
+    ramp = dict(kind="ramp", n=[10, 8, 6], block=4, seed=1)
+    out.append(dict(name="ramp_euler_ausmd_bj", mesh=ramp, ns=False, flux="ausmd", limiter="minmod", coeff=0.0,
+                    state="freestream", free=FREE_M25, seed=12, bcs=RAMP_BCS,
+                    advance=dict(method="lserk", courant=0.5, rk=[3, 3], steps=3)))
+    out.append(dict(name="ramp_ns_roe_venkat", mesh=ramp, ns=True, flux="roe", limiter="venkatakrishnan",
+                    coeff=1.0, mu=0.01, state="random", seed=13, mach=0.6,
+                    bcs={**RAMP_BCS, "bottom": ["adiabatic wall", None]},
+                    advance=dict(method="lserk", courant=0.8, rk=[3, 3], steps=2)))
     return out
+
+
+def ramp_cells(spec):
+    from teal_b200 import meshes
+
+    return meshes.ramp_mesh(n=tuple(spec["n"]), block=spec["block"], seed=spec["seed"])
 
 
 def make_state(case, center, num_cells):
@@ -68,14 +87,17 @@ def make_state(case, center, num_cells):
     if case["state"] == "tgv":
         return taylor_green(center)
     if case["state"] == "freestream":
-        p = np.tile(np.array(FREE), (num_cells, 1))
+        p = np.tile(np.array(case.get("free", FREE)), (num_cells, 1))
         p[:, 0] *= 1 + 0.05 * np.random.default_rng(case["seed"]).random(num_cells)
         return p
     return random_state(num_cells, case["seed"], mach=case["mach"])
 
 
 def ref_equations(case):
-    m = ref.RefMesh(case["lo"], case["hi"], case["n"], case["periodic"])
+    if "mesh" in case:
+        m = ref.RefMesh.from_cells(ramp_cells(case["mesh"]))
+    else:
+        m = ref.RefMesh(case["lo"], case["hi"], case["n"], case["periodic"])
     e = ref.RefEquations(m, case["ns"])
     e.set_space_order(case.get("order", 2))
     e.set_convective_flux(case["flux"])

@@ -25,7 +25,13 @@ def load():
 
 def equations(case):
     """Host mesh + teal_b200 Equations configured as the case."""
-    m = tb.Mesh.create(case["lo"], case["hi"], case["n"], case["periodic"])
+    if "mesh" in case:
+        from teal_b200 import meshes
+
+        spec = case["mesh"]
+        m = tb.Mesh.from_cells(meshes.ramp_mesh(n=tuple(spec["n"]), block=spec["block"], seed=spec["seed"]))
+    else:
+        m = tb.Mesh.create(case["lo"], case["hi"], case["n"], case["periodic"])
     e = tb.Equations.navierstokes(m) if case["ns"] else tb.Equations.euler(m)
     e.set_space_order(case.get("order", 2))
     e.set_convective_flux(case["flux"])

@@ -6,6 +6,7 @@ import pytest
 
 import teal_b200 as tb
 from oracle import ref
+from teal_b200 import meshes
 
 ARRAYS = ["cells.cell.off", "cells.cell.idx", "cells.volume", "cells.center", "cells.projection",
           "cells.offset", "faces.cell_idx", "faces.area", "faces.basis", "faces.weight", "faces.offset",
@@ -51,8 +52,49 @@ def test_jittered_mesh_matches_reference():
 
 @pytest.mark.parametrize("case", CASES)
 def test_mesh_invariants(case):
+    check_invariants(tb.Mesh.create(*case))
+
+
+RAMPS = [dict(n=(10, 8, 6), block=4, seed=1), dict(n=(16, 12, 10), block=4, seed=2),
+         dict(n=(20, 16, 12), block=8, seed=5)]
+
+
+@needs_ref
+@pytest.mark.parametrize("spec", RAMPS)
+def test_unstructured_ramp_matches_reference_bit_for_bit(spec):
+    cells = meshes.ramp_mesh(**spec)
+    r = ref.RefMesh.from_cells(cells)
+    r.validate()  # teal_error would exit the process
+    a = r.arrays()
+    m = tb.Mesh.from_cells(cells)
+    for k in ARRAYS:
+        assert np.array_equal(a[k], m.array(k)), k
+    assert a["sum_volume"] == m.sum_volume
+    assert r.entities() == m.entities
+
+
+@pytest.mark.parametrize("spec", RAMPS)
+def test_unstructured_ramp_invariants(spec):
+    cells = meshes.ramp_mesh(**spec)
+    c = cells["counts"]
+    assert min(c["tetrahedra"], c["pyramids"], c["prisms"], c["hexahedra"]) > 0
+    assert c["tetrahedra"] + c["pyramids"] + c["prisms"] + c["hexahedra"] == cells["num_inner"]
+    m = tb.Mesh.from_cells(cells)
+    check_invariants(m)
+    # the ramp: the bottom wall is flat, then rises at 15 degrees
+    assert [e[0] for e in m.entities] == ["domain", "left", "right", "bottom", "top", "back", "front"]
+
+
+def test_nonconforming_cells_are_rejected():
+    cells = meshes.ramp_mesh(n=(6, 5, 4), block=2, seed=0)
+    cells["node_idx"] = cells["node_idx"].copy()
+    cells["node_idx"][:4] = cells["node_idx"][0]  # a degenerate tetrahedron
+    with pytest.raises(tb.TealError):
+        tb.Mesh.from_cells(cells)
+
+
+def check_invariants(m):
     """Integer and geometric invariants of mesh_validate, recomputed in numpy."""
-    m = tb.Mesh.create(*case)
     s = m.struct
     C, N, F = s.num_inner_cells, s.num_cells, s.num_faces
     lr = m.array("faces.cell_idx")
