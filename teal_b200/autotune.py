@@ -1,11 +1,13 @@
 """Autotuner of the hot kernels' launch shapes.
 
 Builds the library once per candidate of (face-flux block size, face-flux blocks resident per SM,
-cell-gather block size) into a scratch directory, times a fixed number of RK steps of a workload on
-the current GPU with each build (a fresh process per build, selected with TEAL_B200_LIBRARY), and
-writes the fastest shape to teal_b200/csrc/tuned.h (and to --out when given).
+face geometry staged by bulk copies or loaded, cell-gather block size) into a scratch directory,
+times a fixed number of RK steps of a workload on the current GPU with each build (a fresh process
+per build, selected with TEAL_B200_LIBRARY), and writes the fastest shape to
+teal_b200/csrc/tuned.h (and to --out when given). Shapes and the Navier-Stokes staging switch are
+tuned on the Taylor-Green vortex, the Euler staging switch on the unstructured ramp.
 
-    python -m teal_b200.autotune [--n 96] [--steps 10] [--precision fp64] [--out gpurun_out/tuned.h]
+    python -m teal_b200.autotune [--n 96] [--ramp-n 64] [--steps 10] [--precision fp64] [--out gpurun_out/tuned.h]
 
 Needs nvcc and a GPU. Every candidate computes the same results; only speed differs.
 """
@@ -24,16 +26,19 @@ CSRC = os.path.join(HERE, "csrc")
 ROOT = os.path.dirname(HERE)
 
 # face-flux block size x resident face threads per SM (65536 registers / threads = the cap per
-# thread: 512 -> 128, 768 -> 85, 1024 -> 64) x cell-gather block size
+# thread: 512 -> 128, 768 -> 85) x geometry staged in shared memory by bulk copies or loaded by the
+# threads x cell-gather block size. The Navier-Stokes workload tunes the shapes and its staging
+# switch; the Euler staging switch is then tuned on the unstructured ramp with the chosen shapes.
 FACE_BLOCKS = [128, 256]
-FACE_THREADS = [512, 768, 1024]
-CELL_BLOCKS = [128, 256]
+FACE_THREADS = [512, 768]
+STAGED = [0, 1]
+CELL_BLOCKS = [256]
 
 TIMER = r"""
 import json, math, sys, time
 import torch
 import teal_b200 as tb
-n, steps, prec = int(sys.argv[1]), int(sys.argv[2]), sys.argv[3]
+n, steps, prec, workload = int(sys.argv[1]), int(sys.argv[2]), sys.argv[3], sys.argv[4]
 def tgv(c, gamma=1.4, mach=0.1):
     import numpy as np
     x, y, z = c[:, 0], c[:, 1], c[:, 2]
@@ -44,10 +49,23 @@ def tgv(c, gamma=1.4, mach=0.1):
     out[:, 4] = p0 + (np.cos(2 * x) + np.cos(2 * y)) * (np.cos(2 * z) + 2) / 16
     out[:, 0] = out[:, 4] / p0
     return out
-m = tb.Mesh.create((0, 0, 0), (2 * math.pi,) * 3, (n, n, n), (1, 1, 1))
-e = tb.Equations.navierstokes(m)
-e.set_convective_flux("roe"); e.set_limiter("venkatakrishnan", 1.0); e.set_property("dynamic viscosity", 1 / 1600)
-e.set_initial_condition("domain", tgv)
+if workload == "tgv":
+    m = tb.Mesh.create((0, 0, 0), (2 * math.pi,) * 3, (n, n, n), (1, 1, 1))
+    e = tb.Equations.navierstokes(m)
+    e.set_convective_flux("roe"); e.set_limiter("venkatakrishnan", 1.0); e.set_property("dynamic viscosity", 1 / 1600)
+    e.set_initial_condition("domain", tgv)
+else:
+    import numpy as np
+    from teal_b200 import meshes
+    m = tb.Mesh.from_cells(meshes.ramp_mesh(n=(n, n, n)))
+    e = tb.Equations.euler(m)
+    e.set_convective_flux("ausmd"); e.set_limiter("minmod", 0.0)
+    free = (1.0, 2.5, 0.0, 0.0, 1.0 / 1.4)
+    e.set_boundary_condition("left", "supersonic inflow", free)
+    e.set_boundary_condition("right", "supersonic outflow")
+    for side in ("bottom", "top", "back", "front"):
+        e.set_boundary_condition(side, "slipwall")
+    e.set_initial_condition("domain", lambda c: np.tile(np.array(free), (c.shape[0], 1)))
 ctx = e.context(tb.TG_PRECISION_FP64 if prec == "fp64" else tb.TG_PRECISION_FP32_FLUX)
 s = torch.cuda.Stream(); ctx.set_stream(s.cuda_stream)
 ctx.run(tb.TG_ADVANCE_LSERK, 0.99, 3, context=(3, 3)); torch.cuda.synchronize()
@@ -72,9 +90,9 @@ def build(variant, workdir, jobs):
     return name, out
 
 
-def time_variant(lib, n, steps, precision):
+def time_variant(lib, n, steps, precision, workload="tgv"):
     env = dict(os.environ, TEAL_B200_LIBRARY=lib, PYTHONPATH=ROOT + os.pathsep + os.environ.get("PYTHONPATH", ""))
-    r = subprocess.run([sys.executable, "-c", TIMER, str(n), str(steps), precision], capture_output=True,
+    r = subprocess.run([sys.executable, "-c", TIMER, str(n), str(steps), precision, workload], capture_output=True,
                        text=True, env=env, timeout=600)
     if r.returncode != 0:
         raise RuntimeError(r.stderr[-2000:])
@@ -82,11 +100,16 @@ def time_variant(lib, n, steps, precision):
 
 
 def write_header(path, best):
-    lines = ["// Launch shapes of the hot kernels, chosen by teal_b200/autotune.py on a B200 (fastest",
-             "// measured RK step); a value given with -D at build time wins.", "#pragma once", ""]
+    lines = ["// Launch shapes of the hot kernels, chosen by teal_b200/autotune.py on a B200 (fastest measured",
+             "// RK step, TGV for the shapes and the Navier-Stokes staging switch, the ramp for the Euler",
+             "// staging switch; times within 0.5 % of the fastest count as ties, resolved to fewer resident",
+             "// face blocks, i.e. more registers per thread); a value given with -D at build time wins.",
+             "#pragma once", ""]
     notes = {"TG_FACE_BLOCK": "threads per face-flux block",
              "TG_FACE_MINB": "face-flux blocks kept resident per SM (caps registers per thread)",
-             "TG_CELL_BLOCK": "threads per cell-gather block"}
+             "TG_CELL_BLOCK": "threads per cell-gather block",
+             "TG_FACE_STAGED_NS": "Navier-Stokes face kernel: geometry staged by bulk copies (1) or loaded (0)",
+             "TG_FACE_STAGED_EULER": "Euler face kernel: geometry staged by bulk copies (1) or loaded (0)"}
     for k, v in best.items():
         lines += [f"#ifndef {k}", f"#define {k} {v}  // {notes[k]}", "#endif"]
     with open(path, "w") as f:
@@ -96,33 +119,45 @@ def write_header(path, best):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=96)
+    ap.add_argument("--ramp-n", type=int, default=64, help="grid of the unstructured ramp (Euler staging switch)")
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--out", default=None, help="also write the chosen header here")
     ap.add_argument("--jobs", type=int, default=os.cpu_count() or 8)
     args = ap.parse_args()
-    variants = [{"TG_FACE_BLOCK": fb, "TG_FACE_MINB": ft // fb, "TG_CELL_BLOCK": cb}
-                for fb, ft, cb in itertools.product(FACE_BLOCKS, FACE_THREADS, CELL_BLOCKS)]
-    results = []
-    with tempfile.TemporaryDirectory() as work:
-        per = max(2, args.jobs // 4)
+    variants = [{"TG_FACE_BLOCK": fb, "TG_FACE_MINB": ft // fb, "TG_CELL_BLOCK": cb, "TG_FACE_STAGED_NS": st}
+                for fb, ft, st, cb in itertools.product(FACE_BLOCKS, FACE_THREADS, STAGED, CELL_BLOCKS)]
+
+    def sweep(variants, workload, n, work, per):
         with concurrent.futures.ThreadPoolExecutor(max_workers=4) as pool:
             built = list(pool.map(lambda v: (v,) + build(v, work, per), variants))
+        results = []
         for v, name, lib in built:
             try:
-                ms = time_variant(lib, args.n, args.steps, args.precision)
+                ms = time_variant(lib, n, args.steps, args.precision, workload)
             except Exception as exc:  # a variant that fails is reported and skipped
                 print(json.dumps({"variant": v, "error": str(exc)[-300:]}), flush=True)
                 continue
             results.append((ms, v))
-            print(json.dumps({"variant": v, "ms_per_step": ms}), flush=True)
-    if not results:
-        raise SystemExit("no variant ran")
-    ms, best = min(results, key=lambda r: r[0])
+            print(json.dumps({"variant": v, "workload": workload, "ms_per_step": ms}), flush=True)
+        if not results:
+            raise SystemExit("no variant ran")
+        # times within 0.5 % of the fastest are ties: take the one with the fewest resident face
+        # threads per SM (most registers per thread, fewest spills)
+        fastest = min(r[0] for r in results)
+        ties = [r for r in results if r[0] <= 1.005 * fastest]
+        return min(ties, key=lambda r: (r[1]["TG_FACE_BLOCK"] * r[1]["TG_FACE_MINB"], r[0]))
+
+    with tempfile.TemporaryDirectory() as work:
+        per = max(2, args.jobs // 4)
+        ms, best = sweep(variants, "tgv", args.n, work, per)
+        euler = [dict(best, TG_FACE_STAGED_EULER=st) for st in STAGED]
+        ms_e, best = sweep(euler, "ramp", args.ramp_n, work, per)
     write_header(os.path.join(CSRC, "tuned.h"), best)
     if args.out:
         write_header(args.out, best)
-    print(json.dumps({"best": best, "ms_per_step": ms, "workload": f"tgv {args.n}^3 {args.precision}"}))
+    print(json.dumps({"best": best, "ms_per_step": ms, "workload": f"tgv {args.n}^3 {args.precision}",
+                      "ramp_ms_per_step": ms_e}))
 
 
 if __name__ == "__main__":

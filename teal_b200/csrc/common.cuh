@@ -9,6 +9,9 @@
 
 namespace tg {
 
+// bits of the device error word (Steps::error)
+enum DeviceError { ERR_NONFINITE = 1, ERR_TIMEOUT = 2 };
+
 constexpr int BLOCK = 256;
 constexpr int FACE_BLOCK = TG_FACE_BLOCK;
 constexpr int FACE_MINB = TG_FACE_MINB;

@@ -129,7 +129,8 @@ static int dalloc(T **p, size_t n)
 {
     *p = nullptr;
     if (n == 0) n = 1;
-    cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+    // 64 bytes of slack: bulk copies of a tile may read up to 15 bytes past the last element
+    cudaError_t e = cudaMalloc((void **)p, n * sizeof(T) + 64);
     if (e != cudaSuccess) {
         *p = nullptr;
         return fail(TG_ERR_OOM, "cudaMalloc of %zu bytes failed: %s", n * sizeof(T), cudaGetErrorString(e));
@@ -846,6 +847,9 @@ static int create_ctx(MeshInput &in, const tg_equations *e, int precision, tg_ct
             hi_at(c, SI_MAX_ITER, i) = 0x7fffffff;
             hi_at(c, SI_ACTIVE, i) = 1;
         }
+        // the device copy starts as the host mirror (error word clear)
+        CU(cudaMemcpyAsync(c->sd, c->hd, sizeof(double) * SD_COUNT * c->ninst, cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(c->si, c->hi, sizeof(int) * (SI_COUNT * c->ninst + 2), cudaMemcpyHostToDevice, st));
         int n = c->ninst;
         c->st = Steps{c->sd + SD_TIME * n,     c->sd + SD_STEP * n,      c->sd + SD_STEP0 * n,
                       c->sd + SD_MAX_STEP * n, c->sd + SD_MAX_TIME * n,  c->sd + SD_THRESHOLD * n,
@@ -1089,6 +1093,7 @@ static int run_face(tg_ctx *c, const double *q)
     a.mu = c->prop[1];
     a.prandtl = c->prop[2];
     a.G = c->G;
+    a.err = c->st.error;
     bool ns = c->viscous == TG_VISCOUS_CENTRAL;
     bool fold = fold_psi(c);
     Launch l(c, TG_PROF_FACE);
@@ -1189,9 +1194,11 @@ static int write_steps(tg_ctx *c)
 
 static int check_error(tg_ctx *c)
 {
-    if (hi_error(c)) {
+    int e = hi_error(c);
+    if (e) {
         hi_error(c) = 0;
         write_steps(c);
+        if (e & ERR_TIMEOUT) return fail(TG_ERR_TIMEOUT, "a device-side wait for staged face geometry gave up");
         return fail(TG_ERR_NONFINITE, "non-finite time step or residual");
     }
     return TG_OK;
@@ -1224,6 +1231,8 @@ extern "C" int tg_derivative(tg_ctx *c, const double *prim, double *deriv, doubl
     k_soa5_to_aos<<<grid_of(c->s.C), BLOCK, 0, c->stream>>>(c->s.C, c->R, c->aos);
     CU(cudaGetLastError());
     TRY(d2h(c, deriv, c->aos, 5 * (size_t)c->s.C));
+    TRY(read_steps(c));
+    TRY(check_error(c));
     return TG_OK;
 }
 

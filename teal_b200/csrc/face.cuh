@@ -2,6 +2,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "tma.cuh"
 
 namespace tg {
 
@@ -30,21 +31,112 @@ __device__ __forceinline__ void reconstruct(const Prim<R> &q, const R *__restric
     }
 }
 
-// One thread per face. The convective flux comes first (its reconstruction streams the limited
-// gradients), the viscous flux second (its face-averaged gradient re-reads the unlimited gradients,
-// which are still in L1); FACE_MINB caps the registers so that many blocks stay resident per SM.
-template <typename R, int FK, bool NS, int ORDER, bool FOLD>
-__global__ void __launch_bounds__(FACE_BLOCK, FACE_MINB) k_face(Sizes s, Geometry<R> g, const double *__restrict__ q,
-                                                   const R *__restrict__ rec, R gamma, R mu, R prandtl,
-                                                   R *__restrict__ G)
-{
-    int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= s.F) {
-        return;
+// Two ways to reach the geometry of a face: straight from the SoA arrays (DirectGeo, one face per
+// thread, loads issued by the thread) or from a tile staged in shared memory (FaceTile, bulk
+// asynchronous copies). Both expose the same accessors; `i` is the face's element in the tile.
+
+template <typename R>
+struct DirectGeo {
+    const Geometry<R> &g;
+    int F, f;
+    __device__ __forceinline__ int2 cells(int) const { return g.lr[f]; }
+    __device__ __forceinline__ Basis<R> basis(int) const { return load_basis(g.basis, F, f); }
+    // the basis again later in the thread: re-read (L1) instead of kept live in registers
+    __device__ __forceinline__ Basis<R> basis_again(int) const { return reload_basis(g.basis, F, f); }
+    __device__ __forceinline__ V3<R> normal_again(int) const
+    {
+        return v3(reload(g.basis + f), reload(g.basis + F + f), reload(g.basis + 2 * F + f));
     }
-    const int F = s.F, N = s.N;
+    __device__ __forceinline__ V3<R> offl(int) const { return load_v3(g.offl, F, f); }
+    __device__ __forceinline__ V3<R> offr(int) const { return load_v3(g.offr, F, f); }
+    __device__ __forceinline__ R area(int) const { return __ldg(g.area + f); }
+    __device__ __forceinline__ V3<R> corr(int) const { return load_v3(g.corr, F, f); }
+    __device__ __forceinline__ R corr_norm(int) const { return __ldg(g.corr + 3 * F + f); }
+};
+
+// Geometry of one tile of FACE_BLOCK consecutive faces in shared memory, staged by bulk
+// asynchronous copies (one per SoA row, all in flight at once, completing on one mbarrier) so the
+// streamed face geometry costs the threads neither registers nor load instructions; rows: area,
+// basis (9), offsets left / right (3 + 3, second order), correction (4, Navier-Stokes).
+template <typename R, int ORDER, bool NS>
+struct FaceTile {
+    static constexpr int PAD = 16 / int(sizeof(R));
+    static constexpr int SROW = FACE_BLOCK + PAD;
+    static constexpr int ROWS = 10 + (ORDER == 2 ? 6 + (NS ? 4 : 0) : 0);
+    static constexpr int R_AREA = 0, R_BASIS = 1, R_OFFL = 10, R_OFFR = 13, R_CORR = (ORDER == 2) ? 16 : 10;
+    R geo[ROWS][SROW];
+    int2 lr[FACE_BLOCK + 2];
+    uint64_t bar;
+    uint8_t shift[ROWS + 1];  // elements before the tile's first face in each staged row
+
+    __device__ __forceinline__ const R *row_src(const Geometry<R> &g, int F, int r) const
+    {
+        if (r == R_AREA) return g.area;
+        if (r < R_BASIS + 9) return g.basis + (size_t)(r - R_BASIS) * F;
+        if (ORDER == 2 && r < R_OFFL + 3) return g.offl + (size_t)(r - R_OFFL) * F;
+        if (ORDER == 2 && r < R_OFFR + 3) return g.offr + (size_t)(r - R_OFFR) * F;
+        return g.corr + (size_t)(r - R_CORR) * F;
+    }
+
+    // thread 0 issues the copies of faces [f0, f0 + n); every thread then waits (bounded).
+    // Returns false after a wait that gave up (the error word then has the timeout bit); the
+    // decision is the same in every thread of the block.
+    __device__ __forceinline__ bool stage(const Geometry<R> &g, int F, int f0, int n, int *err)
+    {
+        if (threadIdx.x == 0) {
+            mbar_init(&bar, 1);
+            uint32_t total = stage_span(lr, g.lr + f0, n, &bar, false, &shift[ROWS]);
+            for (int r = 0; r < ROWS; r++) {
+                total += stage_span(geo[r], row_src(g, F, r) + f0, n, &bar, false, &shift[r]);
+            }
+            mbar_arrive_expect_tx(&bar, total);
+            stage_span(lr, g.lr + f0, n, &bar, true, nullptr);
+            for (int r = 0; r < ROWS; r++) {
+                stage_span(geo[r], row_src(g, F, r) + f0, n, &bar, true, nullptr);
+            }
+        }
+        __syncthreads();
+        const bool ok = mbar_wait_bounded(&bar, 0);
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) {
+                atomicOr(err, ERR_TIMEOUT);
+            }
+            mbar_wait_bounded(&bar, 0);  // let copies still in flight land before the block exits
+            return false;
+        }
+        return true;
+    }
+
+    __device__ __forceinline__ R at(int r, int i) const { return geo[r][shift[r] + i]; }
+    __device__ __forceinline__ V3<R> v3_at(int r, int i) const { return v3(at(r, i), at(r + 1, i), at(r + 2, i)); }
+    __device__ __forceinline__ int2 cells(int i) const { return lr[shift[ROWS] + i]; }
+    __device__ __forceinline__ Basis<R> basis(int i) const
+    {
+        Basis<R> b;
+        b.x = v3_at(R_BASIS, i);
+        b.y = v3_at(R_BASIS + 3, i);
+        b.z = v3_at(R_BASIS + 6, i);
+        return b;
+    }
+    __device__ __forceinline__ Basis<R> basis_again(int i) const { return basis(i); }
+    __device__ __forceinline__ V3<R> normal_again(int i) const { return v3_at(R_BASIS, i); }
+    __device__ __forceinline__ V3<R> offl(int i) const { return v3_at(R_OFFL, i); }
+    __device__ __forceinline__ V3<R> offr(int i) const { return v3_at(R_OFFR, i); }
+    __device__ __forceinline__ R area(int i) const { return at(R_AREA, i); }
+    __device__ __forceinline__ V3<R> corr(int i) const { return v3_at(R_CORR, i); }
+    __device__ __forceinline__ R corr_norm(int i) const { return at(R_CORR + 3, i); }
+};
+
+// The flux record of face f (element i of its tile). The convective flux comes first (its
+// reconstruction streams the limited gradients), the viscous flux second (its face-averaged
+// gradient re-reads the unlimited gradients, which are still in L1).
+template <typename R, int FK, bool NS, int ORDER, bool FOLD, typename Geo>
+__device__ __forceinline__ void face_flux(const Geo &geo, int i, int f, const Sizes &s, const double *__restrict__ q,
+                                          const R *__restrict__ rec, R gamma, R mu, R prandtl, R *__restrict__ G)
+{
+    const int N = s.N;
     const bool boundary = (f >= s.F_in) && (f < s.F_bd);
-    int2 c = g.lr[f];
+    const int2 c = geo.cells(i);
 
     // convective flux: the basis and the cell states are dead while the flux runs in the face frame
     // and are re-read afterwards
@@ -54,35 +146,34 @@ __global__ void __launch_bounds__(FACE_BLOCK, FACE_MINB) k_face(Sizes s, Geometr
         {
             Prim<R> ql = load_prim<R>(q, N, c.x);
             Prim<R> qr = load_prim<R>(q, N, c.y);
-            Basis<R> b = load_basis(g.basis, F, f);
+            Basis<R> b = geo.basis(i);
             if (ORDER == 1) {
                 l = make_local(ql, gamma, b);
                 r = make_local(qr, gamma, b);
             }
             else {
                 R pl[5], pr[5];
-                reconstruct<R, FOLD>(ql, rec, c.x, load_v3(g.offl, F, f), pl);
+                reconstruct<R, FOLD>(ql, rec, c.x, geo.offl(i), pl);
                 if (boundary) {  // the ghost state enters unreconstructed (derivative.c:203-211)
                     pr[0] = qr.rho, pr[1] = qr.u.x, pr[2] = qr.u.y, pr[3] = qr.u.z, pr[4] = qr.p;
                 }
                 else {
-                    reconstruct<R, FOLD>(qr, rec, c.y, load_v3(g.offr, F, f), pr);
+                    reconstruct<R, FOLD>(qr, rec, c.y, geo.offr(i), pr);
                 }
                 l = make_local(prim_from(pl), gamma, b);
                 r = make_local(prim_from(pr), gamma, b);
             }
         }
         fc = convective_flux_local<FK>(l, r, gamma);
-        fc.m = to_global(reload_basis(g.basis, F, f), fc.m);
+        fc.m = to_global(geo.basis_again(i), fc.m);
     }
-    R area = __ldg(g.area + f);
+    R area = geo.area(i);
     R gf[5] = {fc.rho * area, fc.m.x * area, fc.m.y * area, fc.m.z * area, fc.e * area};
 
     if (NS && ORDER == 2) {
         // face average corrected along the centre-to-centre direction (derivative.c:71-89)
         Prim<R> ql = reload_prim<R>(q, N, c.x);
         Prim<R> qr = reload_prim<R>(q, N, c.y);
-        Basis<R> b = reload_basis(g.basis, F, f);
         R qlv[5] = {ql.rho, ql.u.x, ql.u.y, ql.u.z, ql.p};
         R qrv[5] = {qr.rho, qr.u.x, qr.u.y, qr.u.z, qr.p};
         R qm[5], gm[15];
@@ -102,8 +193,8 @@ __global__ void __launch_bounds__(FACE_BLOCK, FACE_MINB) k_face(Sizes s, Geometr
                 gm[3 * v] = (ax + bx) / R(2), gm[3 * v + 1] = (ay + by) / R(2), gm[3 * v + 2] = (az + bz) / R(2);
             }
         }
-        V3<R> unit = load_v3(g.corr, F, f);
-        R norm = __ldg(g.corr + 3 * F + f);
+        V3<R> unit = geo.corr(i);
+        R norm = geo.corr_norm(i);
 #pragma unroll
         for (int v = 0; v < 5; v++) {
             V3<R> gv = v3(gm[3 * v], gm[3 * v + 1], gm[3 * v + 2]);
@@ -119,7 +210,12 @@ __global__ void __launch_bounds__(FACE_BLOCK, FACE_MINB) k_face(Sizes s, Geometr
         gg.uy = v3(gm[6], gm[7], gm[8]);
         gg.uz = v3(gm[9], gm[10], gm[11]);
         gg.p = v3(gm[12], gm[13], gm[14]);
-        Cons<R> fv = viscous_central(prim_from(qm), gg, gamma, mu, prandtl, b);
+        // the viscous flux needs only the normal row of the basis
+        Basis<R> nb;
+        nb.x = geo.normal_again(i);
+        nb.y = nb.x;
+        nb.z = nb.x;
+        Cons<R> fv = viscous_central(prim_from(qm), gg, gamma, mu, prandtl, nb);
         gf[0] -= fv.rho * area;
         gf[1] -= fv.m.x * area;
         gf[2] -= fv.m.y * area;
@@ -127,6 +223,41 @@ __global__ void __launch_bounds__(FACE_BLOCK, FACE_MINB) k_face(Sizes s, Geometr
         gf[4] -= fv.e * area;
     }
     flux_rec_store(G, f, gf);
+}
+
+// One thread per face, geometry loaded by the threads. FACE_MINB caps the registers so that
+// several blocks stay resident per SM.
+template <typename R, int FK, bool NS, int ORDER, bool FOLD>
+__global__ void __launch_bounds__(FACE_BLOCK, FACE_MINB) k_face(Sizes s, Geometry<R> g, const double *__restrict__ q,
+                                                   const R *__restrict__ rec, R gamma, R mu, R prandtl,
+                                                   R *__restrict__ G)
+{
+    const int f = blockIdx.x * FACE_BLOCK + threadIdx.x;
+    if (f >= s.F) {
+        return;
+    }
+    DirectGeo<R> geo{g, s.F, f};
+    face_flux<R, FK, NS, ORDER, FOLD>(geo, 0, f, s, q, rec, gamma, mu, prandtl, G);
+}
+
+// One tile of FACE_BLOCK faces per block, its geometry staged in shared memory by bulk copies
+// before the threads (one face each) start. A wait that gives up sets ERR_TIMEOUT in the error
+// word and ends the block.
+template <typename R, int FK, bool NS, int ORDER, bool FOLD>
+__global__ void __launch_bounds__(FACE_BLOCK, FACE_MINB) k_face_staged(Sizes s, Geometry<R> g,
+                                                          const double *__restrict__ q,
+                                                          const R *__restrict__ rec, R gamma, R mu,
+                                                          R prandtl, R *__restrict__ G, int *err)
+{
+    __shared__ __align__(16) FaceTile<R, ORDER, NS> t;
+    const int f0 = blockIdx.x * FACE_BLOCK;
+    const int n = min(FACE_BLOCK, s.F - f0);
+    if (!t.stage(g, s.F, f0, n, err)) {
+        return;
+    }
+    if (threadIdx.x < n) {
+        face_flux<R, FK, NS, ORDER, FOLD>(t, threadIdx.x, f0 + threadIdx.x, s, q, rec, gamma, mu, prandtl, G);
+    }
 }
 
 }  // namespace tg

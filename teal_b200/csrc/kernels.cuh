@@ -339,7 +339,7 @@ __global__ void __launch_bounds__(INST_BLOCK) k_inst_begin(Segments seg, const d
         st.step0[i] = step0;
         st.step[i] = fmin(step0, clip);
         if (!isfinite(step0) || !(step0 > 0)) {
-            atomicExch(st.error, 1);
+            atomicOr(st.error, ERR_NONFINITE);
         }
     }
 }
@@ -376,7 +376,7 @@ __global__ void __launch_bounds__(INST_BLOCK) k_inst_end(Segments seg, const dou
         st.residual[5 * i + k] = res[k];
         mx = (res[k] > mx) ? res[k] : mx;
         if (!isfinite(res[k])) {
-            atomicExch(st.error, 1);
+            atomicOr(st.error, ERR_NONFINITE);
         }
     }
     if (!advance) {

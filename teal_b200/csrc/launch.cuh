@@ -15,27 +15,41 @@ struct FaceLaunch {
     const void *rec;
     double gamma, mu, prandtl;
     void *G;
+    int *err;  // device error word (bounded waits that give up set ERR_TIMEOUT)
 };
 
+template <typename R, int FK, bool NS, int ORDER, bool FOLD>
+inline void launch_face_v(bool staged, const FaceLaunch &a, const Geometry<R> &g, const R *rec, R *G, cudaStream_t st)
+{
+    dim3 grid((a.s.F + FACE_BLOCK - 1) / FACE_BLOCK);
+    R gm = R(a.gamma), mu = R(a.mu), pr = R(a.prandtl);
+    if (staged) {
+        k_face_staged<R, FK, NS, ORDER, FOLD><<<grid, FACE_BLOCK, 0, st>>>(a.s, g, a.q, rec, gm, mu, pr, G, a.err);
+    }
+    else {
+        k_face<R, FK, NS, ORDER, FOLD><<<grid, FACE_BLOCK, 0, st>>>(a.s, g, a.q, rec, gm, mu, pr, G);
+    }
+}
+
+// staged geometry (bulk copies into shared memory) or thread loads, per physics (tuned.h)
 template <int FK, typename R>
 inline cudaError_t launch_face_r(bool ns, int order, bool fold, const FaceLaunch &a, cudaStream_t st)
 {
     const Geometry<R> &g = *static_cast<const Geometry<R> *>(a.geom);
     const R *rec = static_cast<const R *>(a.rec);
     R *G = static_cast<R *>(a.G);
-    dim3 grid((a.s.F + FACE_BLOCK - 1) / FACE_BLOCK);
-    R gm = R(a.gamma), mu = R(a.mu), pr = R(a.prandtl);
+    const bool staged = ns ? (TG_FACE_STAGED_NS != 0) : (TG_FACE_STAGED_EULER != 0);
     if (order == 1) {
-        k_face<R, FK, false, 1, true><<<grid, FACE_BLOCK, 0, st>>>(a.s, g, a.q, rec, gm, mu, pr, G);
+        launch_face_v<R, FK, false, 1, true>(staged, a, g, rec, G, st);
     }
     else if (!ns) {
-        k_face<R, FK, false, 2, true><<<grid, FACE_BLOCK, 0, st>>>(a.s, g, a.q, rec, gm, mu, pr, G);
+        launch_face_v<R, FK, false, 2, true>(staged, a, g, rec, G, st);
     }
     else if (fold) {
-        k_face<R, FK, true, 2, true><<<grid, FACE_BLOCK, 0, st>>>(a.s, g, a.q, rec, gm, mu, pr, G);
+        launch_face_v<R, FK, true, 2, true>(staged, a, g, rec, G, st);
     }
     else {
-        k_face<R, FK, true, 2, false><<<grid, FACE_BLOCK, 0, st>>>(a.s, g, a.q, rec, gm, mu, pr, G);
+        launch_face_v<R, FK, true, 2, false>(staged, a, g, rec, G, st);
     }
     return cudaGetLastError();
 }

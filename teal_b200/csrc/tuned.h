@@ -1,6 +1,7 @@
-// Launch shapes of the hot kernels, chosen by teal_b200/autotune.py on a B200 (fastest
-// measured RK step, TGV 96^3 FP64: 1.411 ms vs 1.455 ms for 256 / 2 / 256); a value given with -D
-// at build time wins.
+// Launch shapes of the hot kernels, chosen by teal_b200/autotune.py on a B200 (fastest measured
+// RK step, TGV 96^3 FP64 for the shapes and the Navier-Stokes staging switch, the 64^3 ramp for the
+// Euler staging switch; times within 0.5 % of the fastest count as ties, resolved to fewer
+// resident face blocks, i.e. more registers per thread); a value given with -D at build time wins.
 #pragma once
 
 #ifndef TG_FACE_BLOCK
@@ -11,4 +12,10 @@
 #endif
 #ifndef TG_CELL_BLOCK
 #define TG_CELL_BLOCK 256  // threads per cell-gather block
+#endif
+#ifndef TG_FACE_STAGED_NS
+#define TG_FACE_STAGED_NS 0  // Navier-Stokes face kernel: geometry staged by bulk copies (1) or loaded (0)
+#endif
+#ifndef TG_FACE_STAGED_EULER
+#define TG_FACE_STAGED_EULER 1  // Euler face kernel: geometry staged by bulk copies (1) or loaded (0)
 #endif
