@@ -326,6 +326,117 @@ def run_serving(args, world, rank):
     print(json.dumps(line))
 
 
+def batch_specs(count, seed=11, lo=8_000, hi=512_000):
+    """Instances of the batched workload: ramp-mesh sizes log-uniform in [lo, hi] cells, Mach
+    U(0.3, 3.0), flow angle U(0, 10) degrees, a mesh seed each."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        cells = math.exp(rng.uniform(math.log(lo), math.log(hi)))
+        n = max(8, int(round((cells / 4.64) ** (1.0 / 3.0))))  # the ramp grid holds ~4.64 cells per hex
+        out.append((n, float(rng.uniform(0.3, 3.0)), float(rng.uniform(0.0, 10.0)), 1000 * seed + i))
+    return out
+
+
+def batch_problem(spec):
+    """Euler on a mixed-element ramp mesh, far field around, slip walls at the ramp and the sides
+    (valid for subsonic and supersonic free streams), starting from the free stream."""
+    import teal_b200 as tb
+    from teal_b200 import meshes, serving
+
+    n, mach, angle, mseed = spec
+    m = tb.Mesh.from_cells(meshes.ramp_mesh(n=(n, n, n), seed=mseed))
+    e = tb.Equations.euler(m)
+    e.set_convective_flux("ausmd")
+    e.set_limiter("minmod", 0.0)
+    free = serving.free_stream(mach, angle)
+    for side in ("left", "right", "top"):
+        e.set_boundary_condition(side, "farfield", free)
+    for side in ("bottom", "back", "front"):
+        e.set_boundary_condition(side, "slipwall")
+    e.primitive[:] = np.tile(free, (m.num_cells, 1))
+    return e
+
+
+def run_batch(args, world, rank):
+    """Batched forms: many ramp meshes of uneven size in one arena, advanced together (lserk, or
+    implicit Euler with Newton-GMRES), in FP64 and in the FP32-flux form, against the same meshes
+    solved one at a time in FP64. Reports throughput of each and the FP32-flux error against FP64."""
+    import torch
+
+    import teal_b200 as tb
+
+    if rank != 0:
+        return
+    torch.cuda.set_device(0)
+    specs = batch_specs(args.instances)
+    t0 = time.perf_counter()
+    problems = [batch_problem(sp) for sp in specs]
+    t_setup = time.perf_counter() - t0
+    cells = sum(e.mesh.num_inner_cells for e in problems)
+    implicit = args.method == "implicit"
+    method = tb.TG_ADVANCE_IMPLICIT_EULER if implicit else tb.TG_ADVANCE_LSERK
+    courant = 100.0 if implicit else 0.9
+    context = (0.1, 0.3, 30) if implicit else (3, 3)
+    steps = args.steps
+    stream = torch.cuda.Stream()
+
+    def timed(run):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        run()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / 1000.0
+
+    out, states = {}, {}
+    for name, prec in (("fp64", tb.TG_PRECISION_FP64), ("fp32_flux", tb.TG_PRECISION_FP32_FLUX)):
+        b = tb.Batch(problems, precision=prec)
+        b.set_stream(stream.cuda_stream)
+        b.run(method, courant, min(args.warmup, 3) if not implicit else 1, context=context)
+        for i, e in enumerate(problems):
+            b.set_primitive(i, e.primitive)
+        secs = timed(lambda: b.run(method, courant, steps, context=context))
+        out[name] = {"value": cells * steps / secs, "seconds": secs}
+        states[name] = [b.get_primitive(i)[: e.mesh.num_inner_cells].copy() for i, e in enumerate(problems)]
+        b.close()
+    err = 0.0
+    for a, f in zip(states["fp64"], states["fp32_flux"]):
+        d = np.sqrt(((f - a) ** 2).sum(axis=0)) / np.maximum(np.sqrt((a ** 2).sum(axis=0)), 1e-300)
+        err = max(err, float(d.max()))
+
+    # the same meshes one at a time in FP64 (a sample of them, throughput summed)
+    sample = problems[: min(len(problems), args.solo_sample)]
+    solo_cells, solo_secs = 0, 0.0
+    for e in sample:
+        ctx = tb.Context(e.mesh, e)
+        ctx.set_stream(stream.cuda_stream)
+        ctx.set_primitive(e.primitive)
+        ctx.run(method, courant, 1, context=context)
+        ctx.set_primitive(e.primitive)
+        solo_secs += timed(lambda: ctx.run(method, courant, steps, context=context))
+        solo_cells += e.mesh.num_inner_cells * steps
+        ctx.close()
+    solo = solo_cells / solo_secs
+    line = {
+        "metric": "cell-updates/s batched FP32-flux/FP64-accumulate vs plain FP64", "value": out["fp32_flux"]["value"],
+        "unit": "cell-updates/s", "n_gpus": 1, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": 1000 * out["fp32_flux"]["seconds"] / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32-flux/f64-accumulate", "data": "synthetic",
+        "config": {"workload": f"{len(problems)} euler ramp meshes (tets/prisms/hexes/pyramids), 8k-512k cells "
+                               f"log-uniform, mach 0.3-3.0, angle 0-10 deg, ausmd + barth-jespersen, "
+                               + ("implicit euler cfl 100, newton-krylov {0.1, 0.3, 30}" if implicit
+                                  else "lserk{3,3} cfl 0.9"),
+                   "cells": cells, "instances": len(problems)},
+        "batched_fp64": out["fp64"]["value"], "batched_fp32_flux": out["fp32_flux"]["value"],
+        "solo_fp64": solo, "solo_sample": len(sample),
+        "fp32_flux_over_solo_fp64": out["fp32_flux"]["value"] / solo,
+        "fp32_flux_rel_l2_vs_fp64": err, "setup_s": t_setup,
+    }
+    print(json.dumps(line))
+
+
 def run_reference_arm(args, world, rank):
     if rank != 0:
         return
@@ -358,9 +469,12 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="teal_b200")
-    ap.add_argument("--workload", default="tgv", choices=["tgv", "ramp", "serve"],
+    ap.add_argument("--workload", default="tgv", choices=["tgv", "ramp", "serve", "batch"],
                     help="tgv: Taylor-Green 128^3 (the headline); ramp: the unstructured compression ramp; "
-                         "serve: the solve server under Poisson arrivals")
+                         "serve: the solve server under Poisson arrivals; batch: many meshes in one arena")
+    ap.add_argument("--instances", type=int, default=64, help="batch: meshes in the arena")
+    ap.add_argument("--method", default="lserk", choices=["lserk", "implicit"], help="batch: time integrator")
+    ap.add_argument("--solo-sample", type=int, default=16, help="batch: meshes timed one at a time")
     ap.add_argument("--requests", type=int, default=16, help="serve: number of requests")
     ap.add_argument("--rate", type=float, default=8.0, help="serve: arrivals per second")
     ap.add_argument("--max-active", type=int, default=8, help="serve: concurrent solves")
@@ -382,6 +496,9 @@ def main():
         return
     if args.workload == "serve":
         run_serving(args, world, rank)
+        return
+    if args.workload == "batch":
+        run_batch(args, world, rank)
         return
 
     import torch
