@@ -156,8 +156,11 @@ struct Gmres {
     double *w = nullptr;      // [5][C]
     double *q1 = nullptr;     // [5][N] perturbed primitive state
     double *R1 = nullptr;     // [5][C] derivative of the perturbed state
-    double *part = nullptr;   // block partials
-    double *sc = nullptr;     // device scalars (GmresScalar)
+    double *part = nullptr;   // per-piece partial sums
+    double *sc = nullptr;     // per-instance device scalars (GmresScalar)
+    int *flag = nullptr;      // per-instance progress (GmresFlag)
+    int *count = nullptr;     // [2] instances still iterating (Newton, Arnoldi)
+    int *hcount = nullptr;    // pinned host copy of count
 };
 
 // Host mirror of the per-instance step arrays (pinned; one copy per direction moves all of them):
@@ -193,6 +196,7 @@ struct tg_ctx {
     int2 *lr = nullptr;
     int *slot_nbr = nullptr, *slot_face = nullptr;
     uint8_t *slot_cnt = nullptr;
+    bool full_slots = true;    // every inner cell has MAX_SLOTS faces
     int *owner = nullptr;      // periodic ghost -> owner cell
     int *bface_ent = nullptr;  // boundary face -> boundary index
     int *bkind = nullptr;      // boundary index -> TG_BC_*
@@ -290,7 +294,8 @@ static void free_ctx(tg_ctx *c)
         if (p) cudaFree(p);
     }
     void *gp[] = {c->gm.U, c->gm.Ustart, c->gm.r, c->gm.delta, c->gm.V, c->gm.w, c->gm.q1, c->gm.R1,
-                  c->gm.part, c->gm.sc};
+                  c->gm.part, c->gm.sc, c->gm.flag, c->gm.count};
+    if (c->gm.hcount) cudaFreeHost(c->gm.hcount);
     for (void *p : gp) {
         if (p) cudaFree(p);
     }
@@ -763,6 +768,15 @@ static int create_ctx(MeshInput &in, const tg_equations *e, int precision, tg_ct
                                                                   c->slot_face, c->slot_nbr, c->slot_cnt,
                                                                   c->gb.slot_w, c->gb.slot_off, d_err);
             CU(cudaGetLastError());
+            {
+                // meshes whose cells all have MAX_SLOTS faces (hexahedra) stage every slot row
+                // unconditionally in the gradient kernel; others skip padding slots
+                std::vector<uint8_t> cnt(s.C);
+                CU(cudaMemcpyAsync(cnt.data(), c->slot_cnt, s.C, cudaMemcpyDeviceToHost, st));
+                CU(cudaStreamSynchronize(st));
+                c->full_slots = true;
+                for (uint8_t k : cnt) c->full_slots = c->full_slots && k == MAX_SLOTS;
+            }
 
             // face geometry, structure of arrays
             TRY(upload(&c->gb.area, m->face_area, s.F, st));
@@ -1042,28 +1056,37 @@ static int run_boundary(tg_ctx *c, double *q, bool masked = false)
     return TG_OK;
 }
 
-template <typename R>
-static void launch_gradient(tg_ctx *c, const Geometry<R> &g, bool fold, const double *q)
+template <typename R, bool SKIP>
+static void launch_gradient_s(tg_ctx *c, const Geometry<R> &g, bool fold, const double *q)
 {
     dim3 grid((c->s.C + GRAD_CELLS - 1) / GRAD_CELLS);
     R *rec = (R *)c->grad;
     switch (c->limiter) {
         case TG_LIMITER_NONE:
-            k_gradient<R, 0, true><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
+            k_gradient<R, 0, true, SKIP><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
             break;
         case TG_LIMITER_BARTH_JESPERSEN:
             if (fold)
-                k_gradient<R, 1, true><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
+                k_gradient<R, 1, true, SKIP><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
             else
-                k_gradient<R, 1, false><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
+                k_gradient<R, 1, false, SKIP><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
             break;
         default:
             if (fold)
-                k_gradient<R, 2, true><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
+                k_gradient<R, 2, true, SKIP><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
             else
-                k_gradient<R, 2, false><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
+                k_gradient<R, 2, false, SKIP><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
             break;
     }
+}
+
+template <typename R>
+static void launch_gradient(tg_ctx *c, const Geometry<R> &g, bool fold, const double *q)
+{
+    if (c->full_slots)
+        launch_gradient_s<R, false>(c, g, fold, q);
+    else
+        launch_gradient_s<R, true>(c, g, fold, q);
 }
 
 // gradient with an explicit limiter choice (tg_gradient reports the unlimited one on request)
@@ -1382,8 +1405,31 @@ static int step_graph(tg_ctx *c, int method, int stages, const double *alpha, do
     return TG_OK;
 }
 
-static int implicit_euler_step(tg_ctx *c, const void *context, double courant, double *time,
-                               double max_step, double *residual, double *step0);
+static int implicit_step_all(tg_ctx *c, const void *context, double courant);
+static int implicit_run(tg_ctx *c, const void *context, double courant, int most);
+
+// one implicit step of a single mesh with the Advance semantics (time advanced by the step clipped
+// to max_step; residual and unclipped step returned)
+static int implicit_advance(tg_ctx *c, const void *context, double courant, double *time, double max_step,
+                            double *residual, double *step0)
+{
+    hd_at(c, SD_TIME, 0) = *time;
+    hd_at(c, SD_MAX_STEP, 0) = max_step;
+    hd_at(c, SD_THRESHOLD, 0) = 0.0;
+    hi_at(c, SI_ITER, 0) = 0;
+    hi_at(c, SI_MAX_ITER, 0) = 0x7fffffff;
+    hi_at(c, SI_ACTIVE, 0) = 1;
+    hi_error(c) = 0;
+    c->st.use_max_time = 0;
+    TRY(write_steps(c));
+    TRY(implicit_step_all(c, context, courant));
+    TRY(read_steps(c));
+    TRY(check_error(c));
+    *time = hd_at(c, SD_TIME, 0);
+    if (residual) residual_of(c, 0, residual);
+    if (step0) *step0 = hd_at(c, SD_STEP0, 0);
+    return TG_OK;
+}
 
 extern "C" int tg_advance(tg_ctx *c, int method, const void *context, double courant, double *time,
                           double max_step, double *residual, double *step0)
@@ -1392,7 +1438,7 @@ extern "C" int tg_advance(tg_ctx *c, int method, const void *context, double cou
     if (c->ninst != 1) return fail(TG_ERR_INVALID, "tg_advance takes a single-mesh context (batches: tg_batch_run)");
     if (!(courant > 0)) return fail(TG_ERR_INVALID, "invalid courant number (%g)", courant);
     if (method == TG_ADVANCE_IMPLICIT_EULER) {
-        return implicit_euler_step(c, context, courant, time, max_step, residual, step0);
+        return implicit_advance(c, context, courant, time, max_step, residual, step0);
     }
     if (method != TG_ADVANCE_EULER && method != TG_ADVANCE_LSERK)
         return fail(TG_ERR_INVALID, "invalid advance method (%d)", method);
@@ -1450,26 +1496,7 @@ extern "C" int tg_run(tg_ctx *c, int method, const void *context, double courant
     if (c->ninst != 1) return fail(TG_ERR_INVALID, "tg_run takes a single-mesh context (batches: tg_batch_run)");
     if (variable < -1 || variable > 4) return fail(TG_ERR_INVALID, "invalid termination variable");
     if (!(courant > 0)) return fail(TG_ERR_INVALID, "invalid courant number (%g)", courant);
-    if (method == TG_ADVANCE_IMPLICIT_EULER) {
-        // implicit steps synchronise inside the Newton loop; run them one by one
-        int it = 0;
-        double res[5] = {0, 0, 0, 0, 0};
-        while (it < max_iter && *time < max_time) {
-            double s0;
-            TRY(tg_advance(c, method, context, courant, time, max_time - *time, res, &s0));
-            it++;
-            if (threshold > 0) {
-                double m = 0;
-                for (int v = 0; v < 5; v++) m = res[v] > m ? res[v] : m;
-                if (((variable >= 0) ? res[variable] : m) < threshold) break;
-            }
-        }
-        *iter = it;
-        if (residual)
-            for (int v = 0; v < 5; v++) residual[v] = res[v];
-        return TG_OK;
-    }
-    if (method != TG_ADVANCE_EULER && method != TG_ADVANCE_LSERK)
+    if (method != TG_ADVANCE_EULER && method != TG_ADVANCE_LSERK && method != TG_ADVANCE_IMPLICIT_EULER)
         return fail(TG_ERR_INVALID, "invalid advance method (%d)", method);
     if (max_iter <= 0) {
         *iter = 0;
@@ -1483,9 +1510,16 @@ extern "C" int tg_run(tg_ctx *c, int method, const void *context, double courant
     hi_at(c, SI_MAX_ITER, 0) = max_iter;
     hi_at(c, SI_ACTIVE, 0) = 1;
     hi_error(c) = 0;
-    // stop tests that can end the run early are polled every step, a fixed count only at the end
-    int every = (threshold > 0 || max_time < DBL_MAX) ? 1 : max_iter;
-    TRY(run_instances(c, method, context, courant, max_iter, every));
+    if (method == TG_ADVANCE_IMPLICIT_EULER) {
+        // implicit steps synchronise inside the Newton loop anyway; the stop tests run every step
+        c->st.use_max_time = 1;
+        TRY(implicit_run(c, context, courant, max_iter));
+    }
+    else {
+        // stop tests that can end the run early are polled every step, a fixed count only at the end
+        int every = (threshold > 0 || max_time < DBL_MAX) ? 1 : max_iter;
+        TRY(run_instances(c, method, context, courant, max_iter, every));
+    }
     *time = hd_at(c, SD_TIME, 0);
     *iter = hi_at(c, SI_ITER, 0);
     if (residual) residual_of(c, 0, residual);
@@ -1497,8 +1531,8 @@ extern "C" int tg_batch_run(tg_ctx *c, int method, const void *context, double c
                             int *iter, double *residual)
 {
     if (!c || !max_iter || !time || !iter) return fail(TG_ERR_INVALID, "null argument");
-    if (method != TG_ADVANCE_EULER && method != TG_ADVANCE_LSERK)
-        return fail(TG_ERR_INVALID, "batches run the explicit methods (euler, lserk)");
+    if (method != TG_ADVANCE_EULER && method != TG_ADVANCE_LSERK && method != TG_ADVANCE_IMPLICIT_EULER)
+        return fail(TG_ERR_INVALID, "invalid advance method (%d)", method);
     if (!(courant > 0)) return fail(TG_ERR_INVALID, "invalid courant number (%g)", courant);
     int most = 0;
     bool early = false;
@@ -1516,7 +1550,13 @@ extern "C" int tg_batch_run(tg_ctx *c, int method, const void *context, double c
         early = early || hd_at(c, SD_THRESHOLD, i) > 0 || hd_at(c, SD_MAX_TIME, i) < DBL_MAX;
     }
     hi_error(c) = 0;
-    if (most > 0) TRY(run_instances(c, method, context, courant, most, early ? 8 : most));
+    if (most > 0 && method == TG_ADVANCE_IMPLICIT_EULER) {
+        c->st.use_max_time = 1;
+        TRY(implicit_run(c, context, courant, most));
+    }
+    else if (most > 0) {
+        TRY(run_instances(c, method, context, courant, most, early ? 8 : most));
+    }
     for (int i = 0; i < c->ninst; i++) {
         time[i] = hd_at(c, SD_TIME, i);
         iter[i] = hi_at(c, SI_ITER, i);
@@ -1526,15 +1566,21 @@ extern "C" int tg_batch_run(tg_ctx *c, int method, const void *context, double c
 }
 
 // ---- implicit Euler with Jacobian-free Newton-GMRES (advance.c:119-195, gmres.c:52-149) --------
+//
+// Every instance of the arena takes its own implicit step at once: its own CFL step, Newton and
+// Arnoldi iterations that stop on their own tests, masked out of the vector updates once done.
+// The host loops over Newton and Arnoldi iterations and reads, once per iteration, how many
+// instances go on.
 
 static int gm_alloc(tg_ctx *c, int dim)
 {
     Gmres &g = c->gm;
     if (g.V && g.dim >= dim) return TG_OK;
-    void *old[] = {g.U, g.Ustart, g.r, g.delta, g.V, g.w, g.q1, g.R1, g.part, g.sc};
+    void *old[] = {g.U, g.Ustart, g.r, g.delta, g.V, g.w, g.q1, g.R1, g.part, g.sc, g.flag, g.count};
     for (void *p : old) {
         if (p) cudaFree(p);
     }
+    if (g.hcount) cudaFreeHost(g.hcount);
     g = Gmres{};
     size_t n = 5 * (size_t)c->s.C;
     TRY(dalloc(&g.U, n));
@@ -1546,30 +1592,42 @@ static int gm_alloc(tg_ctx *c, int dim)
     TRY(dalloc(&g.q1, 5 * (size_t)c->s.N));
     CU(cudaMemset(g.q1, 0, 5 * sizeof(double) * c->s.N));
     TRY(dalloc(&g.R1, n));
-    TRY(dalloc(&g.part, 1024));
-    TRY(dalloc(&g.sc, GS_HEAD + (size_t)(dim + 1) * dim + 4 * (size_t)dim + 2));
+    TRY(dalloc(&g.part, (size_t)c->npieces));
+    TRY(dalloc(&g.sc, (size_t)c->ninst * gmres_scn(dim)));
+    TRY(dalloc(&g.flag, (size_t)GF_COUNT * c->ninst));
+    CU(cudaMemset(g.flag, 0, sizeof(int) * GF_COUNT * c->ninst));
+    TRY(dalloc(&g.count, 2));
+    CU(cudaMallocHost(&g.hcount, 2 * sizeof(int)));
     g.dim = dim;
     return TG_OK;
 }
 
-static const int DOT_BLOCKS = 1024;
-
-// dst = x . y (or |x| when x == y and take_sqrt)
-static int gm_dot(tg_ctx *c, const double *x, const double *y, double *dst, int take_sqrt)
+static GmresBatch gm_batch(tg_ctx *c, int dim)
 {
-    long n = 5L * c->s.C;
-    int nb = (int)((n + BLOCK - 1) / BLOCK);
-    nb = nb < DOT_BLOCKS ? nb : DOT_BLOCKS;
-    k_dot_part<<<nb, BLOCK, 0, c->stream>>>(n, x, y, c->gm.part);
-    k_reduce_scalar<<<1, REDUCE_BLOCK, 0, c->stream>>>(c->gm.part, nb, dst, take_sqrt);
+    return GmresBatch{dim, gmres_scn(dim), c->ninst, c->cell_inst, c->gm.sc, c->gm.flag, c->gm.count};
+}
+
+// sc[instance][slot] = x . y (or its square root) for the instances whose flag `which` is set
+static int gm_dot(tg_ctx *c, const GmresBatch &gb, const double *x, const double *y, int which, int slot,
+                  int take_sqrt)
+{
+    k_piece_dot<<<c->npieces, BLOCK, 0, c->stream>>>(c->seg, c->s.C, x, y, c->gm.part);
+    k_inst_dot<<<c->ninst, GM_INST_BLOCK, 0, c->stream>>>(c->seg, c->gm.part, gb, which, slot, take_sqrt);
     CU(cudaGetLastError());
     return TG_OK;
 }
 
-static int gm_read(tg_ctx *c, int idx, double *out)
+static int inst_grid(const tg_ctx *c)
 {
-    CU(cudaMemcpyAsync(out, c->gm.sc + idx, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    return (c->ninst + 127) / 128;
+}
+
+// instances still iterating, as counted by the kernel just enqueued after a reset of the counter
+static int gm_count(tg_ctx *c, int which, int *out)
+{
+    CU(cudaMemcpyAsync(c->gm.hcount + which, c->gm.count + which, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     CU(cudaStreamSynchronize(c->stream));
+    *out = c->gm.hcount[which];
     return TG_OK;
 }
 
@@ -1581,125 +1639,133 @@ static int gm_derivative(tg_ctx *c, double *q, double *Rout)
     return TG_OK;
 }
 
-// one GMRES cycle for the increment (gmres.c:52-149)
-static int gm_solve(tg_ctx *c, double krylov_tol, int dim)
+// one GMRES cycle for the increment of every Newton instance (gmres.c:52-149)
+static int gm_solve(tg_ctx *c, const GmresBatch &gb, double krylov_tol)
 {
     Gmres &g = c->gm;
-    long n = 5L * c->s.C;
-    int gb = (int)((n + BLOCK - 1) / BLOCK);
-    double *sc = g.sc;
-    double norm;
-    TRY(gm_read(c, GS_NORM, &norm));
-    if (norm <= 0) {
-        CU(cudaMemsetAsync(g.delta, 0, n * sizeof(double), c->stream));
-        return TG_OK;
-    }
-    k_gmres_start<<<gb, BLOCK, 0, c->stream>>>(n, dim, g.r, g.V, g.delta, sc, krylov_tol);
+    const int C = c->s.C, cb = grid_of(C), ib = inst_grid(c);
+    const size_t n = 5 * (size_t)C;
+    k_gmres_begin<<<ib, 128, 0, c->stream>>>(gb, krylov_tol);
+    k_gmres_start<<<cb, BLOCK, 0, c->stream>>>(C, g.r, gb, g.V, g.delta);
     CU(cudaGetLastError());
-    int m = 0;
-    for (; m < dim; m++) {
-        double *Vm = g.V + (long)m * n;
+    for (int m = 0; m < gb.dim; m++) {
+        double *Vm = g.V + (size_t)m * n;
         // matvec (gmres.c:12-50)
-        TRY(gm_dot(c, Vm, Vm, sc + GS_VNORM, 1));
-        k_perturb<<<grid_of(c->s.C), BLOCK, 0, c->stream>>>(c->s.C, c->s.N, g.U, Vm, sc, c->prop[0], g.q1);
+        TRY(gm_dot(c, gb, Vm, Vm, GF_ARNOLDI, GS_VNORM, 1));
+        k_perturb<<<cb, BLOCK, 0, c->stream>>>(C, c->s.N, g.U, Vm, gb, c->prop[0], g.q1);
         CU(cudaGetLastError());
         TRY(gm_derivative(c, g.q1, g.R1));
-        k_matvec_finish<<<gb, BLOCK, 0, c->stream>>>(n, Vm, g.R1, c->R, sc, g.w);
+        k_matvec_finish<<<cb, BLOCK, 0, c->stream>>>(C, Vm, g.R1, c->R, gb, g.w);
         // modified Gram-Schmidt
         for (int i = 0; i <= m; i++) {
-            TRY(gm_dot(c, g.V + (long)i * n, g.w, sc + GS_DOT, 0));
-            k_store_h<<<1, 1, 0, c->stream>>>(sc, dim, i, m);
-            k_mgs_axpy<<<gb, BLOCK, 0, c->stream>>>(n, g.V + (long)i * n, sc, dim, i, m, g.w);
+            TRY(gm_dot(c, gb, g.V + (size_t)i * n, g.w, GF_ARNOLDI, GS_HEAD + i * gb.dim + m, 0));
+            k_mgs_axpy<<<cb, BLOCK, 0, c->stream>>>(C, g.V + (size_t)i * n, gb, i, m, g.w);
         }
-        TRY(gm_dot(c, g.w, g.w, sc + GS_DOT, 1));
-        k_store_h<<<1, 1, 0, c->stream>>>(sc, dim, m + 1, m);
-        k_givens<<<1, 1, 0, c->stream>>>(sc, dim, m);
+        TRY(gm_dot(c, gb, g.w, g.w, GF_ARNOLDI, GS_HEAD + (m + 1) * gb.dim + m, 1));
+        CU(cudaMemsetAsync(g.count + 1, 0, sizeof(int), c->stream));
+        k_givens<<<ib, 128, 0, c->stream>>>(gb, m);
         CU(cudaGetLastError());
-        double done;
-        TRY(gm_read(c, GS_DONE, &done));
-        if (done != 0.0) {
-            m += 1;
-            break;
-        }
-        k_normalize<<<gb, BLOCK, 0, c->stream>>>(n, g.w, sc, dim, m, g.V + (long)(m + 1) * n);
+        int going;
+        TRY(gm_count(c, 1, &going));
+        if (going == 0) break;
+        k_normalize<<<cb, BLOCK, 0, c->stream>>>(C, g.w, gb, m, g.V + (size_t)(m + 1) * n);
     }
-    k_backsolve<<<1, 1, 0, c->stream>>>(sc, dim, m);
-    k_accumulate<<<gb, BLOCK, 0, c->stream>>>(n, g.V, sc, dim, m, g.delta);
+    k_backsolve<<<ib, 128, 0, c->stream>>>(gb);
+    k_accumulate<<<cb, BLOCK, 0, c->stream>>>(C, g.V, gb, g.delta);
     CU(cudaGetLastError());
     return TG_OK;
 }
 
-static int implicit_euler_step(tg_ctx *c, const void *context, double courant, double *time,
-                               double max_step, double *residual, double *step0)
+static int newton_params(const void *context, double *newton_tol, double *krylov_tol, int *dim)
 {
-    double newton_tol = 0.1, krylov_tol = 0.3;  // teal's defaults (src/simulation/set.c:113-115)
-    int dim = 32;
+    *newton_tol = 0.1, *krylov_tol = 0.3, *dim = 32;  // teal's defaults (src/simulation/set.c:113-115)
     if (context) {
         const tg_newton_krylov *nk = (const tg_newton_krylov *)context;
-        newton_tol = nk->newton_tolerance;
-        krylov_tol = nk->krylov_tolerance;
-        dim = nk->krylov_dimension;
+        *newton_tol = nk->newton_tolerance;
+        *krylov_tol = nk->krylov_tolerance;
+        *dim = nk->krylov_dimension;
     }
-    if (!(newton_tol > 0)) return fail(TG_ERR_INVALID, "invalid newton tolerance (%g)", newton_tol);
-    if (!(krylov_tol > 0)) return fail(TG_ERR_INVALID, "invalid krylov tolerance (%g)", krylov_tol);
-    if (dim <= 0) return fail(TG_ERR_INVALID, "invalid krylov dimension (%d)", dim);
+    if (!(*newton_tol > 0)) return fail(TG_ERR_INVALID, "invalid newton tolerance (%g)", *newton_tol);
+    if (!(*krylov_tol > 0)) return fail(TG_ERR_INVALID, "invalid krylov tolerance (%g)", *krylov_tol);
+    if (*dim <= 0) return fail(TG_ERR_INVALID, "invalid krylov dimension (%d)", *dim);
+    return TG_OK;
+}
+
+// One implicit Euler step of every active instance (advance.c:119-195): CFL step, Newton iterations
+// with a GMRES solve each, then the residual norm and the run loop's time / iteration / stop
+// bookkeeping (k_inst_end). The device step arrays must be current.
+static int implicit_step_all(tg_ctx *c, const void *context, double courant)
+{
+    double newton_tol, krylov_tol;
+    int dim;
+    TRY(newton_params(context, &newton_tol, &krylov_tol, &dim));
     TRY(gm_alloc(c, dim));
     Gmres &g = c->gm;
-    long n = 5L * c->s.C;
-    int gb = (int)((n + BLOCK - 1) / BLOCK);
-    double *sc = g.sc;
+    const GmresBatch gb = gm_batch(c, dim);
+    const int C = c->s.C, cb = grid_of(C), ib = inst_grid(c);
+    const size_t n = 5 * (size_t)C;
+    // finite-difference perturbation relative to the state: teal's 1e-6 (advance.c:157) in FP64;
+    // the FP32-flux form's residual carries ~1e-7 relative rounding, so it perturbs by 3e-4
+    const double fd_rel = (c->precision == TG_PRECISION_FP64) ? 1e-6 : 3e-4;
 
     // step from the CFL condition; U = cons(q) (advance.c:136-143)
     TRY(run_prepare(c));
-    hd_at(c, SD_TIME, 0) = *time;
-    hd_at(c, SD_MAX_STEP, 0) = max_step;
-    hi_at(c, SI_ACTIVE, 0) = 1;
-    hi_error(c) = 0;
-    c->st.use_max_time = 0;
-    TRY(write_steps(c));
-    k_inst_begin<<<1, INST_BLOCK, 0, c->stream>>>(c->seg, c->part_min, courant, c->st);
+    {
+        Launch l(c, TG_PROF_REDUCE);
+        k_inst_begin<<<c->ninst, INST_BLOCK, 0, c->stream>>>(c->seg, c->part_min, courant, c->st);
+    }
+    k_newton_begin<<<ib, 128, 0, c->stream>>>(gb, c->st);
     CU(cudaGetLastError());
-    TRY(read_steps(c));
-    TRY(check_error(c));
-    double step = hd_at(c, SD_STEP, 0);
     CU(cudaMemcpyAsync(g.U, c->U0, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     CU(cudaMemcpyAsync(g.Ustart, c->U0, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-    CU(cudaMemcpyAsync(sc + GS_STEP, c->st.step, sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     c->prepared = false;
 
-    double t = *time + step;
     TRY(gm_derivative(c, c->q, c->R));
-    k_newton_init<<<gb, BLOCK, 0, c->stream>>>(n, c->R, sc, g.r);
-    TRY(gm_dot(c, g.r, g.r, sc + GS_NORM, 1));
-    TRY(gm_dot(c, g.U, g.U, sc + GS_CONS_NORM, 1));
-    k_fd_scale<<<1, 1, 0, c->stream>>>(sc);
+    k_newton_init<<<cb, BLOCK, 0, c->stream>>>(C, c->R, gb, g.r);
     CU(cudaGetLastError());
-    double norm;
-    TRY(gm_read(c, GS_NORM, &norm));
-    if (!std::isfinite(norm)) return fail(TG_ERR_NONFINITE, "non-finite Newton residual");
-    double tol_norm = newton_tol * norm;
-    long max_iter = 128L * (c->s.C + 1);
-    for (long it = 0; it < max_iter && norm > tol_norm; it++) {
-        TRY(gm_solve(c, krylov_tol, dim));
-        k_newton_update<<<grid_of(c->s.C), BLOCK, 0, c->stream>>>(c->s.C, c->s.N, g.U, g.delta, c->prop[0], c->q);
-        TRY(gm_derivative(c, c->q, c->R));
-        k_newton_residual<<<gb, BLOCK, 0, c->stream>>>(n, g.U, g.Ustart, c->R, sc, g.r);
-        TRY(gm_dot(c, g.r, g.r, sc + GS_NORM, 1));
-        TRY(gm_dot(c, g.U, g.U, sc + GS_CONS_NORM, 1));
-        k_fd_scale<<<1, 1, 0, c->stream>>>(sc);
+    TRY(gm_dot(c, gb, g.r, g.r, GF_NEWTON, GS_NORM, 1));
+    TRY(gm_dot(c, gb, g.U, g.U, GF_NEWTON, GS_CONS_NORM, 1));
+    k_fd_scale<<<ib, 128, 0, c->stream>>>(gb, fd_rel, newton_tol, 1);
+    CU(cudaGetLastError());
+    for (;;) {
+        CU(cudaMemsetAsync(g.count, 0, sizeof(int), c->stream));
+        k_newton_check<<<ib, 128, 0, c->stream>>>(gb, c->seg, c->st.error);
         CU(cudaGetLastError());
-        TRY(gm_read(c, GS_NORM, &norm));
-        if (!std::isfinite(norm)) return fail(TG_ERR_NONFINITE, "non-finite Newton residual");
+        int going;
+        TRY(gm_count(c, 0, &going));
+        if (going == 0) break;
+        TRY(gm_solve(c, gb, krylov_tol));
+        k_newton_update<<<cb, BLOCK, 0, c->stream>>>(C, c->s.N, g.U, g.delta, gb, c->prop[0], c->q);
+        CU(cudaGetLastError());
+        TRY(gm_derivative(c, c->q, c->R));
+        k_newton_residual<<<cb, BLOCK, 0, c->stream>>>(C, g.U, g.Ustart, c->R, gb, g.r);
+        CU(cudaGetLastError());
+        TRY(gm_dot(c, gb, g.r, g.r, GF_NEWTON, GS_NORM, 1));
+        TRY(gm_dot(c, gb, g.U, g.U, GF_NEWTON, GS_CONS_NORM, 1));
+        k_fd_scale<<<ib, 128, 0, c->stream>>>(gb, fd_rel, newton_tol, 0);
+        CU(cudaGetLastError());
     }
-    // residual of the last derivative (advance.c:188)
+    // residual of the last derivative (advance.c:188), time, iteration and the run loop's tests
     TRY(run_pieces(c, 1));
-    k_inst_end<<<1, INST_BLOCK, 0, c->stream>>>(c->seg, c->part_sum, 0, c->st);
+    {
+        Launch l(c, TG_PROF_REDUCE);
+        k_inst_end<<<c->ninst, INST_BLOCK, 0, c->stream>>>(c->seg, c->part_sum, 1, c->st);
+        k_count_active<<<1, 256, 0, c->stream>>>(c->ninst, c->st);
+    }
     CU(cudaGetLastError());
-    TRY(read_steps(c));
-    TRY(check_error(c));
-    *time = t;
-    if (residual) residual_of(c, 0, residual);
-    if (step0) *step0 = hd_at(c, SD_STEP0, 0);
+    return TG_OK;
+}
+
+// implicit steps of every instance until each one stops (iterations, residual threshold, end time)
+static int implicit_run(tg_ctx *c, const void *context, double courant, int most)
+{
+    TRY(write_steps(c));
+    for (int it = 0; it < most; it++) {
+        TRY(implicit_step_all(c, context, courant));
+        TRY(read_steps(c));
+        TRY(check_error(c));
+        if (hi_num_active(c) == 0) break;
+    }
     return TG_OK;
 }
 

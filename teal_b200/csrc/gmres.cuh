@@ -1,118 +1,255 @@
 // Kernels of the implicit Euler step with a Jacobian-free Newton-GMRES solve
-// (src/simulation/advance.c:119-195, src/simulation/gmres.c:12-149). Vectors are the conserved
-// state of the inner cells, [5][C] flattened to n = 5C; dot products and norms are deterministic
-// block-partial reductions; Arnoldi, Givens rotations and back substitution run on the device.
+// (src/simulation/advance.c:119-195, src/simulation/gmres.c:12-149), for every instance of an
+// arena at once. Vectors are the conserved state of the inner cells, [5][C] over the arena; each
+// instance has its own scalars (norms, step, finite-difference scale, Hessenberg matrix, Givens
+// rotations, right-hand side, coefficients) and its own Newton / Arnoldi progress, so instances
+// converge independently: a finished instance is masked out of the vector updates. Dot products
+// and norms are per-piece partial sums, then per-instance sums in piece order: deterministic, and
+// the same bits for an instance alone or in a batch.
 #pragma once
 
 #include "kernels.cuh"
 
 namespace tg {
 
-// scalar slots of the device scalar array
+// scalar slots of an instance's block in the device scalar array
 enum GmresScalar {
-    GS_NORM = 0,      // Newton residual norm
-    GS_CONS_NORM = 1, // norm of the conserved state
-    GS_FD_SCALE = 2,  // finite-difference scale
-    GS_VNORM = 3,     // norm of the Krylov vector being multiplied
-    GS_STEP = 4,      // time step
-    GS_KTOL = 5,      // Krylov tolerance * norm
-    GS_DONE = 6,      // Arnoldi stopped early
-    GS_DOT = 7,       // last dot product
-    GS_HEAD = 16      // H [(dim+1) x dim], cs [dim], sn [dim], rhs [dim+1], coef [dim]
+    GS_NORM = 0,       // Newton residual norm
+    GS_CONS_NORM = 1,  // norm of the conserved state
+    GS_FD_SCALE = 2,   // finite-difference scale
+    GS_VNORM = 3,      // norm of the Krylov vector being multiplied
+    GS_STEP = 4,       // time step
+    GS_KTOL = 5,       // Krylov tolerance * norm
+    GS_TOL_NORM = 6,   // Newton tolerance * first norm
+    GS_HEAD = 8        // H [(dim+1) x dim], cs [dim], sn [dim], rhs [dim+1], coef [dim]
 };
 
-__device__ __forceinline__ double *gm_H(double *sc, int dim, int i, int k)
+// per-instance flags: Newton iterating, Arnoldi iterating, Krylov vectors used, Newton iterations
+enum GmresFlag { GF_NEWTON = 0, GF_ARNOLDI = 1, GF_M = 2, GF_ITER = 3, GF_COUNT = 4 };
+
+struct GmresBatch {
+    int dim;    // Krylov dimension
+    int scn;    // doubles per instance block of `sc`
+    int ninst;
+    const int *__restrict__ cell_inst;
+    double *sc;  // [ninst][scn]
+    int *flag;   // [GF_COUNT][ninst]
+    int *count;  // [2] instances still iterating (Newton, Arnoldi)
+
+    __device__ __forceinline__ double *s(int i) const { return sc + (size_t)i * scn; }
+    __device__ __forceinline__ double *H(int i, int r, int k) const { return s(i) + GS_HEAD + r * dim + k; }
+    __device__ __forceinline__ double *cs(int i) const { return s(i) + GS_HEAD + (dim + 1) * dim; }
+    __device__ __forceinline__ double *sn(int i) const { return cs(i) + dim; }
+    __device__ __forceinline__ double *rhs(int i) const { return sn(i) + dim; }
+    __device__ __forceinline__ double *coef(int i) const { return rhs(i) + dim + 1; }
+    __device__ __forceinline__ int &newton(int i) const { return flag[GF_NEWTON * ninst + i]; }
+    __device__ __forceinline__ int &arnoldi(int i) const { return flag[GF_ARNOLDI * ninst + i]; }
+    __device__ __forceinline__ int &m(int i) const { return flag[GF_M * ninst + i]; }
+    __device__ __forceinline__ int &iter(int i) const { return flag[GF_ITER * ninst + i]; }
+};
+
+__host__ __device__ inline int gmres_scn(int dim)
 {
-    return sc + GS_HEAD + i * dim + k;
+    return GS_HEAD + (dim + 1) * dim + 4 * dim + 2;
 }
 
-// partial sums of x . y over n elements
-__global__ void __launch_bounds__(BLOCK) k_dot_part(long n, const double *__restrict__ x,
-                                                    const double *__restrict__ y, double *__restrict__ part)
+// per-piece partial sums of x . y over the 5 variables of the piece's cells
+__global__ void __launch_bounds__(BLOCK) k_piece_dot(Segments seg, int C, const double *__restrict__ x,
+                                                     const double *__restrict__ y, double *__restrict__ part)
 {
     __shared__ double sh[BLOCK / 32];
+    const int beg = seg.piece_beg[blockIdx.x], end = seg.piece_beg[blockIdx.x + 1];
     double t = 0;
-    for (long i = blockIdx.x * (long)BLOCK + threadIdx.x; i < n; i += (long)gridDim.x * BLOCK) {
-        t += x[i] * y[i];
+    for (int c = beg + threadIdx.x; c < end; c += BLOCK) {
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+            t += x[(size_t)v * C + c] * y[(size_t)v * C + c];
+        }
     }
-    double s = block_sum<BLOCK>(t, sh);
+    double sum = block_sum<BLOCK>(t, sh);
     if (threadIdx.x == 0) {
-        part[blockIdx.x] = s;
+        part[blockIdx.x] = sum;
     }
 }
 
-// dst = sum of partials (optionally its square root)
-__global__ void __launch_bounds__(REDUCE_BLOCK) k_reduce_scalar(const double *__restrict__ part, int nparts,
-                                                                double *dst, int take_sqrt)
+constexpr int GM_INST_BLOCK = 128;
+
+// sc[inst][slot] = sum of the instance's piece partials (or its square root), for instances whose
+// flag `which` is set
+__global__ void __launch_bounds__(GM_INST_BLOCK) k_inst_dot(Segments seg, const double *__restrict__ part,
+                                                           GmresBatch gb, int which, int slot, int take_sqrt)
 {
-    __shared__ double sh[REDUCE_BLOCK / 32];
-    double t = 0;
-    for (int i = threadIdx.x; i < nparts; i += REDUCE_BLOCK) {
-        t += part[i];
+    __shared__ double sh[GM_INST_BLOCK / 32];
+    const int i = blockIdx.x;
+    if (!gb.flag[which * gb.ninst + i]) {
+        return;
     }
-    double s = block_sum<REDUCE_BLOCK>(t, sh);
+    double t = 0;
+    for (int p = seg.inst_piece_off[i] + threadIdx.x; p < seg.inst_piece_off[i + 1]; p += GM_INST_BLOCK) {
+        t += part[p];
+    }
+    double sum = block_sum<GM_INST_BLOCK>(t, sh);
     if (threadIdx.x == 0) {
-        *dst = take_sqrt ? sqrt(s) : s;
+        gb.s(i)[slot] = take_sqrt ? sqrt(sum) : sum;
+    }
+}
+
+// start of a step for every instance: Newton flag on for the active ones, step copied
+__global__ void k_newton_begin(GmresBatch gb, Steps st)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= gb.ninst) {
+        return;
+    }
+    const int on = st.active[i] != 0;
+    gb.newton(i) = on;
+    gb.arnoldi(i) = 0;
+    gb.m(i) = 0;
+    gb.iter(i) = 0;
+    if (on) {
+        gb.s(i)[GS_STEP] = st.step[i];
     }
 }
 
 // r = -R * step (advance.c:148-153)
-__global__ void k_newton_init(long n, const double *__restrict__ R, const double *__restrict__ sc,
-                              double *__restrict__ r)
-{
-    long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (i < n) {
-        r[i] = -R[i] * sc[GS_STEP];
-    }
-}
-
-// r = U - U0 - R * step (advance.c:176-181)
-__global__ void k_newton_residual(long n, const double *__restrict__ U, const double *__restrict__ U0,
-                                  const double *__restrict__ R, const double *__restrict__ sc,
-                                  double *__restrict__ r)
-{
-    long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (i < n) {
-        r[i] = (U[i] - U0[i]) - (R[i] * sc[GS_STEP]);
-    }
-}
-
-// fd_scale = 1e-6 * max(1, |U|) / max(1, |r|) (advance.c:155-159)
-__global__ void k_fd_scale(double *sc)
-{
-    sc[GS_FD_SCALE] = 1e-6 * fmax(1.0, sc[GS_CONS_NORM]) / fmax(1.0, sc[GS_NORM]);
-}
-
-// start of a GMRES cycle (gmres.c:68-83): V0 = -r / norm, rhs = (norm, 0, ...), delta = 0
-__global__ void k_gmres_start(long n, int dim, const double *__restrict__ r, double *__restrict__ V0,
-                              double *__restrict__ delta, double *sc, double krylov_tol)
-{
-    long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    double norm = sc[GS_NORM];
-    if (i < n) {
-        V0[i] = -r[i] / norm;
-        delta[i] = 0.0;
-    }
-    if (i == 0) {
-        double *rhs = sc + GS_HEAD + (dim + 1) * dim + 2 * dim;
-        for (int k = 0; k <= dim; k++) {
-            rhs[k] = 0.0;
-        }
-        rhs[0] = norm;
-        sc[GS_KTOL] = krylov_tol * norm;
-        sc[GS_DONE] = 0.0;
-    }
-}
-
-// perturbed primitive state q1 = prim(U + eps * v), eps = fd_scale / |v| (gmres.c:26-36)
-__global__ void k_perturb(int C, int N, const double *__restrict__ U, const double *__restrict__ v,
-                          const double *__restrict__ sc, double gamma, double *__restrict__ q1)
+__global__ void k_newton_init(int C, const double *__restrict__ R, GmresBatch gb, double *__restrict__ r)
 {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= C) {
         return;
     }
-    double eps = sc[GS_FD_SCALE] / sc[GS_VNORM];
+    const int i = gb.cell_inst[c];
+    if (!gb.newton(i)) {
+        return;
+    }
+    const double step = gb.s(i)[GS_STEP];
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        r[(size_t)v * C + c] = -R[(size_t)v * C + c] * step;
+    }
+}
+
+// r = U - U0 - R * step (advance.c:176-181)
+__global__ void k_newton_residual(int C, const double *__restrict__ U, const double *__restrict__ U0,
+                                  const double *__restrict__ R, GmresBatch gb, double *__restrict__ r)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= C) {
+        return;
+    }
+    const int i = gb.cell_inst[c];
+    if (!gb.newton(i)) {
+        return;
+    }
+    const double step = gb.s(i)[GS_STEP];
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        size_t k = (size_t)v * C + c;
+        r[k] = (U[k] - U0[k]) - (R[k] * step);
+    }
+}
+
+// fd_scale = fd_rel * max(1, |U|) / max(1, |r|) (advance.c:155-159, fd_rel = 1e-6 there); on the
+// first call of a step also the Newton target tol * |r|
+__global__ void k_fd_scale(GmresBatch gb, double fd_rel, double newton_tol, int first)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= gb.ninst || !gb.newton(i)) {
+        return;
+    }
+    double *s = gb.s(i);
+    s[GS_FD_SCALE] = fd_rel * fmax(1.0, s[GS_CONS_NORM]) / fmax(1.0, s[GS_NORM]);
+    if (first) {
+        s[GS_TOL_NORM] = newton_tol * s[GS_NORM];
+    }
+}
+
+// Newton loop test per instance (advance.c:162-165): keep iterating while |r| > tol * |r0| and
+// within 128 (cells + 1) iterations; a non-finite norm sets the error word. count[0] = instances
+// that go on.
+__global__ void k_newton_check(GmresBatch gb, Segments seg, int *err)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= gb.ninst || !gb.newton(i)) {
+        return;
+    }
+    const double norm = gb.s(i)[GS_NORM];
+    if (!isfinite(norm)) {
+        atomicOr(err, ERR_NONFINITE);
+        gb.newton(i) = 0;
+        return;
+    }
+    const long max_iter = 128L * (seg.inst_cell_off[i + 1] - seg.inst_cell_off[i] + 1);
+    const long it = gb.iter(i);
+    if (!(norm > gb.s(i)[GS_TOL_NORM]) || it >= max_iter) {
+        gb.newton(i) = 0;
+        return;
+    }
+    atomicAdd(&gb.count[0], 1);
+}
+
+// start of a GMRES cycle (gmres.c:68-83) per Newton instance: rhs = (norm, 0, ...), Arnoldi on
+// unless the residual is already zero
+__global__ void k_gmres_begin(GmresBatch gb, double krylov_tol)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= gb.ninst) {
+        return;
+    }
+    gb.arnoldi(i) = 0;
+    gb.m(i) = 0;
+    if (!gb.newton(i)) {
+        return;
+    }
+    double *s = gb.s(i);
+    const double norm = s[GS_NORM];
+    double *rhs = gb.rhs(i);
+    for (int k = 0; k <= gb.dim; k++) {
+        rhs[k] = 0.0;
+    }
+    rhs[0] = norm;
+    s[GS_KTOL] = krylov_tol * norm;
+    gb.arnoldi(i) = norm > 0;
+    gb.iter(i) += 1;
+}
+
+// V0 = -r / norm and delta = 0 for every Newton instance (delta stays 0 when the norm is 0)
+__global__ void k_gmres_start(int C, const double *__restrict__ r, GmresBatch gb, double *__restrict__ V0,
+                              double *__restrict__ delta)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= C) {
+        return;
+    }
+    const int i = gb.cell_inst[c];
+    if (!gb.newton(i)) {
+        return;
+    }
+    const double norm = gb.s(i)[GS_NORM];
+    const bool on = gb.arnoldi(i) != 0;
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        size_t k = (size_t)v * C + c;
+        if (on) {
+            V0[k] = -r[k] / norm;
+        }
+        delta[k] = 0.0;
+    }
+}
+
+// perturbed primitive state q1 = prim(U + eps * v), eps = fd_scale / |v| (gmres.c:26-36)
+__global__ void k_perturb(int C, int N, const double *__restrict__ U, const double *__restrict__ v,
+                          GmresBatch gb, double gamma, double *__restrict__ q1)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= C) {
+        return;
+    }
+    const int i = gb.cell_inst[c];
+    if (!gb.arnoldi(i)) {
+        return;
+    }
+    const double eps = gb.s(i)[GS_FD_SCALE] / gb.s(i)[GS_VNORM];
     Cons<double> u;
     u.rho = U[c] + (eps * v[c]);
     u.m.x = U[C + c] + (eps * v[C + c]);
@@ -128,102 +265,149 @@ __global__ void k_perturb(int C, int N, const double *__restrict__ U, const doub
 }
 
 // w = v - step * (R1 - R) / eps (gmres.c:41-46)
-__global__ void k_matvec_finish(long n, const double *__restrict__ v, const double *__restrict__ R1,
-                                const double *__restrict__ R, const double *__restrict__ sc,
-                                double *__restrict__ w)
+__global__ void k_matvec_finish(int C, const double *__restrict__ v, const double *__restrict__ R1,
+                                const double *__restrict__ R, GmresBatch gb, double *__restrict__ w)
 {
-    long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (i < n) {
-        double eps = sc[GS_FD_SCALE] / sc[GS_VNORM];
-        w[i] = v[i] - ((sc[GS_STEP] * (R1[i] - R[i])) / eps);
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= C) {
+        return;
+    }
+    const int i = gb.cell_inst[c];
+    if (!gb.arnoldi(i)) {
+        return;
+    }
+    const double *s = gb.s(i);
+    const double eps = s[GS_FD_SCALE] / s[GS_VNORM];
+    const double step = s[GS_STEP];
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        size_t j = (size_t)k * C + c;
+        w[j] = v[j] - ((step * (R1[j] - R[j])) / eps);
     }
 }
 
-// store a dot product into H[i][k]
-__global__ void k_store_h(double *sc, int dim, int i, int k)
+// modified Gram-Schmidt update w -= H[r][k] * V_r (gmres.c:92-99)
+__global__ void k_mgs_axpy(int C, const double *__restrict__ Vr, GmresBatch gb, int r, int k,
+                           double *__restrict__ w)
 {
-    *gm_H(sc, dim, i, k) = sc[GS_DOT];
-}
-
-// modified Gram-Schmidt update w -= H[i][k] * V_i (gmres.c:92-99)
-__global__ void k_mgs_axpy(long n, const double *__restrict__ Vi, const double *__restrict__ sc, int dim,
-                           int i, int k, double *__restrict__ w)
-{
-    long j = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (j < n) {
-        double h = sc[GS_HEAD + i * dim + k];
-        w[j] -= h * Vi[j];
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= C) {
+        return;
+    }
+    const int i = gb.cell_inst[c];
+    if (!gb.arnoldi(i)) {
+        return;
+    }
+    const double h = *gb.H(i, r, k);
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        size_t j = (size_t)v * C + c;
+        w[j] -= h * Vr[j];
     }
 }
 
-// Givens rotations of column k, new rotation, right-hand side, convergence test (gmres.c:102-119)
-__global__ void k_givens(double *sc, int dim, int k)
+// Givens rotations of column k, new rotation, right-hand side and convergence test per Arnoldi
+// instance (gmres.c:102-119); an instance that converged (or filled the basis) stops with m = k + 1.
+// count[1] = instances that go on.
+__global__ void k_givens(GmresBatch gb, int k)
 {
-    double *cs = sc + GS_HEAD + (dim + 1) * dim;
-    double *sn = cs + dim;
-    double *rhs = sn + dim;
-    for (int i = 0; i < k; i++) {
-        double hik = *gm_H(sc, dim, i, k), hi1k = *gm_H(sc, dim, i + 1, k);
-        double tmp = (cs[i] * hik) + (sn[i] * hi1k);
-        *gm_H(sc, dim, i + 1, k) = (-sn[i] * hik) + (cs[i] * hi1k);
-        *gm_H(sc, dim, i, k) = tmp;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= gb.ninst || !gb.arnoldi(i)) {
+        return;
     }
-    double hkk = *gm_H(sc, dim, k, k), hk1k = *gm_H(sc, dim, k + 1, k);
+    double *cs = gb.cs(i), *sn = gb.sn(i), *rhs = gb.rhs(i);
+    for (int r = 0; r < k; r++) {
+        double hrk = *gb.H(i, r, k), hr1k = *gb.H(i, r + 1, k);
+        double tmp = (cs[r] * hrk) + (sn[r] * hr1k);
+        *gb.H(i, r + 1, k) = (-sn[r] * hrk) + (cs[r] * hr1k);
+        *gb.H(i, r, k) = tmp;
+    }
+    double hkk = *gb.H(i, k, k), hk1k = *gb.H(i, k + 1, k);
     double rot = sqrt((hkk * hkk) + (hk1k * hk1k));
     cs[k] = hkk / rot;
     sn[k] = hk1k / rot;
-    *gm_H(sc, dim, k, k) = rot;
+    *gb.H(i, k, k) = rot;
     rhs[k + 1] = -sn[k] * rhs[k];
     rhs[k] = cs[k] * rhs[k];
-    sc[GS_DONE] = (fabs(rhs[k + 1]) < sc[GS_KTOL]) ? 1.0 : 0.0;
+    gb.m(i) = k + 1;
+    if (fabs(rhs[k + 1]) < gb.s(i)[GS_KTOL] || k + 1 >= gb.dim) {
+        gb.arnoldi(i) = 0;
+        return;
+    }
+    atomicAdd(&gb.count[1], 1);
 }
 
 // V_{k+1} = w / H[k+1][k] (gmres.c:121-125)
-__global__ void k_normalize(long n, const double *__restrict__ w, const double *__restrict__ sc, int dim,
-                            int k, double *__restrict__ Vk1)
+__global__ void k_normalize(int C, const double *__restrict__ w, GmresBatch gb, int k, double *__restrict__ Vk1)
 {
-    long j = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (j < n) {
-        Vk1[j] = w[j] / sc[GS_HEAD + (k + 1) * dim + k];
-    }
-}
-
-// back substitution coefficients for m Krylov vectors (gmres.c:128-136)
-__global__ void k_backsolve(double *sc, int dim, int m)
-{
-    double *rhs = sc + GS_HEAD + (dim + 1) * dim + 2 * dim;
-    double *coef = rhs + dim + 1;
-    for (int i = m - 1; i >= 0; i--) {
-        double ci = rhs[i];
-        for (int j = i + 1; j < m; j++) {
-            ci -= *gm_H(sc, dim, i, j) * coef[j];
-        }
-        coef[i] = ci / *gm_H(sc, dim, i, i);
-    }
-}
-
-// delta += coef[i] * V_i, i from m-1 down to 0 in one pass (gmres.c:137-141)
-__global__ void k_accumulate(long n, const double *__restrict__ V, const double *__restrict__ sc, int dim,
-                             int m, double *__restrict__ delta)
-{
-    long j = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (j >= n) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= C) {
         return;
     }
-    const double *coef = sc + GS_HEAD + (dim + 1) * dim + 2 * dim + dim + 1;
-    double d = delta[j];
-    for (int i = m - 1; i >= 0; i--) {
-        d += coef[i] * V[(long)i * n + j];
+    const int i = gb.cell_inst[c];
+    if (!gb.arnoldi(i)) {
+        return;
     }
-    delta[j] = d;
+    const double h = *gb.H(i, k + 1, k);
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        size_t j = (size_t)v * C + c;
+        Vk1[j] = w[j] / h;
+    }
+}
+
+// back substitution coefficients for the instance's m Krylov vectors (gmres.c:128-136)
+__global__ void k_backsolve(GmresBatch gb)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= gb.ninst || !gb.newton(i)) {
+        return;
+    }
+    const int m = gb.m(i);
+    double *rhs = gb.rhs(i), *coef = gb.coef(i);
+    for (int r = m - 1; r >= 0; r--) {
+        double cr = rhs[r];
+        for (int j = r + 1; j < m; j++) {
+            cr -= *gb.H(i, r, j) * coef[j];
+        }
+        coef[r] = cr / *gb.H(i, r, r);
+    }
+}
+
+// delta += coef[r] * V_r, r from m-1 down to 0 in one pass (gmres.c:137-141)
+__global__ void k_accumulate(int C, const double *__restrict__ V, GmresBatch gb, double *__restrict__ delta)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= C) {
+        return;
+    }
+    const int i = gb.cell_inst[c];
+    if (!gb.newton(i)) {
+        return;
+    }
+    const int m = gb.m(i);
+    const double *coef = gb.coef(i);
+    const size_t n = 5 * (size_t)C;
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        size_t j = (size_t)v * C + c;
+        double d = delta[j];
+        for (int r = m - 1; r >= 0; r--) {
+            d += coef[r] * V[(size_t)r * n + j];
+        }
+        delta[j] = d;
+    }
 }
 
 // U += delta, q = prim(U) (advance.c:168-173)
 __global__ void k_newton_update(int C, int N, double *__restrict__ U, const double *__restrict__ delta,
-                                double gamma, double *__restrict__ q)
+                                GmresBatch gb, double gamma, double *__restrict__ q)
 {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= C) {
+        return;
+    }
+    if (!gb.newton(gb.cell_inst[c])) {
         return;
     }
     Cons<double> u;

@@ -46,7 +46,7 @@ __global__ void k_boundary(Sizes s, const int2 *__restrict__ lr, const double *_
 constexpr int GRAD_CELLS = 32;
 constexpr int GRAD_THREADS = 5 * GRAD_CELLS;
 
-template <typename R, int LIM, bool FOLD>
+template <typename R, int LIM, bool FOLD, bool SKIP>
 __global__ void __launch_bounds__(GRAD_THREADS) k_gradient(Sizes s, Geometry<R> g,
                                                            const double *__restrict__ eps2,
                                                            const double *__restrict__ q,
@@ -59,18 +59,24 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_gradient(Sizes s, Geometry<R> 
     const int C = s.C;
     const int base = blockIdx.x * GRAD_CELLS;
     const int ncell = min(GRAD_CELLS, C - base);
+    // SKIP (meshes with cells of fewer than MAX_SLOTS faces): padding slots are not loaded, each
+    // staging thread reading its cell's face count; nothing reads them
     for (int i = threadIdx.x; i < MAX_SLOTS * GRAD_CELLS; i += GRAD_THREADS) {
         int j = i / GRAD_CELLS, l = i % GRAD_CELLS;
-        s_nbr[j][l] = (l < ncell) ? __ldg(g.slot_nbr + (size_t)j * C + base + l) : 0;
+        if (l < ncell && (!SKIP || j < int(__ldg(g.slot_cnt + base + l)))) {
+            s_nbr[j][l] = __ldg(g.slot_nbr + (size_t)j * C + base + l);
+        }
     }
     if (threadIdx.x < GRAD_CELLS) {
         s_cnt[threadIdx.x] = (threadIdx.x < ncell) ? int(g.slot_cnt[base + threadIdx.x]) : 0;
     }
     for (int i = threadIdx.x; i < 3 * MAX_SLOTS * GRAD_CELLS; i += GRAD_THREADS) {
         int k = i / GRAD_CELLS, l = i % GRAD_CELLS;
-        s_w[k][l] = (l < ncell) ? __ldg(g.slot_w + (size_t)k * C + base + l) : R(0);
-        if (LIM != 0) {
-            s_off[k][l] = (l < ncell) ? __ldg(g.slot_off + (size_t)k * C + base + l) : R(0);
+        if (l < ncell && (!SKIP || (k % MAX_SLOTS) < int(__ldg(g.slot_cnt + base + l)))) {
+            s_w[k][l] = __ldg(g.slot_w + (size_t)k * C + base + l);
+            if (LIM != 0) {
+                s_off[k][l] = __ldg(g.slot_off + (size_t)k * C + base + l);
+            }
         }
     }
     __syncthreads();

@@ -103,3 +103,76 @@ def test_batch_rejects_mixed_lanes():
     c.set_convective_flux("roe")
     with pytest.raises(tb.TealError, match="differs"):
         tb.Batch([a, c])
+
+
+# ---- batched implicit Euler (Jacobian-free Newton-GMRES per instance) ---------------------------
+
+IMPLICIT_SPECS = [(10, 8, 0.5, 1), (14, 6, 1.5, 2), (7, 9, 0.8, 3)]  # nx, ny, Mach, seed
+NK = (0.1, 0.3, 10)
+
+
+def farfield_free(mach):
+    return np.array([1.0, mach * 1.183216, 0.1 * mach, 0.0, 1.0 / 1.4])
+
+
+def farfield_state(num_cells, mach, seed):
+    rng = np.random.default_rng(seed)
+    prim = np.tile(farfield_free(mach), (num_cells, 1))
+    prim[:, 0] *= 1 + 0.05 * rng.random(num_cells)
+    return prim
+
+
+def farfield_problem(nx, ny, mach, seed):
+    m = tb.Mesh.create((0, 0, 0), (1, 1, 0.2), (nx, ny, 2), (0, 0, 1))
+    e = tb.Equations.euler(m)
+    e.set_limiter(None, 0.0)
+    for side in ("left", "right", "bottom", "top"):
+        e.set_boundary_condition(side, "farfield", farfield_free(mach))
+    e.primitive[:] = farfield_state(m.num_cells, mach, seed)
+    return e
+
+
+def farfield_reference(nx, ny, mach, seed):
+    rm = ref.RefMesh((0, 0, 0), (1, 1, 0.2), (nx, ny, 2), (0, 0, 1))
+    re = ref.RefEquations(rm, False)
+    re.set_limiter(None, 0.0)
+    for side in ("left", "right", "bottom", "top"):
+        re.set_boundary_condition(side, "farfield", farfield_free(mach))
+    re.set_primitive(farfield_state(rm.counts()["num_cells"], mach, seed))
+    return re
+
+
+def test_batch_implicit_instances_are_bit_identical_to_solo_runs():
+    ps = [farfield_problem(*spec) for spec in IMPLICIT_SPECS]
+    steps = [3, 1, 2]
+    b = tb.Batch(ps)
+    t, it, res = b.run(tb.TG_ADVANCE_IMPLICIT_EULER, 20.0, steps, context=NK)
+    assert list(it) == steps
+    for i, e in enumerate(ps):
+        ctx = tb.Context(e.mesh, e)
+        ctx.set_primitive(e.primitive)
+        t1, it1, res1 = ctx.run(tb.TG_ADVANCE_IMPLICIT_EULER, 20.0, steps[i], context=NK)
+        C = e.mesh.num_inner_cells
+        assert it1 == steps[i]
+        assert t[i] == t1
+        assert np.array_equal(res[i], res1)
+        assert np.array_equal(b.get_primitive(i)[:C], ctx.get_primitive()[:C])
+
+
+def test_batch_implicit_matches_reference():
+    """Two implicit steps of each instance against the reference. No limiter; the reference's own
+    two-step result moves by up to 1e-4 under a 1e-16 relative input perturbation (Newton / GMRES
+    stopping decisions of step 2 flip), so the bar is 1e-3, as for the single-mesh test."""
+    specs = IMPLICIT_SPECS[:2]
+    ps = [farfield_problem(*spec) for spec in specs]
+    b = tb.Batch(ps)
+    t, it, res = b.run(tb.TG_ADVANCE_IMPLICIT_EULER, 20.0, 2, context=NK)
+    for i, spec in enumerate(specs):
+        re = farfield_reference(*spec)
+        rs = ref.RefSimulation(re, "implicit euler", 20.0, nk=NK)
+        tr = 0.0
+        for _ in range(2):
+            tr, _, rr = rs.advance(tr)
+        C = ps[i].mesh.num_inner_cells
+        assert rel_l2(b.get_primitive(i)[:C], re.primitive[:C]).max() <= 1e-3
+        assert abs(t[i] - tr) <= 1e-3 * tr
