@@ -376,7 +376,9 @@ def run_batch(args, world, rank):
     cells = sum(e.mesh.num_inner_cells for e in problems)
     implicit = args.method == "implicit"
     method = tb.TG_ADVANCE_IMPLICIT_EULER if implicit else tb.TG_ADVANCE_LSERK
-    courant = 100.0 if implicit else 0.9
+    # implicit: CFL 10; from the uniform start at CFL 100 the reference's own first step already
+    # ends in non-finite residuals on some instances of this draw
+    courant = 10.0 if implicit else 0.9
     context = (0.1, 0.3, 30) if implicit else (3, 3)
     steps = args.steps
     stream = torch.cuda.Stream()
@@ -401,10 +403,19 @@ def run_batch(args, world, rank):
         out[name] = {"value": cells * steps / secs, "seconds": secs}
         states[name] = [b.get_primitive(i)[: e.mesh.num_inner_cells].copy() for i, e in enumerate(problems)]
         b.close()
-    err = 0.0
+    # error of the FP32-flux form against FP64: relative L2 per conserved variable (the max over
+    # instances), and over all five together
+    def conserved(p, gamma=1.4):
+        rho, u, pr = p[:, 0], p[:, 1:4], p[:, 4]
+        return np.column_stack([rho, rho[:, None] * u, pr / (gamma - 1) + 0.5 * rho * (u ** 2).sum(axis=1)])
+
+    err_var = np.zeros(5)
+    err_all = 0.0
     for a, f in zip(states["fp64"], states["fp32_flux"]):
-        d = np.sqrt(((f - a) ** 2).sum(axis=0)) / np.maximum(np.sqrt((a ** 2).sum(axis=0)), 1e-300)
-        err = max(err, float(d.max()))
+        ua, uf = conserved(a), conserved(f)
+        d = np.sqrt(((uf - ua) ** 2).sum(axis=0)) / np.maximum(np.sqrt((ua ** 2).sum(axis=0)), 1e-300)
+        err_var = np.maximum(err_var, d)
+        err_all = max(err_all, float(np.sqrt(((uf - ua) ** 2).sum()) / np.sqrt((ua ** 2).sum())))
 
     # the same meshes one at a time in FP64 (a sample of them, throughput summed)
     sample = problems[: min(len(problems), args.solo_sample)]
@@ -426,13 +437,14 @@ def run_batch(args, world, rank):
         "vs_baseline": None, "dtype": "f32-flux/f64-accumulate", "data": "synthetic",
         "config": {"workload": f"{len(problems)} euler ramp meshes (tets/prisms/hexes/pyramids), 8k-512k cells "
                                f"log-uniform, mach 0.3-3.0, angle 0-10 deg, ausmd + barth-jespersen, "
-                               + ("implicit euler cfl 100, newton-krylov {0.1, 0.3, 30}" if implicit
+                               + ("implicit euler cfl 10, newton-krylov {0.1, 0.3, 30}" if implicit
                                   else "lserk{3,3} cfl 0.9"),
                    "cells": cells, "instances": len(problems)},
         "batched_fp64": out["fp64"]["value"], "batched_fp32_flux": out["fp32_flux"]["value"],
         "solo_fp64": solo, "solo_sample": len(sample),
         "fp32_flux_over_solo_fp64": out["fp32_flux"]["value"] / solo,
-        "fp32_flux_rel_l2_vs_fp64": err, "setup_s": t_setup,
+        "fp32_flux_rel_l2_vs_fp64": err_all, "fp32_flux_rel_l2_per_conserved": err_var.tolist(),
+        "setup_s": t_setup,
     }
     print(json.dumps(line))
 

@@ -164,8 +164,11 @@ __device__ __forceinline__ void flux_rec_load(const R *G, int f, double (&v)[5])
 template <typename R>
 __device__ __forceinline__ bool is_close_zero(R x)
 {
-    return fabs(x) <= fmax(R(1e-8), R(1e-5) * fabs(x));
+    // |x| <= max(1e-8, 1e-5 |x|) holds exactly when |x| <= 1e-8 or x is infinite
+    const R a = fabs(x);
+    return (a <= R(1e-8)) || (a == R(INFINITY));
 }
+
 
 // ---- block reductions (fixed shape => deterministic) -----------------------------------------
 
