@@ -150,6 +150,25 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(x, pg):
+    """The largest of every rank's x (each rank's device time): the whole job ends with its slowest
+    replica. Tensors live on the GPU for NCCL and on the host for gloo."""
+    if pg is None:
+        return float(x)
+    import torch
+
+    dev = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(cells_per_rank, steps, world, seconds):
+    """Cell updates per second of all replicas together (weak scaling: each rank advances its own
+    mesh of cells_per_rank cells for the same steps; the job takes the slowest rank's time)."""
+    return cells_per_rank * steps * world / seconds
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -576,12 +595,8 @@ def main():
         pg.barrier()
     clocks = sampler.stop()
     launches = ctx.launch_count() - launches0
-    ms = ev0.elapsed_time(ev1)
-    if pg:
-        t = torch.tensor([ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
-    value = C * args.steps * world / (ms / 1000.0)
+    ms = max_over_ranks(ev0.elapsed_time(ev1), pg)
+    value = whole_job_rate(C, args.steps, world, ms / 1000.0)
 
     # per-kernel CUDA-event timing of the same steps (plain launches, events on the same stream)
     ksteps = min(args.steps, 5)
@@ -606,12 +621,8 @@ def main():
         tt, _, res = ctx.advance(LSERK, 0.99, tt, context=rk)
         ctx.get_primitive(host_out)
         host_in, host_out = host_out, host_in
-    e2e_s = time.perf_counter() - t0
-    if pg:
-        t = torch.tensor([e2e_s], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = C * e2e_steps * world / e2e_s
+    e2e_s = max_over_ranks(time.perf_counter() - t0, pg)
+    e2e_value = whole_job_rate(C, e2e_steps, world, e2e_s)
 
     # roofline of one RK stage (boundary + gradient + face + cell kernels)
     peak, peak_kind = read_peaks()
