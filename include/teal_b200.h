@@ -76,6 +76,16 @@ enum {
     TG_BC_ADIABATIC_WALL = 8 /* "adiabatic wall", "wall" (Navier–Stokes only) */
 };
 
+/* Source terms run on the device (teal's Equations.source, src/equations.h:27-41, is a host
+ * callback pair; the device runs these kinds in its place, selected by tg_source_select):
+ *   TG_SOURCE_BODY_FORCE    constant acceleration g = source_parameter[0..2]:
+ *                           S = (0, rho g, rho g . u)   (run/rayleigh_taylor_instability/run.c:17-24)
+ *   TG_SOURCE_BULK_FORCING  forcing of the bulk x velocity to U = source_parameter[0] with time
+ *                           scale tau = source_parameter[1]: s = rho (U - <u_x>) / tau,
+ *                           S = (0, s, 0, 0, u_x s), <u_x> the volume average over the inner cells of
+ *                           the state being differentiated (run/periodic_hill/run.c:8-21) */
+enum { TG_SOURCE_NONE = 0, TG_SOURCE_BODY_FORCE = 1, TG_SOURCE_BULK_FORCING = 2 };
+
 /* time integrators of simulation_set_advance (src/simulation/set.c:74-131) */
 enum { TG_ADVANCE_EULER = 0, TG_ADVANCE_LSERK = 1, TG_ADVANCE_IMPLICIT_EULER = 2 };
 
@@ -90,6 +100,7 @@ int tg_viscous_select(const char *name);
 int tg_limiter_select(const char *name);
 int tg_boundary_select(const char *name, int physics);
 int tg_advance_select(const char *name);
+int tg_source_select(const char *name); /* "body force", "bulk forcing" */
 
 /* ---- mesh: teal's Mesh arrays (src/mesh.h:13-72), one process ---------------------------------- */
 typedef struct {
@@ -143,6 +154,8 @@ typedef struct {
     int num_boundaries; /* off_boundary_entities - num_inner_entities */
     const int *boundary_kind;       /* [num_boundaries] TG_BC_* */
     const double *boundary_context; /* [num_boundaries][5] primitive state (may be null) */
+    int source;                     /* TG_SOURCE_* */
+    double source_parameter[4];     /* see TG_SOURCE_* */
 } tg_equations;
 
 /* contexts of the Advance methods, teal's layouts (src/simulation.h:25-34) */

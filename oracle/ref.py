@@ -49,6 +49,7 @@ def lib():
             "ref_set_viscous": (None, [vp, ctypes.c_char_p]),
             "ref_set_limiter": (None, [vp, ctypes.c_char_p, ctypes.c_double]),
             "ref_set_property": (None, [vp, ctypes.c_char_p, ctypes.c_double]),
+            "ref_set_source": (None, [vp, ctypes.c_int, dp]),
             "ref_set_boundary": (None, [vp, ctypes.c_char_p, ctypes.c_char_p, dp]),
             "ref_primitive": (dp, [vp]),
             "ref_limiter_parameter": (dp, [vp]),
@@ -207,6 +208,13 @@ class RefEquations:
 
     def set_property(self, name, value):
         lib().ref_set_property(self.ptr, name.encode(), value)
+
+    def set_source(self, name, parameters=()):
+        """The run cases' source callbacks: "body force" (gx, gy, gz) or "bulk forcing" (U, tau)."""
+        kind = {None: 0, "body force": 1, "bulk forcing": 2}[name]
+        p = [float(x) for x in parameters][:4]
+        self._src = np.array(p + [0.0] * (4 - len(p)))
+        lib().ref_set_source(self.ptr, kind, _d(self._src))
 
     def set_boundary_condition(self, entity, name, context=None):
         ctx = None

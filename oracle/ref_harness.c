@@ -235,6 +235,49 @@ void ref_set_limiter(void *eqns, const char *name, double coefficient)
     equations_set_limiter(eqns, (name && name[0]) ? name : 0, coefficient);
 }
 
+/* Source terms as teal's run cases write them (host callbacks handed to equations_set_source):
+ * kind 1, a body force with acceleration (p0, p1, p2) (run/rayleigh_taylor_instability/run.c:17-24,
+ * there (0, -gravity, 0)); kind 2, bulk forcing of the x velocity towards p0 with time scale p1,
+ * its Prepare averaging the state over "domain" with the reference's equations_average
+ * (run/periodic_hill/run.c:8-21, there p0 = 1, p1 = 0.001). One source setting per process. */
+static double src_par[4];
+static double src_average[5];
+
+static void src_body_force(void *source_, const double *property, Vector center, double time, const void *context)
+{
+    double *source = source_;
+    const double *primitive = context;
+    (void)property, (void)center, (void)time;
+    source[1] = src_par[0] * primitive[0];
+    source[2] = src_par[1] * primitive[0];
+    source[3] = src_par[2] * primitive[0];
+    source[4] = ((source[1] * primitive[1]) + (source[2] * primitive[2])) + (source[3] * primitive[3]);
+}
+
+static void src_bulk_prepare(const Equations *eqns, const void *primitive)
+{
+    equations_average(eqns, "domain", primitive, src_average);
+}
+
+static void src_bulk_forcing(void *source_, const double *property, Vector center, double time,
+                             const void *context)
+{
+    double *source = source_;
+    const double *primitive = context;
+    (void)property, (void)center, (void)time;
+    double s1 = primitive[0] * (src_par[0] - src_average[1]) / src_par[1];
+    source[1] = s1;
+    source[4] = primitive[1] * s1;
+}
+
+void ref_set_source(void *eqns, int kind, const double *par)
+{
+    for (int i = 0; i < 4; i++) src_par[i] = par ? par[i] : 0.0;
+    if (kind == 1) equations_set_source(eqns, src_body_force, 0);
+    else if (kind == 2) equations_set_source(eqns, src_bulk_forcing, src_bulk_prepare);
+    else equations_set_source(eqns, 0, 0);
+}
+
 void ref_set_property(void *eqns, const char *name, double value)
 {
     equations_set_property(eqns, name, value);

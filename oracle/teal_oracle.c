@@ -672,8 +672,35 @@ int oracle_derivative(const tg_mesh *m, const tg_equations *e, double *prim, dou
         }
         free(g);
     }
-    for (int i = 0; i < C; i++) { /* finalize_derivative (derivative.c:229-267) */
-        for (int j = 0; j < 5; j++) d[5 * (size_t)i + j] = -d[5 * (size_t)i + j] / m->cell_volume[i];
+    /* finalize_derivative (derivative.c:229-267), with the source kinds of the run cases:
+     * body force (run/rayleigh_taylor_instability/run.c:17-24) and bulk forcing, whose prepare pass
+     * averages the state over the inner cells (run/periodic_hill/run.c:8-21, average.c:8-40) */
+    const double *sp = e->source_parameter;
+    double avg[5] = {0, 0, 0, 0, 0};
+    if (e->source == TG_SOURCE_BULK_FORCING) {
+        for (int i = 0; i < C; i++) {
+            for (int j = 0; j < 5; j++) avg[j] += m->cell_volume[i] * prim[5 * (size_t)i + j];
+        }
+        for (int j = 0; j < 5; j++) avg[j] /= m->sum_volume;
+    }
+    for (int i = 0; i < C; i++) {
+        const double *q = prim + 5 * (size_t)i;
+        double src[5] = {0, 0, 0, 0, 0};
+        if (e->source == TG_SOURCE_BODY_FORCE) {
+            src[1] = sp[0] * q[0];
+            src[2] = sp[1] * q[0];
+            src[3] = sp[2] * q[0];
+            src[4] = ((src[1] * q[1]) + (src[2] * q[2])) + (src[3] * q[3]);
+        }
+        else if (e->source == TG_SOURCE_BULK_FORCING) {
+            double s1 = q[0] * (sp[0] - avg[1]) / sp[1];
+            src[1] = s1;
+            src[4] = q[1] * s1;
+        }
+        for (int j = 0; j < 5; j++) {
+            d[5 * (size_t)i + j] = -d[5 * (size_t)i + j] / m->cell_volume[i];
+            if (e->source != TG_SOURCE_NONE) d[5 * (size_t)i + j] = d[5 * (size_t)i + j] + src[j];
+        }
     }
     return 0;
 }

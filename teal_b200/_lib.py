@@ -25,6 +25,7 @@ TG_VISCOUS_NONE, TG_VISCOUS_CENTRAL = 0, 1
 TG_LIMITER_NONE, TG_LIMITER_BARTH_JESPERSEN, TG_LIMITER_VENKATAKRISHNAN = 0, 1, 2
 TG_ADVANCE_EULER, TG_ADVANCE_LSERK, TG_ADVANCE_IMPLICIT_EULER = 0, 1, 2
 TG_PRECISION_FP64, TG_PRECISION_FP32_FLUX = 0, 1
+TG_SOURCE_NONE, TG_SOURCE_BODY_FORCE, TG_SOURCE_BULK_FORCING = 0, 1, 2
 TG_NOALLOC_MAX_CELLS = 67108864  # cell limit of tg_residual_noalloc (its fixed scratch array)
 
 _int_p = ctypes.POINTER(ctypes.c_int)
@@ -82,6 +83,8 @@ class TgEquations(ctypes.Structure):
         ("num_boundaries", ctypes.c_int),
         ("boundary_kind", _int_p),
         ("boundary_context", _dbl_p),
+        ("source", ctypes.c_int),
+        ("source_parameter", ctypes.c_double * 4),
     ]
 
 
@@ -105,6 +108,7 @@ SIGNATURES = [
     ("tg_limiter_select", ctypes.c_int, [ctypes.c_char_p]),
     ("tg_boundary_select", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int]),
     ("tg_advance_select", ctypes.c_int, [ctypes.c_char_p]),
+    ("tg_source_select", ctypes.c_int, [ctypes.c_char_p]),
     ("tg_create", ctypes.c_int, [ctypes.POINTER(TgMesh), ctypes.POINTER(TgEquations), ctypes.c_int,
                                  ctypes.POINTER(_vp)]),
     ("tg_destroy", ctypes.c_int, [_vp]),

@@ -113,6 +113,14 @@ extern "C" int tg_boundary_select(const char *name, int physics)
     return -1;
 }
 
+extern "C" int tg_source_select(const char *name)
+{
+    if (!name) return -1;
+    if (!strcmp(name, "body force")) return TG_SOURCE_BODY_FORCE;
+    if (!strcmp(name, "bulk forcing")) return TG_SOURCE_BULK_FORCING;
+    return -1;
+}
+
 extern "C" int tg_advance_select(const char *name)
 {
     if (!name) return -1;
@@ -171,6 +179,9 @@ enum { SI_VARIABLE, SI_ITER, SI_MAX_ITER, SI_ACTIVE, SI_COUNT };
 
 struct tg_ctx {
     int device = 0;
+    int source = TG_SOURCE_NONE;  // device source term kind and its parameters
+    double src_par[4] = {0, 0, 0, 0};
+    double *src_avg = nullptr;    // [ninst][5] volume averages (bulk forcing)
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
 
@@ -289,7 +300,7 @@ static void free_ctx(tg_ctx *c)
                     c->gb.slot_w, c->gb.slot_off, c->gb.area32, c->gb.basis32, c->gb.offl32, c->gb.offr32,
                     c->gb.corr32, c->gb.slot_w32, c->gb.slot_off32, c->q, c->U0, c->R, c->qs, c->grad, c->G,
                     c->dtc, c->part_min, c->part_sum, c->sd, c->si, c->aos, c->rowmap, c->cell_inst,
-                    c->inst_cell_off, c->piece_beg, c->inst_piece_off, c->sum_volume};
+                    c->inst_cell_off, c->piece_beg, c->inst_piece_off, c->sum_volume, c->src_avg};
     for (void *p : ptrs) {
         if (p) cudaFree(p);
     }
@@ -435,6 +446,10 @@ static int validate(const tg_mesh *m, const tg_equations *e)
         return fail(TG_ERR_INVALID, "viscous flux needs face corrections");
     if (e->limiter < TG_LIMITER_NONE || e->limiter > TG_LIMITER_VENKATAKRISHNAN)
         return fail(TG_ERR_INVALID, "invalid limiter kind (%d)", e->limiter);
+    if (e->source < TG_SOURCE_NONE || e->source > TG_SOURCE_BULK_FORCING)
+        return fail(TG_ERR_INVALID, "invalid source kind (%d)", e->source);
+    if (e->source == TG_SOURCE_BULK_FORCING && !(e->source_parameter[1] != 0))
+        return fail(TG_ERR_INVALID, "bulk forcing needs a nonzero time scale");
     int nb = m->off_boundary_entities - m->num_inner_entities;
     if (nb != e->num_boundaries)
         return fail(TG_ERR_INVALID, "boundary count %d does not match the mesh (%d)", e->num_boundaries, nb);
@@ -519,7 +534,8 @@ static int merged_input(const tg_mesh *ms, const tg_equations *es, int num, Mesh
         const tg_equations &e = es[i];
         if (e.physics != e0.physics || e.space_order != e0.space_order || e.convective != e0.convective ||
             e.viscous != e0.viscous || e.limiter != e0.limiter || e.property[0] != e0.property[0] ||
-            e.property[1] != e0.property[1] || e.property[2] != e0.property[2])
+            e.property[1] != e0.property[1] || e.property[2] != e0.property[2] || e.source != e0.source ||
+            memcmp(e.source_parameter, e0.source_parameter, sizeof(e.source_parameter)) != 0)
             return fail(TG_ERR_INVALID, "batch instance %d differs in equations, schemes or properties", i);
     }
     long C = 0, NB = 0, NP = 0, Fi = 0, Fb = 0, Fp = 0, nbnd = 0, rows = 0;
@@ -709,6 +725,8 @@ static int create_ctx(MeshInput &in, const tg_equations *e, int precision, tg_ct
         c->limiter = e->limiter;
         c->precision = precision;
         for (int i = 0; i < 3; i++) c->prop[i] = e->property[i];
+        c->source = e->source;
+        for (int i = 0; i < 4; i++) c->src_par[i] = e->source_parameter[i];
 
         // instances and reduction pieces
         c->ninst = (int)in.inst_cell_off.size() - 1;
@@ -848,6 +866,7 @@ static int create_ctx(MeshInput &in, const tg_equations *e, int precision, tg_ct
         CU(cudaMemsetAsync(c->dtc, 0, sizeof(double) * s.C, st));
         TRY(dalloc(&c->part_min, c->npieces));
         TRY(dalloc(&c->part_sum, 5 * (size_t)c->npieces));
+        TRY(dalloc(&c->src_avg, 5 * (size_t)c->ninst));
         TRY(dalloc(&c->sd, (size_t)SD_COUNT * c->ninst));
         TRY(dalloc(&c->si, (size_t)SI_COUNT * c->ninst + 2));
         CU(cudaMallocHost(&c->hd, sizeof(double) * SD_COUNT * c->ninst));
@@ -1136,13 +1155,24 @@ static int run_face(tg_ctx *c, const double *q)
     return TG_OK;
 }
 
+template <int MODE, bool NS, typename GT, int SRC>
+static void launch_cell_s(tg_ctx *c, double alpha, int last, double *q, double *Rout)
+{
+    CellData cd{c->volume, c->proj, c->eps2};
+    Source src{{c->src_par[0], c->src_par[1], c->src_par[2], c->src_par[3]}, c->src_avg};
+    k_cell<MODE, NS, GT, SRC><<<(c->s.C + CELL_BLOCK - 1) / CELL_BLOCK, CELL_BLOCK, 0, c->stream>>>(
+        c->s, c->slot_face, c->slot_cnt, cd, (const GT *)c->G, c->U0, q, Rout, c->seg, c->st, alpha, last,
+        props_of(c), c->dtc, src);
+}
+
 template <int MODE, bool NS, typename GT>
 static void launch_cell_t(tg_ctx *c, double alpha, int last, double *q, double *Rout)
 {
-    CellData cd{c->volume, c->proj, c->eps2};
-    k_cell<MODE, NS, GT><<<(c->s.C + CELL_BLOCK - 1) / CELL_BLOCK, CELL_BLOCK, 0, c->stream>>>(c->s, c->slot_face, c->slot_cnt, cd,
-                                                                  (const GT *)c->G, c->U0, q, Rout, c->seg,
-                                                                  c->st, alpha, last, props_of(c), c->dtc);
+    switch (c->source) {
+        case TG_SOURCE_BODY_FORCE: launch_cell_s<MODE, NS, GT, 1>(c, alpha, last, q, Rout); break;
+        case TG_SOURCE_BULK_FORCING: launch_cell_s<MODE, NS, GT, 2>(c, alpha, last, q, Rout); break;
+        default: launch_cell_s<MODE, NS, GT, 0>(c, alpha, last, q, Rout); break;
+    }
 }
 
 template <int MODE>
@@ -1169,6 +1199,13 @@ static int launch_cell(tg_ctx *c, double alpha, int last, double *q, double *Rou
 // boundary pass, gradient + limiter, face fluxes: everything of a residual before the gather
 static int run_fluxes(tg_ctx *c, double *q, bool masked = false)
 {
+    if (c->source == TG_SOURCE_BULK_FORCING) {
+        // the Prepare pass: volume averages of the state being differentiated, per instance
+        Launch l(c, TG_PROF_REDUCE);
+        k_piece_average<<<c->npieces, BLOCK, 0, c->stream>>>(c->seg, c->s.N, q, c->volume, c->part_sum);
+        k_inst_average<<<(c->ninst + 127) / 128, 128, 0, c->stream>>>(c->seg, c->part_sum, c->src_avg);
+        CU(cudaGetLastError());
+    }
     TRY(run_boundary(c, q, masked));
     if (c->order == 2) TRY(run_gradient(c, q));
     TRY(run_face(c, q));

@@ -187,13 +187,84 @@ struct Props {
 // U = U0 + R * alpha * step, q = prim(U), with the step of the cell's instance (cells of inactive
 // instances keep their state). With `last`, also: R kept, U0 <- cons(q) for the next step and the
 // cell's stable time step of the new state.
-template <int MODE, bool NS, typename GT>
+// Device source terms in place of teal's Compute / Prepare callbacks (src/equations.h:27-41):
+// kind TG_SOURCE_BODY_FORCE (p = acceleration) or TG_SOURCE_BULK_FORCING (p = target x velocity,
+// time scale; avg = per-instance volume average of the primitive state being differentiated)
+struct Source {
+    double p[4];
+    const double *avg;  // [ninst][5]
+};
+
+// R += S(q) as teal's finalize_derivative adds source[j] to -sum / V (derivative.c:260-265)
+template <int SRC>
+__device__ __forceinline__ void add_source(const Source &src, const Prim<double> &q, int inst, double (&r)[5])
+{
+    double sv[5] = {0, 0, 0, 0, 0};
+    if (SRC == 1) {  // body force (run/rayleigh_taylor_instability/run.c:17-24)
+        sv[1] = src.p[0] * q.rho;
+        sv[2] = src.p[1] * q.rho;
+        sv[3] = src.p[2] * q.rho;
+        sv[4] = ((sv[1] * q.u.x) + (sv[2] * q.u.y)) + (sv[3] * q.u.z);
+    }
+    else if (SRC == 2) {  // bulk forcing (run/periodic_hill/run.c:8-21)
+        const double s1 = (q.rho * (src.p[0] - src.avg[5 * inst + 1])) / src.p[1];
+        sv[1] = s1;
+        sv[4] = q.u.x * s1;
+    }
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        r[v] = r[v] + sv[v];
+    }
+}
+
+// per-piece volume-weighted sums of the primitive state (the Prepare of the bulk forcing:
+// equations_average over the inner cells, src/equations/average.c:8-40)
+__global__ void __launch_bounds__(BLOCK) k_piece_average(Segments seg, int N, const double *__restrict__ q,
+                                                         const double *__restrict__ volume,
+                                                         double *__restrict__ part)
+{
+    __shared__ double sh[BLOCK / 32];
+    const int beg = seg.piece_beg[blockIdx.x], end = seg.piece_beg[blockIdx.x + 1];
+    double t[5] = {0, 0, 0, 0, 0};
+    for (int c = beg + threadIdx.x; c < end; c += BLOCK) {
+        const double v = volume[c];
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+            t[k] += v * q[(size_t)k * N + c];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        double sum = block_sum<BLOCK>(t[k], sh);
+        if (threadIdx.x == 0) {
+            part[5 * blockIdx.x + k] = sum;
+        }
+    }
+}
+
+// avg[i] = sum of instance i's piece sums / its volume
+__global__ void k_inst_average(Segments seg, const double *__restrict__ part, double *__restrict__ avg)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= seg.ninst) {
+        return;
+    }
+    for (int k = 0; k < 5; k++) {
+        double t = 0;
+        for (int p = seg.inst_piece_off[i]; p < seg.inst_piece_off[i + 1]; p++) {
+            t += part[5 * p + k];
+        }
+        avg[5 * i + k] = t / seg.sum_volume[i];
+    }
+}
+
+template <int MODE, bool NS, typename GT, int SRC>
 __global__ void __launch_bounds__(CELL_BLOCK) k_cell(Sizes s, const int *__restrict__ slot_face,
                                                 const uint8_t *__restrict__ slot_cnt, CellData cd,
                                                 const GT *__restrict__ G, double *__restrict__ U0,
                                                 double *__restrict__ q, double *__restrict__ Rout,
                                                 Segments seg, Steps st, double alpha, int last, Props prop,
-                                                double *__restrict__ dtc)
+                                                double *__restrict__ dtc, Source src)
 {
     const int C = s.C, N = s.N;
     int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -229,6 +300,11 @@ __global__ void __launch_bounds__(CELL_BLOCK) k_cell(Sizes s, const int *__restr
         for (int v = 0; v < 5; v++) {
             r[v] = -acc[v] / vol;
         }
+    }
+    if (SRC != 0) {
+        // the state being differentiated (plain loads: this kernel writes q afterwards)
+        Prim<double> qc{q[c], v3(q[N + c], q[2 * N + c], q[3 * N + c]), q[4 * N + c]};
+        add_source<SRC>(src, qc, __ldg(seg.cell_inst + c), r);
     }
     if (MODE == 0 || last) {
 #pragma unroll

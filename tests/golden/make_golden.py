@@ -63,6 +63,18 @@ def cases():
                     ns=False, flux="roe", limiter=None, coeff=0.0, state="freestream", seed=6,
                     bcs={s: ["farfield", FREE] for s in SIDES[:4]},
                     advance=dict(method="implicit euler", courant=20.0, nk=[0.1, 0.3, 10], steps=1)))
+    # device source terms in place of the run cases' callbacks: a body force (Rayleigh-Taylor-like
+    # stratification between slip walls) and bulk forcing of the x velocity (channel between walls)
+    out.append(dict(name="source_body_force", n=[10, 12, 2], lo=[-0.25, -0.75, 0], hi=[0.25, 0.75, 0.1],
+                    periodic=[1, 0, 1], ns=False, flux="hllc", limiter="minmod", coeff=0.0, state="random",
+                    seed=21, mach=0.3, bcs={"bottom": ["slipwall", None], "top": ["slipwall", None]},
+                    source=["body force", [0.0, -0.1, 0.0]],
+                    advance=dict(method="lserk", courant=0.5, rk=[3, 3], steps=3)))
+    out.append(dict(name="source_bulk_forcing", n=[12, 8, 2], lo=[0, 0, 0], hi=[3, 1, 0.25], periodic=[1, 0, 1],
+                    ns=True, flux="roe", limiter="venkatakrishnan", coeff=1.0, mu=0.01, state="random",
+                    seed=22, mach=0.3, bcs={"bottom": ["adiabatic wall", None], "top": ["adiabatic wall", None]},
+                    source=["bulk forcing", [1.0, 0.5]],
+                    advance=dict(method="lserk", courant=0.5, rk=[3, 3], steps=3)))
     # the unstructured compression ramp (tetrahedra, prisms, hexahedra, pyramid transitions)
     ramp = dict(kind="ramp", n=[10, 8, 6], block=4, seed=1)
     out.append(dict(name="ramp_euler_ausmd_bj", mesh=ramp, ns=False, flux="ausmd", limiter="minmod", coeff=0.0,
@@ -106,6 +118,8 @@ def ref_equations(case):
         e.set_property("dynamic viscosity", case["mu"])
     for ent, (name, ctx) in case.get("bcs", {}).items():
         e.set_boundary_condition(ent, name, ctx)
+    if "source" in case:
+        e.set_source(*case["source"])
     return m, e
 
 

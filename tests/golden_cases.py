@@ -40,4 +40,6 @@ def equations(case):
         e.set_property("dynamic viscosity", case["mu"])
     for ent, (name, ctx) in case.get("bcs", {}).items():
         e.set_boundary_condition(ent, name, ctx)
+    if "source" in case:
+        e.set_source(*case["source"])
     return m, e

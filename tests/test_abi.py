@@ -96,3 +96,9 @@ def test_create_rejects_invalid_input_before_touching_a_device():
     st = _lib.lib.tg_create(_lib.ctypes.byref(m.struct), _lib.ctypes.byref(s), 0, _lib.ctypes.byref(h))
     assert st == _lib.TG_ERR_INVALID
     assert b"space order" in _lib.lib.tg_last_error()
+
+
+def test_source_select():
+    assert _lib.lib.tg_source_select(b"body force") == _lib.TG_SOURCE_BODY_FORCE
+    assert _lib.lib.tg_source_select(b"bulk forcing") == _lib.TG_SOURCE_BULK_FORCING
+    assert _lib.lib.tg_source_select(b"gravity") == -1

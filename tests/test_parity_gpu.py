@@ -383,3 +383,65 @@ def test_unstructured_ramp_implicit_step():
     # the reference's own step on this case moves by 4.4e-8..4.6e-8 under a 1e-16 relative input
     # perturbation (measured, three seeds); the bar is ~10x that
     assert rel_l2(pd, pr).max() <= 5e-7
+
+
+# ---- device source terms (in place of the run cases' host callbacks) ---------------------------
+
+def rayleigh_taylor_state(center, gravity=0.1):
+    """Heavy over light fluid in hydrostatic balance with a small velocity perturbation (the shape
+    of run/rayleigh_taylor_instability/run.c's initial condition)."""
+    x, y = center[:, 0], center[:, 1]
+    rho = np.where(y > 0, 2.0, 1.0)
+    out = np.zeros((center.shape[0], 5))
+    out[:, 0] = rho
+    out[:, 2] = 0.01 * (1 + np.cos(4 * np.pi * x)) * (1 + np.cos(3 * np.pi * y)) / 4
+    out[:, 4] = 2.5 - gravity * rho * y
+    return out
+
+
+def test_source_body_force_rayleigh_taylor():
+    bcs = {"bottom": ("slipwall", None), "top": ("slipwall", None)}
+    rm, re, dm, de = pair((16, 48, 2), (-0.25, -0.75, 0), (0.25, 0.75, 0.05), (1, 0, 1), bcs=bcs)
+    for e in (re, de):
+        e.set_source("body force", (0.0, -0.1, 0.0))
+    prim = rayleigh_taylor_state(dm.cell_center)
+    check_derivative(re, de, prim)
+    (tr, sr, rr, pr), (td, sd, rd, pd) = run_both(re, de, prim, "lserk", 0.5, 10, rk=(3, 3))
+    assert rel_l2(pd, pr).max() <= TOL
+    assert abs(td - tr) <= 1e-13 * tr
+
+
+def test_source_bulk_forcing_channel():
+    """Bulk forcing with the periodic hill's constants (target 1, time scale 0.001) on a walled
+    channel: the prepare pass averages the state being differentiated, on the device."""
+    bcs = {"bottom": ("wall", None), "top": ("wall", None)}
+    rm, re, dm, de = pair((18, 10, 2), (0, 0, 0), (9, 3, 0.3), (1, 0, 1), ns=True, flux="roe",
+                          limiter="venkatakrishnan", coeff=1.0, mu=0.01, bcs=bcs)
+    for e in (re, de):
+        e.set_source("bulk forcing", (1.0, 0.001))
+    prim = random_state(dm.num_cells, seed=41, mach=0.4)
+    check_derivative(re, de, prim)
+    (tr, sr, rr, pr), (td, sd, rd, pd) = run_both(re, de, prim, "lserk", 0.3, 5, rk=(3, 3))
+    assert rel_l2(pd, pr).max() <= TOL
+
+
+def test_source_in_a_batch_is_bit_identical_to_solo():
+    def problem(n):
+        m = tb.Mesh.create((-0.25, -0.75, 0), (0.25, 0.75, 0.05), (n, 3 * n, 2), (1, 0, 1))
+        e = tb.Equations.euler(m)
+        for side in ("bottom", "top"):
+            e.set_boundary_condition(side, "slipwall")
+        e.set_source("body force", (0.0, -0.1, 0.0))
+        e.set_initial_condition("domain", rayleigh_taylor_state)
+        return e
+
+    ps = [problem(8), problem(12)]
+    b = tb.Batch(ps)
+    t, it, res = b.run(tb.TG_ADVANCE_LSERK, 0.5, [4, 6], context=(3, 3))
+    for i, e in enumerate(ps):
+        ctx = tb.Context(e.mesh, e)
+        ctx.set_primitive(e.primitive)
+        t1, it1, res1 = ctx.run(tb.TG_ADVANCE_LSERK, 0.5, [4, 6][i], context=(3, 3))
+        C = e.mesh.num_inner_cells
+        assert t[i] == t1 and np.array_equal(res[i], res1)
+        assert np.array_equal(b.get_primitive(i)[:C], ctx.get_primitive()[:C])
