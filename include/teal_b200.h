@@ -212,6 +212,10 @@ int tg_residual(tg_ctx *ctx, const double *derivative, double *residual);
 int tg_advance(tg_ctx *ctx, int method, const void *context, double courant, double *time,
                double max_step, double *residual, double *step0);
 
+/* Unclipped step (step0) of the last step taken by `instance` (0 for a single mesh), as teal's run
+ * loop prints it (simulation/run.c:95-96). */
+int tg_last_step(tg_ctx *ctx, int instance, double *step0);
+
 /* simulation_run's loop with the state resident: up to max_iter steps or until max_time, or until
  * the residual of `variable` (-1 = maximum) drops below `threshold` (threshold <= 0: never).
  * Steps are replayed from CUDA graphs; the host synchronises only when it must test the residual.

@@ -64,6 +64,8 @@ def lib():
             "ref_simulation_set_max_iter": (None, [vp, ctypes.c_int]),
             "ref_simulation_set_max_time": (None, [vp, ctypes.c_double]),
             "ref_simulation_set_termination": (None, [vp, ctypes.c_char_p, ctypes.c_double]),
+            "ref_simulation_set_out_time": (None, [vp, ctypes.c_double]),
+            "ref_simulation_set_out_iter": (None, [vp, ctypes.c_int]),
             "ref_simulation_run": (ctypes.c_double, [vp]),
             "ref_advance": (ctypes.c_double, [vp, dp, dp, ctypes.c_double]),
             "ref_simulation_destroy": (None, [vp]),
@@ -279,6 +281,12 @@ class RefSimulation:
 
     def set_termination(self, condition, threshold):
         lib().ref_simulation_set_termination(self.ptr, condition.encode(), threshold)
+
+    def set_out_time(self, t):
+        lib().ref_simulation_set_out_time(self.ptr, t)
+
+    def set_out_iter(self, n):
+        lib().ref_simulation_set_out_iter(self.ptr, n)
 
     def run(self):
         return lib().ref_simulation_run(self.ptr)

@@ -370,6 +370,16 @@ void ref_simulation_set_max_time(void *sim, double time)
     simulation_set_max_time(sim, time);
 }
 
+void ref_simulation_set_out_time(void *sim, double time)
+{
+    simulation_set_out_time(sim, time);
+}
+
+void ref_simulation_set_out_iter(void *sim, int iter)
+{
+    simulation_set_out_iter(sim, iter);
+}
+
 void ref_simulation_set_termination(void *sim, const char *condition, double threshold)
 {
     simulation_set_termination(sim, condition, threshold);

@@ -124,6 +124,7 @@ SIGNATURES = [
                                   _vp, _dbl_p]),
     ("tg_run", ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_double, ctypes.c_int, ctypes.c_double,
                               ctypes.c_int, ctypes.c_double, _dbl_p, _int_p, _vp]),
+    ("tg_last_step", ctypes.c_int, [_vp, ctypes.c_int, _dbl_p]),
     ("tg_batch_create", ctypes.c_int, [ctypes.POINTER(TgMesh), ctypes.POINTER(TgEquations), ctypes.c_int,
                                        ctypes.c_int, ctypes.POINTER(_vp)]),
     ("tg_batch_size", ctypes.c_int, [_vp, _int_p]),

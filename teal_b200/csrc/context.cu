@@ -1563,6 +1563,15 @@ extern "C" int tg_run(tg_ctx *c, int method, const void *context, double courant
     return TG_OK;
 }
 
+extern "C" int tg_last_step(tg_ctx *c, int instance, double *step0)
+{
+    if (!c || !step0) return fail(TG_ERR_INVALID, "null argument");
+    if (instance < 0 || instance >= c->ninst) return fail(TG_ERR_INVALID, "invalid instance (%d)", instance);
+    TRY(read_steps(c));
+    *step0 = hd_at(c, SD_STEP0, instance);
+    return TG_OK;
+}
+
 extern "C" int tg_batch_run(tg_ctx *c, int method, const void *context, double courant, const int *max_iter,
                             const double *max_time, const int *variable, const double *threshold, double *time,
                             int *iter, double *residual)

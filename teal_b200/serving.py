@@ -48,6 +48,7 @@ class Request:
     residual: object = None
     state: object = None
     error: str = ""
+    cancelled: bool = False          # set by Scheduler.cancel; a running solve stops at its next chunk
 
     @property
     def num_cells(self):
@@ -90,8 +91,37 @@ class Scheduler:
         self.peak_used = 0
         self.peak_active = 0
         self.t0 = None
+        self._cancel_pending = set()
+
+    def cancel(self, rid):
+        """Cancel request `rid`: a waiting or not yet arrived request never runs, a running one stops
+        at its next chunk boundary (its memory and slot are released when its worker returns)."""
+        with self.lock:
+            for k, (arrival, wid, r) in enumerate(self.waiting):
+                if wid == rid:
+                    self.waiting.pop(k)
+                    heapq.heapify(self.waiting)
+                    r.cancelled = True
+                    r.error = "cancelled"
+                    r.finished = (self.clock() - self.t0) if self.t0 is not None else r.arrival
+                    self.done.append(r)
+                    self.lock.notify_all()
+                    return True
+            if rid in self.active:
+                self.active[rid][0].cancelled = True
+                return True
+            self._cancel_pending.add(rid)
+            return False
 
     def submit(self, req):
+        if req.id in self._cancel_pending or req.cancelled:
+            req.cancelled = True
+            req.error = "cancelled"
+            req.finished = req.arrival
+            with self.lock:
+                self.done.append(req)
+                self.lock.notify_all()
+            return
         if self.estimate(req) > self.budget:
             req.error = "request exceeds the device memory budget"
             req.finished = req.arrival
@@ -105,6 +135,8 @@ class Scheduler:
     def _worker(self, req, nbytes):
         try:
             self.execute(req)
+            if req.cancelled and not req.error:
+                req.error = "cancelled"
         except Exception as exc:  # a failing request is reported, never fatal to the server
             req.error = f"{type(exc).__name__}: {exc}"
         with self.lock:
@@ -153,7 +185,7 @@ class Scheduler:
         return sorted(self.done, key=lambda r: r.id)
 
 
-def solve(req, stream=None):
+def solve(req, stream=None, chunk=25):
     """Solve one request on the current GPU (its own context; used alone or by the server)."""
     from .api import Equations, Mesh
 
@@ -180,10 +212,15 @@ def solve(req, stream=None):
     method = _lib.TG_ADVANCE_LSERK
     t, it, res = ctx.run(method, req.courant, 1, context=(3, 3))
     total = it
-    if req.steps > 1:
-        threshold = req.tolerance * float(np.max(res)) if req.tolerance > 0 else 0.0
-        t, it, res = ctx.run(method, req.courant, req.steps - 1, threshold=threshold, context=(3, 3), time=t)
+    threshold = req.tolerance * float(np.max(res)) if req.tolerance > 0 else 0.0
+    # the remaining steps in chunks (the same steps, replayed from the same graph), so a cancelled
+    # request stops at the next chunk boundary
+    while total < req.steps and not req.cancelled:
+        n = min(chunk, req.steps - total)
+        t, it, res = ctx.run(method, req.courant, n, threshold=threshold, context=(3, 3), time=t)
         total += it
+        if it < n:  # the residual fell below the threshold
+            break
     req.iterations = total
     req.residual = res
     req.state = ctx.get_primitive()[: mesh.num_inner_cells]

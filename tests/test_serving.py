@@ -28,7 +28,9 @@ class FakeExec:
             self.peak = max(self.peak, self.running)
             self.order.append(req.id)
         try:
-            time.sleep(self.seconds)
+            t_end = time.perf_counter() + self.seconds
+            while time.perf_counter() < t_end and not req.cancelled:
+                time.sleep(0.002)
             if req.id in self.fail_ids:
                 raise RuntimeError("device fault injected on the host")
             req.iterations = req.steps
@@ -92,3 +94,18 @@ def test_poisson_requests_are_seeded():
     assert [(r.cells, r.mach, r.flux, r.arrival) for r in a] == [(r.cells, r.mach, r.flux, r.arrival) for r in b]
     assert all(20_000 * 0.8 <= r.num_cells <= 2_000_000 * 1.2 for r in a)
     assert serving.percentile([1, 2, 3, 4], 50) == pytest.approx(2.5)
+
+
+def test_cancel_waiting_and_running_requests():
+    reqs = make(4)
+    ex = FakeExec(seconds=0.3)
+    s = serving.Scheduler(budget_bytes=1 << 40, max_active=1, execute=ex)
+    s.cancel(3)  # not yet arrived: never runs
+    timer = threading.Timer(0.05, lambda: (s.cancel(0), s.cancel(2)))  # 0 running, 2 waiting
+    timer.start()
+    done = s.run(reqs, timeout=30)
+    timer.join()
+    assert [r.error for r in done] == ["cancelled", "", "cancelled", "cancelled"]
+    assert ex.order == [0, 1]
+    assert done[0].finished < 0.3  # the running request stopped early
+    assert s.used == 0 and not s.active

@@ -33,3 +33,28 @@ def test_tolerance_stops_a_request_early():
     r = serving.Request(id=0, cells=(24, 12, 2), mach=0.5, steps=400, tolerance=1e-1)
     serving.solve(r)
     assert 1 < r.iterations < 400
+
+
+def test_cancelled_request_stops_early():
+    import threading
+
+    server = serving.Server(max_active=2)
+    reqs = [serving.Request(id=0, cells=(200, 100, 2), steps=200000, arrival=0.0),
+            serving.Request(id=1, cells=(40, 20, 2), steps=20, arrival=0.0)]
+
+    def cancel_once_running():
+        import math
+        import time
+
+        for _ in range(3000):
+            if not math.isnan(reqs[0].admitted) and server.scheduler.cancel(0):
+                return
+            time.sleep(0.01)
+
+    timer = threading.Thread(target=cancel_once_running)
+    timer.start()
+    done = server.serve(reqs, timeout=300)
+    timer.join()
+    assert done[0].error == "cancelled" and done[0].iterations < 200000
+    assert not done[1].error and done[1].iterations == 20
+    assert server.scheduler.used == 0
