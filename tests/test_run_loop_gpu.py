@@ -89,3 +89,25 @@ def test_stop_request_ends_at_the_next_output_point():
 
     sim.run(on_output=on_output)
     assert seen == [3] and sim.iterations == 3
+
+
+def test_runs_are_deterministic():
+    """No floating-point atomics: the same steps give the same bits on every run (a fresh context
+    each time)."""
+    out = []
+    for _ in range(2):
+        m = tb.Mesh.create((0, 0, 0), (2 * np.pi,) * 3, (12, 12, 12), (1, 1, 1))
+        e = tb.Equations.navierstokes(m)
+        e.set_convective_flux("roe")
+        e.set_limiter("venkatakrishnan", 1.0)
+        e.set_property("dynamic viscosity", 1 / 1600)
+        from tests.cases import taylor_green
+
+        e.set_initial_condition("domain", taylor_green)
+        ctx = tb.Context(m, e)
+        ctx.set_primitive(e.primitive)
+        t, it, res = ctx.run(tb.TG_ADVANCE_LSERK, 0.99, 7, context=(3, 3))
+        out.append((t, res.copy(), ctx.get_primitive().copy()))
+        ctx.close()
+    assert out[0][0] == out[1][0]
+    assert np.array_equal(out[0][1], out[1][1]) and np.array_equal(out[0][2], out[1][2])
