@@ -26,11 +26,12 @@ CSRC = os.path.join(HERE, "csrc")
 ROOT = os.path.dirname(HERE)
 
 # face-flux block size x resident face threads per SM (65536 registers / threads = the cap per
-# thread: 512 -> 128, 768 -> 85) x geometry staged in shared memory by bulk copies or loaded by the
-# threads x cell-gather block size. The Navier-Stokes workload tunes the shapes and its staging
-# switch; the Euler staging switch is then tuned on the unstructured ramp with the chosen shapes.
-FACE_BLOCKS = [128, 256]
-FACE_THREADS = [512, 768]
+# thread: 512 -> 128, 640 -> 102, 768 -> 85) x geometry staged in shared memory by bulk copies or
+# loaded by the threads x cell-gather block size. The Navier-Stokes workload tunes the shapes and
+# its staging switch; the Euler staging switch is then tuned on the unstructured ramp with the
+# chosen shapes.
+FACE_BLOCKS = [32, 64, 128]
+FACE_THREADS = [512, 640, 768]
 STAGED = [0, 1]
 CELL_BLOCKS = [256]
 

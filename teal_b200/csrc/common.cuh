@@ -107,12 +107,10 @@ __device__ __forceinline__ Prim<R> reload_prim(const double *__restrict__ q, int
     return p;
 }
 
-// Per-cell gradient records. FOLD = false (Navier-Stokes with a limiter: the viscous flux needs the
-// unlimited gradient): (gx, gy, gz, psi) per variable, 20 values per cell, two 2-vector accesses per
-// variable. FOLD = true (psi multiplied in, or no limiter): the compact (gx, gy, gz) per variable,
-// 15 values + 1 pad = 16 per cell (128 bytes in FP64: one cache line per cell), a 2-vector and a
-// scalar access per variable (which comes first alternates with the variable's parity so the
-// 2-vector stays aligned).
+// Per-cell gradient record: (gx, gy, gz, psi) for each of the 5 variables, 20 values per cell,
+// read and written as two 2-vectors per variable (16-byte accesses in FP64). (A compact 16-value
+// layout for folded records, one cache line per cell, was measured slower: the per-variable
+// writers leave partially written sectors.)
 template <typename R>
 struct Vec2;
 template <>
@@ -124,49 +122,19 @@ struct Vec2<float> {
     using T = float2;
 };
 
-template <bool FOLD, typename R>
+template <typename R>
 __device__ __forceinline__ void grad_rec_store(R *rec, int c, int v, R gx, R gy, R gz, R psi)
 {
     using T2 = typename Vec2<R>::T;
-    if (FOLD) {
-        R *p = rec + (size_t)c * 16 + 3 * v;
-        if (v & 1) {
-            p[0] = gx;
-            *reinterpret_cast<T2 *>(p + 1) = T2{gy, gz};
-        }
-        else if (v == 4) {  // the last variable also writes the pad: whole lines, no partial sectors
-            *reinterpret_cast<T2 *>(p) = T2{gx, gy};
-            *reinterpret_cast<T2 *>(p + 2) = T2{gz, R(0)};
-        }
-        else {
-            *reinterpret_cast<T2 *>(p) = T2{gx, gy};
-            p[2] = gz;
-        }
-        return;
-    }
     T2 *p = reinterpret_cast<T2 *>(rec + ((size_t)c * 5 + v) * 4);
     p[0] = T2{gx, gy};
     p[1] = T2{gz, psi};
 }
 
-// psi is 1 for folded records
-template <bool FOLD, typename R>
+template <typename R>
 __device__ __forceinline__ void grad_rec_load(const R *rec, int c, int v, R &gx, R &gy, R &gz, R &psi)
 {
     using T2 = typename Vec2<R>::T;
-    if (FOLD) {
-        const R *p = rec + (size_t)c * 16 + 3 * v;
-        if (v & 1) {
-            T2 b = __ldg(reinterpret_cast<const T2 *>(p + 1));
-            gx = __ldg(p), gy = b.x, gz = b.y;
-        }
-        else {
-            T2 a = __ldg(reinterpret_cast<const T2 *>(p));
-            gx = a.x, gy = a.y, gz = __ldg(p + 2);
-        }
-        psi = R(1);
-        return;
-    }
     const T2 *p = reinterpret_cast<const T2 *>(rec + ((size_t)c * 5 + v) * 4);
     T2 a = __ldg(p), b = __ldg(p + 1);
     gx = a.x, gy = a.y, gz = b.x, psi = b.y;

@@ -1304,16 +1304,16 @@ extern "C" int tg_gradient(tg_ctx *c, double time, int limited, double *gradient
     TRY(run_boundary(c, c->q));
     int lim = limited ? c->limiter : TG_LIMITER_NONE;
     TRY(run_gradient(c, c->q, lim));
-    // the record layout the gradient pass used (folded: compact, psi multiplied in); an unfolded
-    // record gets psi multiplied in here
-    const int compact = (lim == TG_LIMITER_NONE || c->viscous != TG_VISCOUS_CENTRAL) ? 1 : 0;
-    int limit = (limited && lim != TG_LIMITER_NONE && !compact) ? 1 : 0;
+    // a folded record already carries psi (or none was applied); an unfolded one gets it
+    // multiplied in here
+    const bool folded = lim == TG_LIMITER_NONE || c->viscous != TG_VISCOUS_CENTRAL;
+    int limit = (limited && lim != TG_LIMITER_NONE && !folded) ? 1 : 0;
     if (c->precision == TG_PRECISION_FP64)
         k_grad_to_aos<double><<<grid_of(c->s.C), BLOCK, 0, c->stream>>>(c->s.C, (const double *)c->grad, limit,
-                                                                        compact, c->aos);
+                                                                        c->aos);
     else
         k_grad_to_aos<float><<<grid_of(c->s.C), BLOCK, 0, c->stream>>>(c->s.C, (const float *)c->grad, limit,
-                                                                       compact, c->aos);
+                                                                       c->aos);
     CU(cudaGetLastError());
     TRY(d2h(c, gradient, c->aos, 15 * (size_t)c->s.C));
     return TG_OK;

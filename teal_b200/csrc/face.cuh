@@ -22,7 +22,7 @@ __device__ __forceinline__ void reconstruct(const Prim<R> &q, const R *__restric
 #pragma unroll
     for (int v = 0; v < 5; v++) {
         R gx, gy, gz, ps;
-        grad_rec_load<FOLD>(rec, c, v, gx, gy, gz, ps);
+        grad_rec_load(rec, c, v, gx, gy, gz, ps);
         V3<R> gv = v3(gx, gy, gz);
         if (!FOLD) {
             gv = v3(gv.x * ps, gv.y * ps, gv.z * ps);
@@ -184,12 +184,12 @@ __device__ __forceinline__ void face_flux(const Geo &geo, int i, int f, const Si
 #pragma unroll
         for (int v = 0; v < 5; v++) {
             R ax, ay, az, ap, bx, by, bz, bp;
-            grad_rec_load<FOLD>(rec, c.x, v, ax, ay, az, ap);
+            grad_rec_load(rec, c.x, v, ax, ay, az, ap);
             if (boundary) {
                 gm[3 * v] = ax, gm[3 * v + 1] = ay, gm[3 * v + 2] = az;
             }
             else {
-                grad_rec_load<FOLD>(rec, c.y, v, bx, by, bz, bp);
+                grad_rec_load(rec, c.y, v, bx, by, bz, bp);
                 gm[3 * v] = (ax + bx) / R(2), gm[3 * v + 1] = (ay + by) / R(2), gm[3 * v + 2] = (az + bz) / R(2);
             }
         }

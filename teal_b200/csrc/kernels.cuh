@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_gradient(Sizes s, Geometry<R> 
         gy *= psi;
         gz *= psi;
     }
-    grad_rec_store<FOLD>(rec, c, v, gx, gy, gz, psi);
+    grad_rec_store(rec, c, v, gx, gy, gz, psi);
 }
 
 // per-cell time step of the equations' Timestep plugin
@@ -688,7 +688,7 @@ __global__ void k_aos5_to_soa(int C, const double *__restrict__ aos, double *__r
 
 // gradient records -> teal's [C][5][3] (limited when `limit` and the record is not folded)
 template <typename R>
-__global__ void k_grad_to_aos(int C, const R *__restrict__ rec, int limit, int compact, double *__restrict__ aos)
+__global__ void k_grad_to_aos(int C, const R *__restrict__ rec, int limit, double *__restrict__ aos)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= C) {
@@ -696,10 +696,7 @@ __global__ void k_grad_to_aos(int C, const R *__restrict__ rec, int limit, int c
     }
     for (int v = 0; v < 5; v++) {
         R gx, gy, gz, psi;
-        if (compact)
-            grad_rec_load<true>(rec, i, v, gx, gy, gz, psi);
-        else
-            grad_rec_load<false>(rec, i, v, gx, gy, gz, psi);
+        grad_rec_load(rec, i, v, gx, gy, gz, psi);
         if (limit) {
             gx *= psi, gy *= psi, gz *= psi;
         }
