@@ -1,14 +1,14 @@
 // Launch shapes of the hot kernels, chosen by teal_b200/autotune.py on a B200 (fastest measured
-// RK step, TGV 96^3 FP64 for the shapes and the Navier-Stokes staging switch, the 64^3 ramp for the
-// Euler staging switch; times within 0.5 % of the fastest count as ties, resolved to fewer
-// resident face blocks, i.e. more registers per thread); a value given with -D at build time wins.
+// RK step, TGV for the shapes and the Navier-Stokes staging switch, the ramp for the Euler
+// staging switch; times within 0.5 % of the fastest count as ties, resolved to fewer resident
+// face blocks, i.e. more registers per thread); a value given with -D at build time wins.
 #pragma once
 
 #ifndef TG_FACE_BLOCK
-#define TG_FACE_BLOCK 128  // threads per face-flux block
+#define TG_FACE_BLOCK 32  // threads per face-flux block
 #endif
 #ifndef TG_FACE_MINB
-#define TG_FACE_MINB 4  // face-flux blocks kept resident per SM (caps registers per thread)
+#define TG_FACE_MINB 20  // face-flux blocks kept resident per SM (caps registers per thread)
 #endif
 #ifndef TG_CELL_BLOCK
 #define TG_CELL_BLOCK 256  // threads per cell-gather block
