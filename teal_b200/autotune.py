@@ -34,6 +34,8 @@ FACE_BLOCKS = [32, 64, 128]
 FACE_THREADS = [512, 640, 768]
 STAGED = [0, 1]
 CELL_BLOCKS = [256]
+# then cell-gather block size x blocks resident per SM (1536 threads -> 42 registers per thread)
+CELL_SHAPES = [(256, 1), (128, 8), (128, 12), (64, 24)]
 
 TIMER = r"""
 import json, math, sys, time
@@ -109,6 +111,7 @@ def write_header(path, best):
     notes = {"TG_FACE_BLOCK": "threads per face-flux block",
              "TG_FACE_MINB": "face-flux blocks kept resident per SM (caps registers per thread)",
              "TG_CELL_BLOCK": "threads per cell-gather block",
+             "TG_CELL_MINB": "cell-gather blocks kept resident per SM (caps registers per thread)",
              "TG_FACE_STAGED_NS": "Navier-Stokes face kernel: geometry staged by bulk copies (1) or loaded (0)",
              "TG_FACE_STAGED_EULER": "Euler face kernel: geometry staged by bulk copies (1) or loaded (0)"}
     for k, v in best.items():
@@ -152,6 +155,8 @@ def main():
     with tempfile.TemporaryDirectory() as work:
         per = max(2, args.jobs // 4)
         ms, best = sweep(variants, "tgv", args.n, work, per)
+        cells = [dict(best, TG_CELL_BLOCK=cb, TG_CELL_MINB=cm) for cb, cm in CELL_SHAPES]
+        ms, best = sweep(cells, "tgv", args.n, work, per)
         euler = [dict(best, TG_FACE_STAGED_EULER=st) for st in STAGED]
         ms_e, best = sweep(euler, "ramp", args.ramp_n, work, per)
     write_header(os.path.join(CSRC, "tuned.h"), best)

@@ -16,6 +16,7 @@ constexpr int BLOCK = 256;
 constexpr int FACE_BLOCK = TG_FACE_BLOCK;
 constexpr int FACE_MINB = TG_FACE_MINB;
 constexpr int CELL_BLOCK = TG_CELL_BLOCK;
+constexpr int CELL_MINB = TG_CELL_MINB;
 constexpr int REDUCE_BLOCK = 1024;
 
 // ---- small helpers ---------------------------------------------------------------------------

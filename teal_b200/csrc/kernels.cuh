@@ -259,7 +259,7 @@ __global__ void k_inst_average(Segments seg, const double *__restrict__ part, do
 }
 
 template <int MODE, bool NS, typename GT, int SRC>
-__global__ void __launch_bounds__(CELL_BLOCK) k_cell(Sizes s, const int *__restrict__ slot_face,
+__global__ void __launch_bounds__(CELL_BLOCK, CELL_MINB) k_cell(Sizes s, const int *__restrict__ slot_face,
                                                 const uint8_t *__restrict__ slot_cnt, CellData cd,
                                                 const GT *__restrict__ G, double *__restrict__ U0,
                                                 double *__restrict__ q, double *__restrict__ Rout,

@@ -1,6 +1,6 @@
 // Launch shapes of the hot kernels, chosen by teal_b200/autotune.py on a B200 (fastest measured
-// RK step, TGV for the shapes and the Navier-Stokes staging switch, the ramp for the Euler
-// staging switch; times within 0.5 % of the fastest count as ties, resolved to fewer resident
+// RK step, TGV for the face and cell shapes and the Navier-Stokes staging switch, the ramp for the
+// Euler staging switch; cell shape from its sweep: 0.113 vs 0.133 ms per TGV 128^3 launch; times within 0.5 % of the fastest count as ties, resolved to fewer resident
 // face blocks, i.e. more registers per thread); a value given with -D at build time wins.
 #pragma once
 
@@ -11,11 +11,14 @@
 #define TG_FACE_MINB 20  // face-flux blocks kept resident per SM (caps registers per thread)
 #endif
 #ifndef TG_CELL_BLOCK
-#define TG_CELL_BLOCK 256  // threads per cell-gather block
+#define TG_CELL_BLOCK 128  // threads per cell-gather block
 #endif
 #ifndef TG_FACE_STAGED_NS
 #define TG_FACE_STAGED_NS 0  // Navier-Stokes face kernel: geometry staged by bulk copies (1) or loaded (0)
 #endif
 #ifndef TG_FACE_STAGED_EULER
 #define TG_FACE_STAGED_EULER 1  // Euler face kernel: geometry staged by bulk copies (1) or loaded (0)
+#endif
+#ifndef TG_CELL_MINB
+#define TG_CELL_MINB 12  // cell-gather blocks kept resident per SM (caps registers per thread)
 #endif
