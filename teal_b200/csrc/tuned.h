@@ -1,7 +1,8 @@
-// Launch shapes of the hot kernels, chosen by teal_b200/autotune.py on a B200 (fastest measured
-// RK step, TGV for the face and cell shapes and the Navier-Stokes staging switch, the ramp for the
-// Euler staging switch; cell shape from its sweep: 0.113 vs 0.133 ms per TGV 128^3 launch; times within 0.5 % of the fastest count as ties, resolved to fewer resident
-// face blocks, i.e. more registers per thread); a value given with -D at build time wins.
+// Launch shapes of the hot kernels, chosen by teal_b200/autotune.py on a B200 (fastest measured RK
+// step: TGV for the face and cell shapes and the Navier-Stokes staging switch, the ramp for the
+// Euler staging switch; times within 0.5 % of the fastest count as ties, resolved to fewer resident
+// face blocks, i.e. more registers per thread). The cell shape comes from its sweep (0.113 vs
+// 0.133 ms per TGV 128^3 launch). A value given with -D at build time wins.
 #pragma once
 
 #ifndef TG_FACE_BLOCK
