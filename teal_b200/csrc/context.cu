@@ -663,8 +663,8 @@ static int alloc_geom32(tg_ctx *c)
     TRY(dalloc(&c->gb.offl32, 3 * (size_t)s.F));
     TRY(dalloc(&c->gb.offr32, 3 * (size_t)s.F));
     if (c->gb.corr) TRY(dalloc(&c->gb.corr32, 4 * (size_t)s.F));
-    TRY(dalloc(&c->gb.slot_w32, 3 * MAX_SLOTS * (size_t)s.C));
-    TRY(dalloc(&c->gb.slot_off32, 3 * MAX_SLOTS * (size_t)s.C));
+    TRY(dalloc(&c->gb.slot_w32, 3 * MAX_SLOTS * (size_t)s.SL));
+    TRY(dalloc(&c->gb.slot_off32, 3 * MAX_SLOTS * (size_t)s.SL));
     return TG_OK;
 }
 
@@ -717,6 +717,7 @@ static int create_ctx(MeshInput &in, const tg_equations *e, int precision, tg_ct
         s.F = m->num_faces;
         s.F_in = m->num_inner_faces;
         s.F_bd = m->off_boundary_faces;
+        s.SL = (s.C + 3) & ~3;
         c->num_periodic = m->num_cells - m->off_boundary_cells;
         c->physics = e->physics;
         c->order = e->space_order;
@@ -773,16 +774,21 @@ static int create_ctx(MeshInput &in, const tg_equations *e, int precision, tg_ct
             // per-cell slot lists: count, scatter, sort by face (integer work on the device)
             TRY(dalloc(&d_cnt, 2 * (size_t)s.C));
             CU(cudaMemsetAsync(d_cnt, 0, 2 * sizeof(int) * s.C, st));
-            TRY(dalloc(&c->slot_face, MAX_SLOTS * (size_t)s.C));
-            TRY(dalloc(&c->slot_nbr, MAX_SLOTS * (size_t)s.C));
+            // slot rows are SL = C rounded up to 4 long (16-byte rows); the padding columns stay zero
+            TRY(dalloc(&c->slot_face, MAX_SLOTS * (size_t)s.SL));
+            TRY(dalloc(&c->slot_nbr, MAX_SLOTS * (size_t)s.SL));
             TRY(dalloc(&c->slot_cnt, s.C));
-            TRY(dalloc(&c->gb.slot_w, 3 * MAX_SLOTS * (size_t)s.C));
-            TRY(dalloc(&c->gb.slot_off, 3 * MAX_SLOTS * (size_t)s.C));
+            TRY(dalloc(&c->gb.slot_w, 3 * MAX_SLOTS * (size_t)s.SL));
+            TRY(dalloc(&c->gb.slot_off, 3 * MAX_SLOTS * (size_t)s.SL));
+            CU(cudaMemsetAsync(c->slot_face, 0, MAX_SLOTS * sizeof(int) * (size_t)s.SL, st));
+            CU(cudaMemsetAsync(c->slot_nbr, 0, MAX_SLOTS * sizeof(int) * (size_t)s.SL, st));
+            CU(cudaMemsetAsync(c->gb.slot_w, 0, 3 * MAX_SLOTS * sizeof(double) * (size_t)s.SL, st));
+            CU(cudaMemsetAsync(c->gb.slot_off, 0, 3 * MAX_SLOTS * sizeof(double) * (size_t)s.SL, st));
             k_slot_count<<<grid_of(s.F), BLOCK, 0, st>>>(s.F, s.F_in, c->lr, d_cnt);
-            k_slot_fill<<<grid_of(s.F), BLOCK, 0, st>>>(s.F, s.F_in, s.C, c->lr, d_cnt + s.C, c->slot_face);
+            k_slot_fill<<<grid_of(s.F), BLOCK, 0, st>>>(s.F, s.F_in, s.SL, c->lr, d_cnt + s.C, c->slot_face);
             TRY(upload(&d_weight, m->face_weight, 6 * (size_t)s.F, st));
             TRY(upload(&d_offset, m->face_offset, 6 * (size_t)s.F, st));
-            k_slot_finish<double><<<grid_of(s.C), BLOCK, 0, st>>>(s.C, c->lr, d_cnt, d_weight, d_offset,
+            k_slot_finish<double><<<grid_of(s.C), BLOCK, 0, st>>>(s.C, s.SL, c->lr, d_cnt, d_weight, d_offset,
                                                                   c->slot_face, c->slot_nbr, c->slot_cnt,
                                                                   c->gb.slot_w, c->gb.slot_off, d_err);
             CU(cudaGetLastError());
@@ -842,8 +848,8 @@ static int create_ctx(MeshInput &in, const tg_equations *e, int precision, tg_ct
             TRY(to_float(c->gb.offl, c->gb.offl32, 3 * (size_t)s.F, st));
             TRY(to_float(c->gb.offr, c->gb.offr32, 3 * (size_t)s.F, st));
             TRY(to_float(c->gb.corr, c->gb.corr32, 4 * (size_t)s.F, st));
-            TRY(to_float(c->gb.slot_w, c->gb.slot_w32, 3 * MAX_SLOTS * (size_t)s.C, st));
-            TRY(to_float(c->gb.slot_off, c->gb.slot_off32, 3 * MAX_SLOTS * (size_t)s.C, st));
+            TRY(to_float(c->gb.slot_w, c->gb.slot_w32, 3 * MAX_SLOTS * (size_t)s.SL, st));
+            TRY(to_float(c->gb.slot_off, c->gb.slot_off32, 3 * MAX_SLOTS * (size_t)s.SL, st));
         }
         c->g64 = Geometry<double>{c->lr,       c->gb.area,  c->gb.basis,   c->gb.offl,   c->gb.offr,   c->gb.corr,
                                   c->slot_nbr, c->slot_face, c->slot_cnt, c->gb.slot_w, c->gb.slot_off};
@@ -1871,16 +1877,16 @@ extern "C" int tg_layout(tg_ctx *c, const char *name, void *out, long count)
 {
     if (!c || !name || !out) return fail(TG_ERR_INVALID, "null argument");
     const void *src = nullptr;
-    size_t bytes = 0;
+    size_t bytes = 0, pitch = 0;  // pitch: row length of a pitched [6][SL] slot array
     long expect = 0;
     if (!strcmp(name, "face_lr")) {
         src = c->lr, expect = 2L * c->s.F, bytes = sizeof(int);
     }
     else if (!strcmp(name, "slot_face")) {
-        src = c->slot_face, expect = (long)MAX_SLOTS * c->s.C, bytes = sizeof(int);
+        src = c->slot_face, expect = (long)MAX_SLOTS * c->s.C, bytes = sizeof(int), pitch = c->s.SL;
     }
     else if (!strcmp(name, "slot_nbr")) {
-        src = c->slot_nbr, expect = (long)MAX_SLOTS * c->s.C, bytes = sizeof(int);
+        src = c->slot_nbr, expect = (long)MAX_SLOTS * c->s.C, bytes = sizeof(int), pitch = c->s.SL;
     }
     else if (!strcmp(name, "slot_cnt")) {
         src = c->slot_cnt, expect = c->s.C, bytes = 1;
@@ -1893,7 +1899,14 @@ extern "C" int tg_layout(tg_ctx *c, const char *name, void *out, long count)
     }
     if (count != expect) return fail(TG_ERR_INVALID, "layout array %s has %ld elements, not %ld", name, expect, count);
     if (count == 0) return TG_OK;
-    CU(cudaMemcpyAsync(out, src, bytes * count, cudaMemcpyDeviceToHost, c->stream));
+    if (pitch) {
+        // returned unpitched, [6][C]
+        CU(cudaMemcpy2DAsync(out, bytes * c->s.C, src, bytes * pitch, bytes * c->s.C, MAX_SLOTS,
+                             cudaMemcpyDeviceToHost, c->stream));
+    }
+    else {
+        CU(cudaMemcpyAsync(out, src, bytes * count, cudaMemcpyDeviceToHost, c->stream));
+    }
     CU(cudaStreamSynchronize(c->stream));
     return TG_OK;
 }

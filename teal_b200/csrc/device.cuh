@@ -43,6 +43,7 @@ struct CellData {
 
 struct Sizes {
     int C, N, F, F_in, F_bd;
+    int SL;  // leading dimension of the per-cell slot arrays: C rounded up to 4 (16-byte rows)
 };
 
 // Instances packed in one arena (a single mesh is one instance). Inner cells of instance i are

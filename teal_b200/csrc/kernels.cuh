@@ -52,32 +52,60 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_gradient(Sizes s, Geometry<R> 
                                                            const double *__restrict__ q,
                                                            R *__restrict__ rec)
 {
-    __shared__ int s_nbr[MAX_SLOTS][GRAD_CELLS];
+    __shared__ __align__(16) int s_nbr[MAX_SLOTS][GRAD_CELLS];
     __shared__ int s_cnt[GRAD_CELLS];
-    __shared__ R s_w[3 * MAX_SLOTS][GRAD_CELLS];
-    __shared__ R s_off[(LIM != 0) ? 3 * MAX_SLOTS : 1][GRAD_CELLS];
+    __shared__ __align__(16) R s_w[3 * MAX_SLOTS][GRAD_CELLS];
+    __shared__ __align__(16) R s_off[(LIM != 0) ? 3 * MAX_SLOTS : 1][GRAD_CELLS];
     const int C = s.C;
     const int base = blockIdx.x * GRAD_CELLS;
     const int ncell = min(GRAD_CELLS, C - base);
-    // SKIP (meshes with cells of fewer than MAX_SLOTS faces): padding slots are not loaded, each
-    // staging thread reading its cell's face count; nothing reads them
-    for (int i = threadIdx.x; i < MAX_SLOTS * GRAD_CELLS; i += GRAD_THREADS) {
-        int j = i / GRAD_CELLS, l = i % GRAD_CELLS;
-        if (l < ncell && (!SKIP || j < int(__ldg(g.slot_cnt + base + l)))) {
-            s_nbr[j][l] = __ldg(g.slot_nbr + (size_t)j * C + base + l);
+    const int SL = s.SL;
+    if (!SKIP) {
+        // every slot row of the block's 32 cells is 16-byte aligned and contiguous (SL is a multiple
+        // of 4 and base of 32): copy the 6 + 18 + 18 rows with 16-byte vector loads
+        constexpr int NV = GRAD_CELLS * int(sizeof(int)) / 16;  // vectors per neighbour row
+        constexpr int RV = GRAD_CELLS * int(sizeof(R)) / 16;    // vectors per weight / offset row
+        const int live = min(GRAD_CELLS, SL - base);            // cells of the rows inside the arrays
+        for (int i = threadIdx.x; i < MAX_SLOTS * NV; i += GRAD_THREADS) {
+            const int j = i / NV, k = i % NV;
+            if (k * 16 < live * int(sizeof(int))) {
+                reinterpret_cast<uint4 *>(&s_nbr[j][0])[k] =
+                    __ldg(reinterpret_cast<const uint4 *>(g.slot_nbr + (size_t)j * SL + base) + k);
+            }
+        }
+        for (int i = threadIdx.x; i < 3 * MAX_SLOTS * RV; i += GRAD_THREADS) {
+            const int j = i / RV, k = i % RV;
+            if (k * 16 < live * int(sizeof(R))) {
+                reinterpret_cast<uint4 *>(&s_w[j][0])[k] =
+                    __ldg(reinterpret_cast<const uint4 *>(g.slot_w + (size_t)j * SL + base) + k);
+                if (LIM != 0) {
+                    reinterpret_cast<uint4 *>(&s_off[j][0])[k] =
+                        __ldg(reinterpret_cast<const uint4 *>(g.slot_off + (size_t)j * SL + base) + k);
+                }
+            }
+        }
+    }
+    else {
+        // meshes with cells of fewer than MAX_SLOTS faces: padding slots are not loaded, each
+        // staging thread reading its cell's face count; nothing reads them
+        for (int i = threadIdx.x; i < MAX_SLOTS * GRAD_CELLS; i += GRAD_THREADS) {
+            int j = i / GRAD_CELLS, l = i % GRAD_CELLS;
+            if (l < ncell && j < int(__ldg(g.slot_cnt + base + l))) {
+                s_nbr[j][l] = __ldg(g.slot_nbr + (size_t)j * SL + base + l);
+            }
+        }
+        for (int i = threadIdx.x; i < 3 * MAX_SLOTS * GRAD_CELLS; i += GRAD_THREADS) {
+            int k = i / GRAD_CELLS, l = i % GRAD_CELLS;
+            if (l < ncell && (k % MAX_SLOTS) < int(__ldg(g.slot_cnt + base + l))) {
+                s_w[k][l] = __ldg(g.slot_w + (size_t)k * SL + base + l);
+                if (LIM != 0) {
+                    s_off[k][l] = __ldg(g.slot_off + (size_t)k * SL + base + l);
+                }
+            }
         }
     }
     if (threadIdx.x < GRAD_CELLS) {
         s_cnt[threadIdx.x] = (threadIdx.x < ncell) ? int(g.slot_cnt[base + threadIdx.x]) : 0;
-    }
-    for (int i = threadIdx.x; i < 3 * MAX_SLOTS * GRAD_CELLS; i += GRAD_THREADS) {
-        int k = i / GRAD_CELLS, l = i % GRAD_CELLS;
-        if (l < ncell && (!SKIP || (k % MAX_SLOTS) < int(__ldg(g.slot_cnt + base + l)))) {
-            s_w[k][l] = __ldg(g.slot_w + (size_t)k * C + base + l);
-            if (LIM != 0) {
-                s_off[k][l] = __ldg(g.slot_off + (size_t)k * C + base + l);
-            }
-        }
     }
     __syncthreads();
 
@@ -279,7 +307,7 @@ __global__ void __launch_bounds__(CELL_BLOCK, CELL_MINB) k_cell(Sizes s, const i
         int sf[MAX_SLOTS];
 #pragma unroll
         for (int j = 0; j < MAX_SLOTS; j++) {
-            sf[j] = (j < cnt) ? __ldg(slot_face + j * C + c) : 0;
+            sf[j] = (j < cnt) ? __ldg(slot_face + j * s.SL + c) : 0;
         }
         double gv[MAX_SLOTS][5];
 #pragma unroll
@@ -518,7 +546,7 @@ __global__ void k_slot_count(int F, int F_in, const int2 *__restrict__ lr, int *
 }
 
 // scatter face references into the ELL slots (arbitrary order; sorted afterwards)
-__global__ void k_slot_fill(int F, int F_in, int C, const int2 *__restrict__ lr, int *__restrict__ cursor,
+__global__ void k_slot_fill(int F, int F_in, int SL, const int2 *__restrict__ lr, int *__restrict__ cursor,
                             int *__restrict__ slot_face)
 {
     int f = blockIdx.x * blockDim.x + threadIdx.x;
@@ -528,12 +556,12 @@ __global__ void k_slot_fill(int F, int F_in, int C, const int2 *__restrict__ lr,
     int2 c = lr[f];
     int j = atomicAdd(cursor + c.x, 1);
     if (j < MAX_SLOTS) {
-        slot_face[j * C + c.x] = f;
+        slot_face[j * SL + c.x] = f;
     }
     if (f < F_in) {
         int k = atomicAdd(cursor + c.y, 1);
         if (k < MAX_SLOTS) {
-            slot_face[k * C + c.y] = ~f;
+            slot_face[k * SL + c.y] = ~f;
         }
     }
 }
@@ -545,7 +573,7 @@ __device__ __forceinline__ int face_of(int sf)
 
 // sort each cell's slots by face index, then fill neighbour, weight and offset of each slot
 template <typename G>
-__global__ void k_slot_finish(int C, const int2 *__restrict__ lr, const int *__restrict__ cnt_in,
+__global__ void k_slot_finish(int C, int SL, const int2 *__restrict__ lr, const int *__restrict__ cnt_in,
                               const double *__restrict__ weight_aos, const double *__restrict__ offset_aos,
                               int *__restrict__ slot_face, int *__restrict__ slot_nbr,
                               uint8_t *__restrict__ slot_cnt, G *__restrict__ slot_w,
@@ -562,7 +590,7 @@ __global__ void k_slot_finish(int C, const int2 *__restrict__ lr, const int *__r
     }
     int sf[MAX_SLOTS];
     for (int j = 0; j < cnt; j++) {
-        sf[j] = slot_face[j * C + c];
+        sf[j] = slot_face[j * SL + c];
     }
     for (int i = 1; i < cnt; i++) {  // insertion sort by face index
         int key = sf[i];
@@ -579,19 +607,19 @@ __global__ void k_slot_finish(int C, const int2 *__restrict__ lr, const int *__r
             int f = face_of(sf[j]);
             int side = sf[j] >= 0 ? 0 : 1;
             int2 p = lr[f];
-            slot_face[j * C + c] = sf[j];
-            slot_nbr[j * C + c] = side == 0 ? p.y : p.x;
+            slot_face[j * SL + c] = sf[j];
+            slot_nbr[j * SL + c] = side == 0 ? p.y : p.x;
             for (int d = 0; d < 3; d++) {
-                slot_w[(d * MAX_SLOTS + j) * C + c] = G(weight_aos[(size_t)f * 6 + side * 3 + d]);
-                slot_off[(d * MAX_SLOTS + j) * C + c] = G(offset_aos[(size_t)f * 6 + side * 3 + d]);
+                slot_w[(size_t)(d * MAX_SLOTS + j) * SL + c] = G(weight_aos[(size_t)f * 6 + side * 3 + d]);
+                slot_off[(size_t)(d * MAX_SLOTS + j) * SL + c] = G(offset_aos[(size_t)f * 6 + side * 3 + d]);
             }
         }
         else {  // padding: a self-reference with zero weight and offset
-            slot_face[j * C + c] = 0;
-            slot_nbr[j * C + c] = c;
+            slot_face[j * SL + c] = 0;
+            slot_nbr[j * SL + c] = c;
             for (int d = 0; d < 3; d++) {
-                slot_w[(d * MAX_SLOTS + j) * C + c] = G(0);
-                slot_off[(d * MAX_SLOTS + j) * C + c] = G(0);
+                slot_w[(size_t)(d * MAX_SLOTS + j) * SL + c] = G(0);
+                slot_off[(size_t)(d * MAX_SLOTS + j) * SL + c] = G(0);
             }
         }
     }
