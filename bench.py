@@ -36,11 +36,18 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "cell-updates/s"
-WORKLOAD = "taylor-green vortex 128^3 periodic hex, navier-stokes, roe + ls gradient + venkatakrishnan(1), lserk{3,3}, cfl 0.99"
-RAMP_WORKLOAD = ("compression ramp 80^3 jittered hex grid split into tetrahedra / prisms / hexahedra / pyramid "
+WORKLOAD = "taylor-green vortex {n}^3 periodic hex, navier-stokes, roe + ls gradient + venkatakrishnan(1), lserk{{3,3}}, cfl 0.99"
+RAMP_WORKLOAD = ("compression ramp {n}^3 jittered hex grid split into tetrahedra / prisms / hexahedra / pyramid "
                  "transitions, 15 deg ramp, Mach 2.5, euler, ausmd + ls gradient + barth-jespersen, "
-                 "supersonic inflow / outflow + slip walls, lserk{3,3}, cfl 0.99")
+                 "supersonic inflow / outflow + slip walls, lserk{{3,3}}, cfl 0.99")
 M25 = (1.0, 2.5, 0.0, 0.0, 1.0 / 1.4)
+
+
+def workload_name(workload, n):
+    """Description of the tgv / ramp workload at n cells per axis (None: the default size)."""
+    if workload == "tgv":
+        return WORKLOAD.format(n=n or 128)
+    return RAMP_WORKLOAD.format(n=n or 80)
 RAMP_BCS = {"left": ("supersonic inflow", M25), "right": ("supersonic outflow", None),
             "bottom": ("slipwall", None), "top": ("slipwall", None), "back": ("slipwall", None),
             "front": ("slipwall", None)}
@@ -482,7 +489,7 @@ def run_reference_arm(args, world, rank):
         "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000 * secs / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD if args.workload == "tgv" else RAMP_WORKLOAD,
+        "config": {"workload": workload_name(args.workload, None),
                    "sample_mesh": f"{n_sample}^3 per core", "parallelism": f"{procs} cores"},
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": procs, "kind": "reference",
@@ -653,7 +660,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32-flux/f64-accumulate",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD if ns else RAMP_WORKLOAD, "cells": C, "faces": F, "mesh": f"{n}^3",
+        "config": {"workload": workload_name("tgv" if ns else "ramp", n), "cells": C, "faces": F, "mesh": f"{n}^3",
                    "global_batch": world, "parallelism": f"replicas x{world}" if world > 1 else "1 gpu",
                    "l2": f"inputs larger than L2 (state + geometry ~{b_stage / 1e9:.1f} GB per stage)"},
         "roofline": {"bound": "hbm", "kernel": "rk stage (boundary+gradient+face+cell)", "achieved": achieved,

@@ -36,6 +36,8 @@ STAGED = [0, 1]
 CELL_BLOCKS = [256]
 # then cell-gather block size x blocks resident per SM (1536 threads -> 42 registers per thread)
 CELL_SHAPES = [(256, 1), (128, 8), (128, 12), (64, 24)]
+# then gradient blocks (160 threads) resident per SM: 9 leaves the registers free, 12 caps them at 32
+GRAD_MINB = [9, 12]
 
 TIMER = r"""
 import json, math, sys, time
@@ -104,16 +106,18 @@ def time_variant(lib, n, steps, precision, workload="tgv"):
 
 def write_header(path, best):
     lines = ["// Launch shapes of the hot kernels, chosen by teal_b200/autotune.py on a B200 (fastest measured",
-             "// RK step, TGV for the shapes and the Navier-Stokes staging switch, the ramp for the Euler",
-             "// staging switch; times within 0.5 % of the fastest count as ties, resolved to fewer resident",
-             "// face blocks, i.e. more registers per thread); a value given with -D at build time wins.",
+             "// RK step: TGV for the face, cell and gradient shapes and the Navier-Stokes staging switch, the",
+             "// ramp for the Euler staging switch; times within 0.5 % of the fastest count as ties, resolved to",
+             "// fewer resident face blocks, i.e. more registers per thread). A value given with -D at build",
+             "// time wins.",
              "#pragma once", ""]
     notes = {"TG_FACE_BLOCK": "threads per face-flux block",
              "TG_FACE_MINB": "face-flux blocks kept resident per SM (caps registers per thread)",
              "TG_CELL_BLOCK": "threads per cell-gather block",
              "TG_CELL_MINB": "cell-gather blocks kept resident per SM (caps registers per thread)",
              "TG_FACE_STAGED_NS": "Navier-Stokes face kernel: geometry staged by bulk copies (1) or loaded (0)",
-             "TG_FACE_STAGED_EULER": "Euler face kernel: geometry staged by bulk copies (1) or loaded (0)"}
+             "TG_FACE_STAGED_EULER": "Euler face kernel: geometry staged by bulk copies (1) or loaded (0)",
+             "TG_GRAD_MINB": "gradient blocks (160 threads) kept resident per SM (caps registers per thread)"}
     for k, v in best.items():
         lines += [f"#ifndef {k}", f"#define {k} {v}  // {notes[k]}", "#endif"]
     with open(path, "w") as f:
@@ -157,6 +161,8 @@ def main():
         ms, best = sweep(variants, "tgv", args.n, work, per)
         cells = [dict(best, TG_CELL_BLOCK=cb, TG_CELL_MINB=cm) for cb, cm in CELL_SHAPES]
         ms, best = sweep(cells, "tgv", args.n, work, per)
+        grads = [dict(best, TG_GRAD_MINB=gm) for gm in GRAD_MINB]
+        ms, best = sweep(grads, "tgv", args.n, work, per)
         euler = [dict(best, TG_FACE_STAGED_EULER=st) for st in STAGED]
         ms_e, best = sweep(euler, "ramp", args.ramp_n, work, per)
     write_header(os.path.join(CSRC, "tuned.h"), best)

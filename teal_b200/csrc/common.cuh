@@ -17,6 +17,7 @@ constexpr int FACE_BLOCK = TG_FACE_BLOCK;
 constexpr int FACE_MINB = TG_FACE_MINB;
 constexpr int CELL_BLOCK = TG_CELL_BLOCK;
 constexpr int CELL_MINB = TG_CELL_MINB;
+constexpr int GRAD_MINB = TG_GRAD_MINB;
 constexpr int REDUCE_BLOCK = 1024;
 
 // ---- small helpers ---------------------------------------------------------------------------

@@ -47,7 +47,7 @@ constexpr int GRAD_CELLS = 32;
 constexpr int GRAD_THREADS = 5 * GRAD_CELLS;
 
 template <typename R, int LIM, bool FOLD, bool SKIP>
-__global__ void __launch_bounds__(GRAD_THREADS) k_gradient(Sizes s, Geometry<R> g,
+__global__ void __launch_bounds__(GRAD_THREADS, GRAD_MINB) k_gradient(Sizes s, Geometry<R> g,
                                                            const double *__restrict__ eps2,
                                                            const double *__restrict__ q,
                                                            R *__restrict__ rec)
@@ -117,7 +117,8 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_gradient(Sizes s, Geometry<R> 
     const int c = base + l;
     const double *qv = q + (size_t)v * s.N;
     const double qc = __ldg(qv + c);
-    const int cnt = s_cnt[l];
+    // without SKIP every cell has MAX_SLOTS slots: the slot tests below fold away
+    const int cnt = SKIP ? s_cnt[l] : MAX_SLOTS;
     double qn[MAX_SLOTS];
 #pragma unroll
     for (int j = 0; j < MAX_SLOTS; j++) {
@@ -137,14 +138,19 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_gradient(Sizes s, Geometry<R> 
         }
     }
 
-    // limiter factor: the minimum over the cell's faces of teal's candidate ratios. In FP64 the
-    // running minimum is kept as a fraction (numerator, positive denominator), compared by cross
-    // multiplication, and divided once: one division per thread instead of one or two per face,
-    // within two ulps of teal's per-face quotients. FP32 divides per face (its products could
-    // underflow).
+    // limiter factor: the minimum over the cell's faces of teal's candidate ratios. Each candidate
+    // is a fraction num / den with num >= 0 and den > 0 (delta1 has delta2's sign or is zero):
+    //   Barth-Jespersen  min(1, delta1 / delta2) = |delta1| / |delta2|, the 1 by psi's start value
+    //                    (limiter.c:54-58);
+    //   Venkatakrishnan  top / bot / delta2 (limiter.c:100-106) with delta2 divided out of top:
+    //                    (d1 (d1 + 2 d2) + eps2) / (d1 (d1 + d2) + 2 d2^2 + eps2), every term >= 0.
+    // In FP64 the running minimum stays a fraction compared by cross multiplication and is divided
+    // once: one division per thread instead of one or two per face, within a few ulps of teal's
+    // per-face quotients. FP32 divides per face (its products could underflow).
     R psi = R(1);
     if (LIM != 0) {
-        R e2 = (LIM == 2) ? R(__ldg(eps2 + c)) : R(0);
+        const R e2 = (LIM == 2) ? R(__ldg(eps2 + c)) : R(0);
+        const R dmx = R(mx - qc), dmn = R(mn - qc);
         R best_n = R(1), best_d = R(1);
 #pragma unroll
         for (int j = 0; j < MAX_SLOTS; j++) {
@@ -152,30 +158,24 @@ __global__ void __launch_bounds__(GRAD_THREADS) k_gradient(Sizes s, Geometry<R> 
                 R d2 = ((gx * s_off[0 * MAX_SLOTS + j][l]) + (gy * s_off[1 * MAX_SLOTS + j][l])) +
                        (gz * s_off[2 * MAX_SLOTS + j][l]);
                 if (!is_close_zero(d2)) {
-                    R d1 = R(((d2 > R(0)) ? mx : mn) - qc);
+                    const R d1 = (d2 > R(0)) ? dmx : dmn;
                     R num, den;
-                    if (LIM == 1) {  // Barth-Jespersen: min(1, d1 / d2) (limiter.c:54-58)
-                        num = d1;
-                        den = d2;
+                    if (LIM == 1) {
+                        num = fabs(d1);
+                        den = fabs(d2);
                     }
-                    else {  // Venkatakrishnan: top / bot / d2 (limiter.c:100-106); bot > 0
-                        R top = (((d1 * d1) + e2) * d2) + ((R(2) * (d2 * d2)) * d1);
-                        R bot = (((d1 * d1) + (R(2) * (d2 * d2))) + (d1 * d2)) + e2;
-                        num = top;
-                        den = bot * d2;
+                    else {
+                        num = fma(d1, fma(R(2), d2, d1), e2);
+                        den = fma(d1, d1 + d2, fma(d2 + d2, d2, e2));
                     }
                     if constexpr (sizeof(R) == sizeof(double)) {
-                        if (den < R(0)) {
-                            num = -num;
-                            den = -den;
-                        }
                         if (num * best_d < best_n * den) {
                             best_n = num;
                             best_d = den;
                         }
                     }
                     else {
-                        psi = fmin(psi, (LIM == 1) ? fmin(R(1), num / den) : num / den);
+                        psi = fmin(psi, num / den);
                     }
                 }
             }

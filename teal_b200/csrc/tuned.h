@@ -1,8 +1,9 @@
 // Launch shapes of the hot kernels, chosen by teal_b200/autotune.py on a B200 (fastest measured RK
-// step: TGV for the face and cell shapes and the Navier-Stokes staging switch, the ramp for the
-// Euler staging switch; times within 0.5 % of the fastest count as ties, resolved to fewer resident
-// face blocks, i.e. more registers per thread). The cell shape comes from its sweep (0.113 vs
-// 0.133 ms per TGV 128^3 launch). A value given with -D at build time wins.
+// step: TGV for the face, cell and gradient shapes and the Navier-Stokes staging switch, the ramp
+// for the Euler staging switch; times within 0.5 % of the fastest count as ties, resolved to fewer
+// resident face blocks, i.e. more registers per thread). The cell shape comes from its sweep (0.113
+// vs 0.133 ms per TGV 128^3 launch), the gradient's from its own (0.264 vs 0.280 ms). A value given
+// with -D at build time wins.
 #pragma once
 
 #ifndef TG_FACE_BLOCK
@@ -22,4 +23,7 @@
 #endif
 #ifndef TG_CELL_MINB
 #define TG_CELL_MINB 12  // cell-gather blocks kept resident per SM (caps registers per thread)
+#endif
+#ifndef TG_GRAD_MINB
+#define TG_GRAD_MINB 12  // gradient blocks (160 threads) kept resident per SM (caps registers per thread)
 #endif
