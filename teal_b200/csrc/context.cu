@@ -793,8 +793,8 @@ static int create_ctx(MeshInput &in, const tg_equations *e, int precision, tg_ct
                                                                   c->gb.slot_w, c->gb.slot_off, d_err);
             CU(cudaGetLastError());
             {
-                // meshes whose cells all have MAX_SLOTS faces (hexahedra) stage every slot row
-                // unconditionally in the gradient kernel; others skip padding slots
+                // on meshes whose cells all have MAX_SLOTS faces (hexahedra) the gradient kernel
+                // takes the slot count as a compile-time constant
                 std::vector<uint8_t> cnt(s.C);
                 CU(cudaMemcpyAsync(cnt.data(), c->slot_cnt, s.C, cudaMemcpyDeviceToHost, st));
                 CU(cudaStreamSynchronize(st));
@@ -1081,26 +1081,26 @@ static int run_boundary(tg_ctx *c, double *q, bool masked = false)
     return TG_OK;
 }
 
-template <typename R, bool SKIP>
+template <typename R, bool MIXED>
 static void launch_gradient_s(tg_ctx *c, const Geometry<R> &g, bool fold, const double *q)
 {
     dim3 grid((c->s.C + GRAD_CELLS - 1) / GRAD_CELLS);
     R *rec = (R *)c->grad;
     switch (c->limiter) {
         case TG_LIMITER_NONE:
-            k_gradient<R, 0, true, SKIP><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
+            k_gradient<R, 0, true, MIXED><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
             break;
         case TG_LIMITER_BARTH_JESPERSEN:
             if (fold)
-                k_gradient<R, 1, true, SKIP><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
+                k_gradient<R, 1, true, MIXED><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
             else
-                k_gradient<R, 1, false, SKIP><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
+                k_gradient<R, 1, false, MIXED><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
             break;
         default:
             if (fold)
-                k_gradient<R, 2, true, SKIP><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
+                k_gradient<R, 2, true, MIXED><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
             else
-                k_gradient<R, 2, false, SKIP><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
+                k_gradient<R, 2, false, MIXED><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
             break;
     }
 }
