@@ -109,10 +109,12 @@ __device__ __forceinline__ Prim<R> reload_prim(const double *__restrict__ q, int
     return p;
 }
 
-// Per-cell gradient record: (gx, gy, gz, psi) for each of the 5 variables, 20 values per cell,
-// read and written as two 2-vectors per variable (16-byte accesses in FP64). (A compact 16-value
-// layout for folded records, one cache line per cell, was measured slower: the per-variable
-// writers leave partially written sectors.)
+// Per-cell gradient record: (gx, gy, gz, psi) for each of the 5 variables, 20 values per cell;
+// each variable's 4 values are one aligned 32-byte access in FP64, a single 256-bit load or store,
+// so that a record gather costs one instruction per variable (TGV 128^3 face kernel 0.493 -> 0.479
+// ms, gradient kernel 0.264 -> 0.246 ms against two 16-byte accesses). (A
+// compact 16-value layout for folded records, one cache line per cell, was measured slower: the
+// per-variable writers leave partially written sectors.)
 template <typename R>
 struct Vec2;
 template <>
@@ -124,27 +126,56 @@ struct Vec2<float> {
     using T = float2;
 };
 
-template <typename R>
-__device__ __forceinline__ void grad_rec_store(R *rec, int c, int v, R gx, R gy, R gz, R psi)
+__device__ __forceinline__ void grad_rec_store(double *rec, int c, int v, double gx, double gy, double gz,
+                                               double psi)
 {
-    using T2 = typename Vec2<R>::T;
-    T2 *p = reinterpret_cast<T2 *>(rec + ((size_t)c * 5 + v) * 4);
-    p[0] = T2{gx, gy};
-    p[1] = T2{gz, psi};
+    double *p = rec + ((size_t)c * 5 + v) * 4;
+    asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(gx), "d"(gy), "d"(gz), "d"(psi)
+                 : "memory");
+}
+__device__ __forceinline__ void grad_rec_store(float *rec, int c, int v, float gx, float gy, float gz, float psi)
+{
+    float2 *p = reinterpret_cast<float2 *>(rec + ((size_t)c * 5 + v) * 4);
+    p[0] = make_float2(gx, gy);
+    p[1] = make_float2(gz, psi);
 }
 
-template <typename R>
-__device__ __forceinline__ void grad_rec_load(const R *rec, int c, int v, R &gx, R &gy, R &gz, R &psi)
+// read-only loads: the records are written by an earlier launch
+__device__ __forceinline__ void grad_rec_load(const double *rec, int c, int v, double &gx, double &gy, double &gz,
+                                              double &psi)
 {
-    using T2 = typename Vec2<R>::T;
-    const T2 *p = reinterpret_cast<const T2 *>(rec + ((size_t)c * 5 + v) * 4);
-    T2 a = __ldg(p), b = __ldg(p + 1);
+    const double *p = rec + ((size_t)c * 5 + v) * 4;
+    asm volatile("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(gx), "=d"(gy), "=d"(gz), "=d"(psi) : "l"(p));
+}
+__device__ __forceinline__ void grad_rec_load(const float *rec, int c, int v, float &gx, float &gy, float &gz,
+                                              float &psi)
+{
+    // two 8-byte loads: one 16-byte load was measured slower in the FP32 face kernel (0.371 vs
+    // 0.326 ms, TGV 128^3)
+    const float2 *p = reinterpret_cast<const float2 *>(rec + ((size_t)c * 5 + v) * 4);
+    const float2 a = __ldg(p), b = __ldg(p + 1);
     gx = a.x, gy = a.y, gz = b.x, psi = b.y;
 }
 
-// Per-face flux records, 5 values per face without padding: components 0-3 as [F][4] (two 2-vector
-// accesses), component 4 as [F] after them.
+// Per-face flux records, 5 values per face without padding: components 0-3 as [F][4] (one 256-bit
+// access in FP64, two 2-vector accesses in FP32), component 4 as [F] after them.
 constexpr int FLUX_REC = 5;
+
+__device__ __forceinline__ void flux_rec_store(double *G, int F, int f, const double (&v)[5])
+{
+    asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(G + (size_t)f * 4), "d"(v[0]), "d"(v[1]),
+                 "d"(v[2]), "d"(v[3])
+                 : "memory");
+    G[(size_t)4 * F + f] = v[4];
+}
+
+__device__ __forceinline__ void flux_rec_load(const double *G, int F, int f, double (&v)[5])
+{
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+        : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3])
+        : "l"(G + (size_t)f * 4));
+    v[4] = __ldg(G + (size_t)4 * F + f);
+}
 
 template <typename R>
 __device__ __forceinline__ void flux_rec_store(R *G, int F, int f, const R (&v)[5])
