@@ -220,7 +220,7 @@ struct tg_ctx {
     // state
     double *q = nullptr, *U0 = nullptr, *R = nullptr;
     double *qs = nullptr;  // scratch state for derivatives of host-given states (allocated on use)
-    void *grad = nullptr, *G = nullptr;  // gradient records [C][5][4], face flux records [F][6]
+    void *grad = nullptr, *G = nullptr;  // gradient records [C][5][4], face flux records [F][4] + [F]
     double *dtc = nullptr;               // per-cell stable step
     double *part_min = nullptr, *part_sum = nullptr;
     double *sd = nullptr;  // device step doubles [SD_COUNT][ninst]
