@@ -16,7 +16,9 @@ ausmd flux, Barth-Jespersen limiter, supersonic inflow / outflow and slip walls,
 With --gpus N (launched by torchrun) every rank advances its own replica of the workload (the path is
 one mesh per GPU; there is no exchange), timed on the device, max over ranks; `value` is the
 whole-job throughput. `--impl reference` times the reference solver (compiled from its own C
-sources) on the host cores.
+sources) on the host cores: for tgv teal's own MPI domain decomposition of the full case, one rank
+per core (oracle/_ref/teal_ref_mpi); for ramp, whose partitioner needs ParMETIS, one single-process
+run per core on a sample mesh (an upper bound of the MPI run).
 """
 
 import argparse
@@ -291,6 +293,31 @@ def reference_cpu_all(n, steps, workload="tgv", procs=None):
     return sum(r[0] * r[1] for r in res) / wall, wall, steps, procs
 
 
+MPI_RUN = os.path.join(ROOT, "oracle", "_ref", "teal_ref_mpi")
+
+
+def reference_mpi(n, steps, warmup=2, ranks=None):
+    """teal's own domain-decomposed Taylor-Green run on all host cores (oracle/_ref/teal_ref_mpi: the
+    reference's mesh_create split, halo exchanges and reductions over a fork / shared-memory MPI
+    subset), n^3 cells, `steps` timed lserk steps after `warmup`. Returns (cell-updates/s, seconds of
+    the slowest rank, steps, ranks)."""
+    ranks = ranks or min(len(os.sched_getaffinity(0)), 1024)
+    env = dict(os.environ, TEAL_SHIM_RANKS=str(ranks), TEAL_SHIM_TIMEOUT="900")
+    r = subprocess.run([MPI_RUN, "--n", str(n), "--steps", str(steps), "--warmup", str(warmup)],
+                       capture_output=True, text=True, env=env, timeout=1800)
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    if r.returncode != 0 or not lines:
+        raise RuntimeError(f"teal_ref_mpi failed ({r.returncode}): {r.stderr[-500:]}")
+    out = json.loads(lines[-1])
+    return out["cells"] * out["steps"] / out["seconds"], out["seconds"], out["steps"], out["ranks"]
+
+
+def mpi_sample(steps, warmup, ranks, n=128):
+    return (f"teal's own MPI run of the full {n}^3 case (mesh_create domain decomposition, halo "
+            f"exchanges, global reductions) on {ranks} ranks, one per host core, over a fork / "
+            f"shared-memory MPI subset: {steps} lserk steps after {warmup} warm-up steps, slowest rank")
+
+
 def run_serving(args, world, rank):
     """Serving benchmark: seeded Poisson arrivals of steady solve requests (meshes of 20k-2M cells,
     Mach 0.2-3.0, flux scheme and tolerance per request), served with continuous admission by HBM
@@ -483,19 +510,25 @@ def run_reference_arm(args, world, rank):
     if not ref.available():
         print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref not built"}))
         return
-    n_sample = args.ref_n
-    value, secs, steps, procs = reference_cpu_all(n_sample, args.steps, workload=args.workload)
+    if args.workload == "tgv" and os.path.exists(MPI_RUN):
+        value, secs, steps, procs = reference_mpi(args.n, args.steps, args.warmup)
+        sample = mpi_sample(steps, args.warmup, procs, args.n)
+        config_extra = {"mesh": f"{args.n}^3", "parallelism": f"{procs} MPI ranks"}
+    else:
+        n_sample = args.ref_n
+        value, secs, steps, procs = reference_cpu_all(n_sample, args.steps, workload=args.workload)
+        sample = (f"{procs} single-process reference runs at once (one per host core), each {steps} lserk "
+                  f"steps of the same case on a {n_sample}^3 mesh; no halo exchange, so an upper bound of "
+                  "the all-core MPI run")
+        config_extra = {"sample_mesh": f"{n_sample}^3 per core", "parallelism": f"{procs} cores"}
     line = {
         "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000 * secs / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": workload_name(args.workload, None),
-                   "sample_mesh": f"{n_sample}^3 per core", "parallelism": f"{procs} cores"},
+        "config": dict({"workload": workload_name(args.workload, None)}, **config_extra),
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": procs, "kind": "reference",
-                         "sample": f"{procs} single-process reference runs at once (one per host core), each "
-                                   f"{steps} lserk steps of the same case on a {n_sample}^3 mesh; no halo "
-                                   "exchange, so an upper bound of the all-core MPI run"},
+                         "sample": sample},
         "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -519,13 +552,16 @@ def main():
     ap.add_argument("--n", type=int, default=None, help="mesh cells per axis (tgv 128, ramp 80)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--ref-n", type=int, default=None, help="mesh size of the CPU reference sample (tgv 48, ramp 32)")
-    ap.add_argument("--ref-steps", type=int, default=20, help="steps of the CPU baseline sample")
+    ap.add_argument("--ref-steps", type=int, default=None,
+                    help="steps of the CPU baseline sample (tgv: the all-core MPI run, 10; ramp: 20)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.n is None:
         args.n = 128 if args.workload == "tgv" else 80
     if args.ref_n is None:
         args.ref_n = 48 if args.workload == "tgv" else 32
+    if args.ref_steps is None:
+        args.ref_steps = 10 if args.workload == "tgv" else 20
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()
 
@@ -679,7 +715,11 @@ def main():
         try:
             from oracle import ref
 
-            if ref.available():
+            if args.workload == "tgv" and os.path.exists(MPI_RUN):
+                v, secs, st, procs = reference_mpi(args.n, args.ref_steps, 2)
+                line["cpu_baseline"] = {"value": v, "unit": "cell-updates/s", "cores": procs, "kind": "reference",
+                                        "sample": mpi_sample(st, 2, procs, args.n) + f" ({secs:.1f} s)"}
+            elif ref.available():
                 v, secs, st, procs = reference_cpu_all(args.ref_n, args.ref_steps, workload=args.workload)
                 line["cpu_baseline"] = {"value": v, "unit": "cell-updates/s", "cores": procs, "kind": "reference",
                                         "sample": f"{procs} single-process reference runs at once (one per host "

@@ -1,13 +1,17 @@
 /*
- * Single-rank MPI stand-in used ONLY to compile the reference solver's sources in place as a test
- * oracle (no MPI library exists in this image). It is test infrastructure, never product code.
+ * MPI stand-ins used ONLY to compile and run the reference solver's sources in place as a test
+ * oracle and CPU baseline (no MPI library exists in this image). Test infrastructure, never product
+ * code. Two implementations of this subset:
  *
- * Semantics: one process, rank 0, size 1. Collectives reduce over one rank (in place = no-op,
- * otherwise a copy). Point-to-point messages are self-sends matched by tag in posting order, which
- * is what the reference's periodic halo exchange needs on one rank (equations/exchange.c:8-51,
- * mesh/create.c:351-440: a periodic Cartesian axis makes the rank its own neighbour).
- * Cartesian topology: every coordinate is 0; a periodic axis shifts to rank 0, a non-periodic
- * axis to MPI_PROC_NULL.
+ * shim_mpi.c (linked into _ref/libteal_ref.so, loaded in-process by the tests): one process, rank 0,
+ * size 1. Collectives reduce over one rank (in place = no-op, otherwise a copy). Point-to-point
+ * messages are self-sends matched by tag in posting order, which is what the reference's periodic
+ * halo exchange needs on one rank (equations/exchange.c:8-51, mesh/create.c:351-440: a periodic
+ * Cartesian axis makes the rank its own neighbour). Cartesian topology: every coordinate is 0; a
+ * periodic axis shifts to rank 0, a non-periodic axis to MPI_PROC_NULL.
+ *
+ * shim_mpi_fork.c (linked into _ref/teal_ref_mpi): TEAL_SHIM_RANKS processes forked by MPI_Init,
+ * messages through shared-memory inboxes; see that file.
  */
 #pragma once
 
