@@ -28,11 +28,11 @@ struct Geometry {
     const G *offl;        // [3][F] face centre - left centre
     const G *offr;        // [3][F] face centre - right centre (teal's ghost centre for ghosts)
     const G *corr;        // [4][F] unit vector left->right centre, distance (Navier–Stokes)
-    const int *slot_nbr;  // [6][C] neighbour state row
-    const int *slot_face; // [6][C] face index f (cell is left) or ~f (cell is right)
+    const int *slot_nbr;  // [6][SL] neighbour state row
+    const int *slot_face; // [6][SL] face index f (cell is left) or ~f (cell is right)
     const uint8_t *slot_cnt; // [C]
-    const G *slot_w;      // [3][6][C] least-squares weight of this cell's side
-    const G *slot_off;    // [3][6][C] face centre - cell centre (limiter)
+    const G *slot_w;      // [3][6][SL] least-squares weight of this cell's side
+    const G *slot_off;    // [3][6][SL] face centre - cell centre (limiter)
 };
 
 struct CellData {
