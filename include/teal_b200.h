@@ -73,7 +73,9 @@ enum {
     TG_BC_SUBSONIC_OUTFLOW = 5,
     TG_BC_PRESSURE_OUTFLOW = 6,
     TG_BC_FARFIELD = 7,
-    TG_BC_ADIABATIC_WALL = 8 /* "adiabatic wall", "wall" (Navier–Stokes only) */
+    TG_BC_ADIABATIC_WALL = 8, /* "adiabatic wall", "wall" (Navier–Stokes only) */
+    TG_BC_CUSTOM = 9          /* "custom": teal's Compute callback (src/equations/boundary.c:27-33) as
+                                 a registered device function, tg_bind_boundary_function */
 };
 
 /* Source terms run on the device (teal's Equations.source, src/equations.h:27-41, is a host
@@ -84,7 +86,9 @@ enum {
  *                           scale tau = source_parameter[1]: s = rho (U - <u_x>) / tau,
  *                           S = (0, s, 0, 0, u_x s), <u_x> the volume average over the inner cells of
  *                           the state being differentiated (run/periodic_hill/run.c:8-21) */
-enum { TG_SOURCE_NONE = 0, TG_SOURCE_BODY_FORCE = 1, TG_SOURCE_BULK_FORCING = 2 };
+enum { TG_SOURCE_NONE = 0, TG_SOURCE_BODY_FORCE = 1, TG_SOURCE_BULK_FORCING = 2, TG_SOURCE_DEVICE = 3 };
+/*   TG_SOURCE_DEVICE        teal's source Compute callback (src/equations/derivative.c:242-266) as a
+ *                           registered device function, tg_bind_source_function */
 
 /* time integrators of simulation_set_advance (src/simulation/set.c:74-131) */
 enum { TG_ADVANCE_EULER = 0, TG_ADVANCE_LSERK = 1, TG_ADVANCE_IMPLICIT_EULER = 2 };
@@ -333,6 +337,34 @@ int tg_residual_noalloc(const double *derivative, const double *volume, int num_
 
 /* ---- version / build info ---------------------------------------------------------------------- */
 const char *tg_build_info(void);
+
+/* ---- device functions: teal's host Compute callbacks (src/equations.h:27-41) as CUDA C --------- */
+/* kinds of device function */
+enum { TG_FUNCTION_BOUNDARY = 1, TG_FUNCTION_SOURCE = 2 };
+
+/* Register `source`, CUDA C that defines
+ *   __device__ void <name>(double *out, const double *property, const double *center, double time,
+ *                          const double *context)
+ * with the arguments teal passes its Compute callback: out = the ghost cell's primitive state
+ * (boundary; it holds the ghost row's current values on entry, as teal's in-place call does) or the
+ * cell's source in conserved variables (source; zero on entry); property = the equations'
+ * properties (heat capacity ratio, then dynamic viscosity and Prandtl number for Navier-Stokes);
+ * center = the ghost cell's centre (boundary) or the cell's centre (source), 3 doubles; time = the
+ * time of the residual being evaluated (teal's stage time); context = the inner cell's primitive
+ * state (boundary) or the cell's primitive state (source), 5 doubles. The function is compiled at
+ * once with NVRTC for sm_100a without FMA contraction (libnvrtc is loaded at run time, no device
+ * needed); a compile error returns TG_ERR_INVALID with the compiler log in `log` (`log_size` bytes,
+ * may be null). A second registration of a name replaces the first for later bindings. */
+int tg_function_register(const char *name, int kind, const char *source, char *log, long log_size);
+
+/* Use the registered boundary function `name` for boundary `boundary` (the index into
+ * tg_equations.boundary_kind, whose kind must be TG_BC_CUSTOM). One-mesh contexts only; every
+ * custom boundary must be bound before the first residual. */
+int tg_bind_boundary_function(tg_ctx *ctx, int boundary, const char *name);
+
+/* Use the registered source function `name` (tg_equations.source must be TG_SOURCE_DEVICE). One-mesh
+ * contexts only. */
+int tg_bind_source_function(tg_ctx *ctx, const char *name);
 
 #ifdef __cplusplus
 }

@@ -51,6 +51,7 @@ def lib():
             "ref_set_property": (None, [vp, ctypes.c_char_p, ctypes.c_double]),
             "ref_set_source": (None, [vp, ctypes.c_int, dp]),
             "ref_set_boundary": (None, [vp, ctypes.c_char_p, ctypes.c_char_p, dp]),
+            "ref_set_boundary_custom": (None, [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_double]),
             "ref_primitive": (dp, [vp]),
             "ref_limiter_parameter": (dp, [vp]),
             "ref_derivative": (None, [vp, dp, dp, ctypes.c_double]),
@@ -212,11 +213,18 @@ class RefEquations:
         lib().ref_set_property(self.ptr, name.encode(), value)
 
     def set_source(self, name, parameters=()):
-        """The run cases' source callbacks: "body force" (gx, gy, gz) or "bulk forcing" (U, tau)."""
-        kind = {None: 0, "body force": 1, "bulk forcing": 2}[name]
+        """The run cases' source callbacks: "body force" (gx, gy, gz) or "bulk forcing" (U, tau), or
+        "unsteady" (the harness's time- and position-dependent forcing)."""
+        kind = {None: 0, "body force": 1, "bulk forcing": 2, "unsteady": 3}[name]
         p = [float(x) for x in parameters][:4]
         self._src = np.array(p + [0.0] * (4 - len(p)))
         lib().ref_set_source(self.ptr, kind, _d(self._src))
+
+    def set_boundary_custom(self, entity, kind, speed=1.0):
+        """teal's "custom" boundary with the harness's Compute callback: "moving wall" (speed along x)
+        or "unsteady inflow"."""
+        k = {"moving wall": 1, "unsteady inflow": 2}[kind]
+        lib().ref_set_boundary_custom(self.ptr, entity.encode(), k, float(speed))
 
     def set_boundary_condition(self, entity, name, context=None):
         ctx = None

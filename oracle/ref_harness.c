@@ -4,6 +4,7 @@
  * reference's own results. It only calls the reference's public API (src/*.h) and reads its
  * structs; it computes nothing itself.
  */
+#include <math.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -270,12 +271,65 @@ static void src_bulk_forcing(void *source_, const double *property, Vector cente
     source[4] = primitive[1] * s1;
 }
 
+/* kind 3: a time- and position-dependent momentum forcing f = rho (0.1 sin(x + t), 0.05 cos(y - t), 0)
+ * with its work u . f as the energy source; the device-function tests compile the same formula */
+static void src_unsteady(void *source_, const double *property, Vector center, double time, const void *context)
+{
+    double *source = source_;
+    const double *primitive = context;
+    (void)property;
+    double fx = 0.1 * primitive[0] * sin(center.x + time);
+    double fy = 0.05 * primitive[0] * cos(center.y - time);
+    source[0] = 0;
+    source[1] = fx;
+    source[2] = fy;
+    source[3] = 0;
+    source[4] = (primitive[1] * fx) + (primitive[2] * fy);
+}
+
 void ref_set_source(void *eqns, int kind, const double *par)
 {
     for (int i = 0; i < 4; i++) src_par[i] = par ? par[i] : 0.0;
     if (kind == 1) equations_set_source(eqns, src_body_force, 0);
     else if (kind == 2) equations_set_source(eqns, src_bulk_forcing, src_bulk_prepare);
+    else if (kind == 3) equations_set_source(eqns, src_unsteady, 0);
     else equations_set_source(eqns, 0, 0);
+}
+
+/* Custom boundary conditions (teal's "custom" kind with a Compute callback, boundary.c:27-33) as the
+ * run cases write them; the device-function tests compile the same formulas. Kind 1: a wall moving
+ * with speed bc_speed along x (run/lid_driven_cavity/run.c:7-17, there speed 1); kind 2: an
+ * unsteady inflow state of the ghost centre and time. One setting per process. */
+static double bc_speed = 1.0;
+
+static void bc_moving_wall(void *outer_, const double *property, Vector center, double time, const void *context)
+{
+    double *outer = outer_;
+    const double *inner = context;
+    (void)property, (void)center, (void)time;
+    outer[0] = inner[0];
+    outer[1] = (2 * bc_speed) - inner[1];
+    outer[2] = -inner[2];
+    outer[3] = -inner[3];
+    outer[4] = inner[4];
+}
+
+static void bc_unsteady_inflow(void *outer_, const double *property, Vector center, double time,
+                               const void *context)
+{
+    double *outer = outer_;
+    (void)context;
+    outer[0] = 1 + (0.1 * sin(center.x - time));
+    outer[1] = 0.5 + (0.05 * cos(center.y + (2 * time)));
+    outer[2] = 0.01 * center.z;
+    outer[3] = 0;
+    outer[4] = (1 / property[0]) + (0.02 * sin(3 * time));
+}
+
+void ref_set_boundary_custom(void *eqns, const char *entity, int kind, double speed)
+{
+    bc_speed = speed;
+    equations_set_boundary_condition(eqns, entity, "custom", kind == 1 ? bc_moving_wall : bc_unsteady_inflow, 0);
 }
 
 void ref_set_property(void *eqns, const char *name, double value)

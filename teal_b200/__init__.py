@@ -24,4 +24,5 @@ from .api import (  # noqa: F401
     euler_create,
     mesh_create,
     navierstokes_create,
+    register_function,
 )

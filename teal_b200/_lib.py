@@ -25,7 +25,9 @@ TG_VISCOUS_NONE, TG_VISCOUS_CENTRAL = 0, 1
 TG_LIMITER_NONE, TG_LIMITER_BARTH_JESPERSEN, TG_LIMITER_VENKATAKRISHNAN = 0, 1, 2
 TG_ADVANCE_EULER, TG_ADVANCE_LSERK, TG_ADVANCE_IMPLICIT_EULER = 0, 1, 2
 TG_PRECISION_FP64, TG_PRECISION_FP32_FLUX = 0, 1
-TG_SOURCE_NONE, TG_SOURCE_BODY_FORCE, TG_SOURCE_BULK_FORCING = 0, 1, 2
+TG_SOURCE_NONE, TG_SOURCE_BODY_FORCE, TG_SOURCE_BULK_FORCING, TG_SOURCE_DEVICE = 0, 1, 2, 3
+TG_BC_CUSTOM = 9
+TG_FUNCTION_BOUNDARY, TG_FUNCTION_SOURCE = 1, 2
 TG_NOALLOC_MAX_CELLS = 67108864  # cell limit of tg_residual_noalloc (its fixed scratch array)
 
 _int_p = ctypes.POINTER(ctypes.c_int)
@@ -151,6 +153,10 @@ SIGNATURES = [
     ("tg_launch_count", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_long)]),
     ("tg_layout", ctypes.c_int, [_vp, ctypes.c_char_p, _vp, ctypes.c_long]),
     ("tg_residual_noalloc", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_double, _vp, _vp]),
+    ("tg_function_register", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p,
+                                            ctypes.c_long]),
+    ("tg_bind_boundary_function", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_char_p]),
+    ("tg_bind_source_function", ctypes.c_int, [_vp, ctypes.c_char_p]),
     ("tg_build_info", ctypes.c_char_p, []),
 ]
 

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/teal_b200.h"
+#include "functions.h"
 #include "gmres.cuh"
 #include "kernels.cuh"
 #include "launch.cuh"
@@ -110,6 +111,7 @@ extern "C" int tg_boundary_select(const char *name, int physics)
     if (!strcmp(name, "subsonic outflow")) return TG_BC_SUBSONIC_OUTFLOW;
     if (!strcmp(name, "pressure outflow")) return TG_BC_PRESSURE_OUTFLOW;
     if (!strcmp(name, "farfield")) return TG_BC_FARFIELD;
+    if (!strcmp(name, "custom")) return TG_BC_CUSTOM;
     return -1;
 }
 
@@ -118,6 +120,7 @@ extern "C" int tg_source_select(const char *name)
     if (!name) return -1;
     if (!strcmp(name, "body force")) return TG_SOURCE_BODY_FORCE;
     if (!strcmp(name, "bulk forcing")) return TG_SOURCE_BULK_FORCING;
+    if (!strcmp(name, "device function")) return TG_SOURCE_DEVICE;
     return -1;
 }
 
@@ -246,6 +249,19 @@ struct tg_ctx {
     double prof_ms[TG_PROF_CATEGORIES] = {0};
     long prof_n[TG_PROF_CATEGORIES] = {0};
 
+    // device functions in place of teal's Compute callbacks (one-mesh contexts)
+    std::vector<std::pair<int, int>> bd_range;  // boundary index -> teal face range [beg, end)
+    std::vector<const void *> bd_kernel;        // boundary index -> bound kernel (custom kinds)
+    double *bcenter = nullptr;  // [F_bd - F_in][3] ghost cell centres of the boundary faces
+    double *ccenter = nullptr;  // [C][3] cell centres (device source)
+    double *S = nullptr;        // [5][C] device source values of the residual being evaluated
+    double *dprop = nullptr;    // [3] properties
+    const void *src_kernel = nullptr;
+    // time of the residual being evaluated: time[0] + coef * step[0] on the device (inside step
+    // sequences), else host
+    const double *t_time = nullptr, *t_step = nullptr;
+    double t_coef = 0, t_host = 0;
+
     // step graph cache
     cudaGraphExec_t graph = nullptr;
     int graph_method = -1, graph_stages = 0;
@@ -295,7 +311,8 @@ static void free_ctx(tg_ctx *c)
         cudaEventDestroy(p.second.second);
     }
     if (c->graph) cudaGraphExecDestroy(c->graph);
-    void *ptrs[] = {c->lr, c->slot_nbr, c->slot_face, c->slot_cnt, c->owner, c->bface_ent, c->bkind, c->bctx,
+    void *ptrs[] = {c->bcenter, c->ccenter, c->S, c->dprop,
+                    c->lr, c->slot_nbr, c->slot_face, c->slot_cnt, c->owner, c->bface_ent, c->bkind, c->bctx,
                     c->volume, c->proj, c->eps2, c->gb.area, c->gb.basis, c->gb.offl, c->gb.offr, c->gb.corr,
                     c->gb.slot_w, c->gb.slot_off, c->gb.area32, c->gb.basis32, c->gb.offl32, c->gb.offr32,
                     c->gb.corr32, c->gb.slot_w32, c->gb.slot_off32, c->q, c->U0, c->R, c->qs, c->grad, c->G,
@@ -446,7 +463,7 @@ static int validate(const tg_mesh *m, const tg_equations *e)
         return fail(TG_ERR_INVALID, "viscous flux needs face corrections");
     if (e->limiter < TG_LIMITER_NONE || e->limiter > TG_LIMITER_VENKATAKRISHNAN)
         return fail(TG_ERR_INVALID, "invalid limiter kind (%d)", e->limiter);
-    if (e->source < TG_SOURCE_NONE || e->source > TG_SOURCE_BULK_FORCING)
+    if (e->source < TG_SOURCE_NONE || e->source > TG_SOURCE_DEVICE)
         return fail(TG_ERR_INVALID, "invalid source kind (%d)", e->source);
     if (e->source == TG_SOURCE_BULK_FORCING && !(e->source_parameter[1] != 0))
         return fail(TG_ERR_INVALID, "bulk forcing needs a nonzero time scale");
@@ -455,7 +472,7 @@ static int validate(const tg_mesh *m, const tg_equations *e)
         return fail(TG_ERR_INVALID, "boundary count %d does not match the mesh (%d)", e->num_boundaries, nb);
     for (int i = 0; i < nb; i++) {
         int k = e->boundary_kind ? e->boundary_kind[i] : 0;
-        if (k < TG_BC_SYMMETRY || k > TG_BC_ADIABATIC_WALL)
+        if (k < TG_BC_SYMMETRY || k > TG_BC_CUSTOM)
             return fail(TG_ERR_INVALID, "boundary %d has no device boundary condition", i);
         if (k == TG_BC_ADIABATIC_WALL && e->physics != TG_NAVIERSTOKES)
             return fail(TG_ERR_INVALID, "adiabatic wall needs the Navier-Stokes equations");
@@ -532,6 +549,12 @@ static int merged_input(const tg_mesh *ms, const tg_equations *es, int num, Mesh
     for (int i = 0; i < num; i++) {
         TRY(validate(&ms[i], &es[i]));
         const tg_equations &e = es[i];
+        if (e.source == TG_SOURCE_DEVICE)
+            return fail(TG_ERR_INVALID, "device source functions need a one-mesh context");
+        for (int b = 0; b < e.num_boundaries; b++) {
+            if (e.boundary_kind[b] == TG_BC_CUSTOM)
+                return fail(TG_ERR_INVALID, "custom boundary functions need a one-mesh context");
+        }
         if (e.physics != e0.physics || e.space_order != e0.space_order || e.convective != e0.convective ||
             e.viscous != e0.viscous || e.limiter != e0.limiter || e.property[0] != e0.property[0] ||
             e.property[1] != e0.property[1] || e.property[2] != e0.property[2] || e.source != e0.source ||
@@ -912,13 +935,109 @@ static int create_ctx(MeshInput &in, const tg_equations *e, int precision, tg_ct
     return TG_OK;
 }
 
+// Device data of the device functions: boundary ranges and ghost centres for custom boundaries,
+// cell centres and the source buffer for a device source, the properties.
+static int setup_functions(tg_ctx *c, const tg_mesh *m, const tg_equations *e)
+{
+    int nb = e->num_boundaries;
+    c->bd_range.resize(nb);
+    c->bd_kernel.assign(nb, nullptr);
+    bool custom = false;
+    for (int i = 0; i < nb; i++) {
+        int ent = m->num_inner_entities + i;
+        c->bd_range[i] = {m->entity_face_off[ent], m->entity_face_off[ent + 1]};
+        custom = custom || e->boundary_kind[i] == TG_BC_CUSTOM;
+    }
+    cudaStream_t st = c->stream;
+    if (custom || e->source == TG_SOURCE_DEVICE) {
+        TRY(upload(&c->dprop, c->prop, 3, st));
+    }
+    if (custom) {
+        int F_in = m->num_inner_faces, nbf = m->off_boundary_faces - F_in;
+        std::vector<double> centre(3 * (size_t)std::max(nbf, 1));
+        for (int i = 0; i < nbf; i++) {
+            int r = m->face_cell[2 * (size_t)(F_in + i) + 1];
+            for (int d = 0; d < 3; d++) centre[3 * (size_t)i + d] = m->cell_center[3 * (size_t)r + d];
+        }
+        TRY(upload(&c->bcenter, centre.data(), centre.size(), st));
+    }
+    if (e->source == TG_SOURCE_DEVICE) {
+        TRY(upload(&c->ccenter, m->cell_center, 3 * (size_t)c->s.C, st));
+        TRY(dalloc(&c->S, 5 * (size_t)c->s.C));
+        CU(cudaMemsetAsync(c->S, 0, 5 * sizeof(double) * c->s.C, st));
+    }
+    CU(cudaStreamSynchronize(st));
+    return TG_OK;
+}
+
+static void drop_graph(tg_ctx *c)
+{
+    if (c->graph) {
+        cudaGraphExecDestroy(c->graph);
+        c->graph = nullptr;
+    }
+}
+
+extern "C" int tg_function_register(const char *name, int kind, const char *source, char *log, long log_size)
+{
+    std::string error;
+    int rc = function_register(name, kind, source, log, log_size, error);
+    if (rc == 1) return fail(TG_ERR_INVALID, "%s", error.c_str());
+    if (rc != 0) return fail(TG_ERR_CUDA, "%s", error.c_str());
+    return TG_OK;
+}
+
+extern "C" int tg_bind_boundary_function(tg_ctx *c, int boundary, const char *name)
+{
+    if (!c || !name) return fail(TG_ERR_INVALID, "null argument");
+    if (c->ninst != 1) return fail(TG_ERR_INVALID, "device functions need a one-mesh context");
+    if (boundary < 0 || boundary >= (int)c->bd_range.size())
+        return fail(TG_ERR_INVALID, "boundary %d out of range", boundary);
+    int kind = 0;
+    CU(cudaMemcpy(&kind, c->bkind + boundary, sizeof(int), cudaMemcpyDeviceToHost));
+    if (kind != TG_BC_CUSTOM) return fail(TG_ERR_INVALID, "boundary %d is not a custom boundary", boundary);
+    std::string error;
+    const void *k = nullptr;
+    int rc = function_kernel(name, FUNCTION_BOUNDARY, &k, error);
+    if (rc == 1) return fail(TG_ERR_INVALID, "%s", error.c_str());
+    if (rc != 0) return fail(TG_ERR_CUDA, "%s", error.c_str());
+    CU(cudaStreamSynchronize(c->stream));
+    c->bd_kernel[boundary] = k;
+    drop_graph(c);  // captured steps launch the previous binding
+    return TG_OK;
+}
+
+extern "C" int tg_bind_source_function(tg_ctx *c, const char *name)
+{
+    if (!c || !name) return fail(TG_ERR_INVALID, "null argument");
+    if (c->ninst != 1) return fail(TG_ERR_INVALID, "device functions need a one-mesh context");
+    if (c->source != TG_SOURCE_DEVICE) return fail(TG_ERR_INVALID, "the equations' source is not a device function");
+    std::string error;
+    const void *k = nullptr;
+    int rc = function_kernel(name, FUNCTION_SOURCE, &k, error);
+    if (rc == 1) return fail(TG_ERR_INVALID, "%s", error.c_str());
+    if (rc != 0) return fail(TG_ERR_CUDA, "%s", error.c_str());
+    CU(cudaStreamSynchronize(c->stream));
+    c->src_kernel = k;
+    drop_graph(c);
+    return TG_OK;
+}
+
 extern "C" int tg_create(const tg_mesh *m, const tg_equations *e, int precision, tg_ctx **out)
 {
     if (!out) return fail(TG_ERR_INVALID, "null output pointer");
     *out = nullptr;
     MeshInput in;
     TRY(single_input(m, e, in));
-    return create_ctx(in, e, precision, out);
+    TRY(create_ctx(in, e, precision, out));
+    int rc = setup_functions(*out, m, e);
+    if (rc != TG_OK) {
+        std::string msg = g_error;
+        tg_destroy(*out);
+        *out = nullptr;
+        return fail(rc, "%s", msg.c_str());
+    }
+    return TG_OK;
 }
 
 extern "C" int tg_batch_create(const tg_mesh *meshes, const tg_equations *eqns, int num, int precision,
@@ -1078,6 +1197,20 @@ static int run_boundary(tg_ctx *c, double *q, bool masked = false)
     k_boundary<<<grid_of(nbf), BLOCK, 0, c->stream>>>(c->s, c->lr, c->gb.basis, c->bface_ent, c->bkind, c->bctx, q,
                                                       c->prop[0], c->cell_inst, masked ? c->st.active : nullptr);
     CU(cudaGetLastError());
+    // custom boundaries: their device functions, face by face of each boundary
+    for (size_t b = 0; b < c->bd_kernel.size(); b++) {
+        if (!c->bd_kernel[b]) continue;
+        int n = c->bd_range[b].second - c->bd_range[b].first, f0 = c->bd_range[b].first;
+        if (n <= 0) continue;
+        Launch lc(c, TG_PROF_BOUNDARY);
+        const int *lr = reinterpret_cast<const int *>(c->lr);
+        const double *centre = c->bcenter + 3 * (size_t)(f0 - c->s.F_in);
+        long N = c->s.N;
+        const int *active = masked ? c->st.active : nullptr;
+        void *args[] = {&n, &f0, &lr, &centre, &q, &N, &c->dprop, &c->t_time, &c->t_step, &c->t_coef, &c->t_host,
+                        &active};
+        CU(cudaLaunchKernel(c->bd_kernel[b], dim3((n + 127) / 128), dim3(128), args, 0, c->stream));
+    }
     return TG_OK;
 }
 
@@ -1165,7 +1298,8 @@ template <int MODE, bool NS, typename GT, int SRC>
 static void launch_cell_s(tg_ctx *c, double alpha, int last, double *q, double *Rout)
 {
     CellData cd{c->volume, c->proj, c->eps2};
-    Source src{{c->src_par[0], c->src_par[1], c->src_par[2], c->src_par[3]}, c->src_avg};
+    Source src{{c->src_par[0], c->src_par[1], c->src_par[2], c->src_par[3]},
+               c->source == TG_SOURCE_DEVICE ? c->S : c->src_avg};
     k_cell<MODE, NS, GT, SRC><<<(c->s.C + CELL_BLOCK - 1) / CELL_BLOCK, CELL_BLOCK, 0, c->stream>>>(
         c->s, c->slot_face, c->slot_cnt, cd, (const GT *)c->G, c->U0, q, Rout, c->seg, c->st, alpha, last,
         props_of(c), c->dtc, src);
@@ -1177,6 +1311,7 @@ static void launch_cell_t(tg_ctx *c, double alpha, int last, double *q, double *
     switch (c->source) {
         case TG_SOURCE_BODY_FORCE: launch_cell_s<MODE, NS, GT, 1>(c, alpha, last, q, Rout); break;
         case TG_SOURCE_BULK_FORCING: launch_cell_s<MODE, NS, GT, 2>(c, alpha, last, q, Rout); break;
+        case TG_SOURCE_DEVICE: launch_cell_s<MODE, NS, GT, 3>(c, alpha, last, q, Rout); break;
         default: launch_cell_s<MODE, NS, GT, 0>(c, alpha, last, q, Rout); break;
     }
 }
@@ -1205,6 +1340,26 @@ static int launch_cell(tg_ctx *c, double alpha, int last, double *q, double *Rou
 // boundary pass, gradient + limiter, face fluxes: everything of a residual before the gather
 static int run_fluxes(tg_ctx *c, double *q, bool masked = false)
 {
+    for (size_t b = 0; b < c->bd_kernel.size(); b++) {
+        if (!c->bd_kernel[b] && c->bcenter) {
+            int kind = 0;
+            CU(cudaMemcpy(&kind, c->bkind + b, sizeof(int), cudaMemcpyDeviceToHost));
+            if (kind == TG_BC_CUSTOM)
+                return fail(TG_ERR_INVALID, "custom boundary %d has no device function (tg_bind_boundary_function)",
+                            (int)b);
+        }
+    }
+    if (c->source == TG_SOURCE_DEVICE) {
+        if (!c->src_kernel)
+            return fail(TG_ERR_INVALID, "the device source has no function (tg_bind_source_function)");
+        // the source of every cell from the state being differentiated, added by the cell gather
+        Launch l(c, TG_PROF_CELL);
+        int C = c->s.C;
+        long N = c->s.N;
+        const double *qc = q;
+        void *args[] = {&C, &c->ccenter, &qc, &N, &c->dprop, &c->t_time, &c->t_step, &c->t_coef, &c->t_host, &c->S};
+        CU(cudaLaunchKernel(c->src_kernel, dim3((C + 127) / 128), dim3(128), args, 0, c->stream));
+    }
     if (c->source == TG_SOURCE_BULK_FORCING) {
         // the Prepare pass: volume averages of the state being differentiated, per instance
         Launch l(c, TG_PROF_REDUCE);
@@ -1280,8 +1435,8 @@ static void residual_of(tg_ctx *c, int i, double *out)
 
 extern "C" int tg_derivative(tg_ctx *c, const double *prim, double *deriv, double time)
 {
-    (void)time;  // device boundary conditions do not depend on time
     if (!c || !deriv) return fail(TG_ERR_INVALID, "null argument");
+    c->t_time = c->t_step = nullptr, c->t_host = time;  // time reaches the device functions only
     if (c->ninst != 1) return fail(TG_ERR_INVALID, "tg_derivative takes a single-mesh context");
     double *q = c->q;
     if (prim) {  // evaluate a host-given state in scratch memory; the resident state stays as it is
@@ -1304,8 +1459,8 @@ extern "C" int tg_derivative(tg_ctx *c, const double *prim, double *deriv, doubl
 
 extern "C" int tg_gradient(tg_ctx *c, double time, int limited, double *gradient)
 {
-    (void)time;
     if (!c || !gradient) return fail(TG_ERR_INVALID, "null argument");
+    c->t_time = c->t_step = nullptr, c->t_host = time;  // for custom boundaries
     if (c->order != 2) return fail(TG_ERR_INVALID, "gradients exist only at space order 2");
     TRY(run_boundary(c, c->q));
     int lim = limited ? c->limiter : TG_LIMITER_NONE;
@@ -1391,6 +1546,8 @@ static int enqueue_explicit_step(tg_ctx *c, int stages, const double *alpha, dou
     }
     CU(cudaGetLastError());
     for (int i = 0; i < stages; i++) {
+        // the residual of stage i at time + alpha_i step (advance.c:100)
+        c->t_time = c->st.time, c->t_step = c->st.step, c->t_coef = alpha[i];
         TRY(run_fluxes(c, c->q, true));
         TRY(launch_cell<1>(c, alpha[i + 1], i == stages - 1, c->q, c->R));
     }
@@ -1690,6 +1847,8 @@ static int gm_count(tg_ctx *c, int which, int *out)
 // derivative of a primitive state q (boundary rows refreshed) into Rout
 static int gm_derivative(tg_ctx *c, double *q, double *Rout)
 {
+    // implicit Euler evaluates every residual at the end of the step, time + step (advance.c:144)
+    c->t_time = c->st.time, c->t_step = c->st.step, c->t_coef = 1.0;
     TRY(run_fluxes(c, q));
     TRY(launch_cell<0>(c, 0.0, 0, q, Rout));
     return TG_OK;

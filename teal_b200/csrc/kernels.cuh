@@ -26,10 +26,14 @@ __global__ void k_boundary(Sizes s, const int2 *__restrict__ lr, const double *_
         return;
     }
     int e = bface_ent[i];
+    const int kind = bkind[e];
+    if (kind == BC_CUSTOM) {  // written by the boundary's device function
+        return;
+    }
     Prim<double> in = load_prim<double>(q, s.N, c.x);
     Basis<double> b = load_basis(basis, s.F, f);
     Prim<double> ctx = prim_from(bctx + 5 * e);
-    Prim<double> out = boundary_state(bkind[e], in, ctx, gamma, b);
+    Prim<double> out = boundary_state(kind, in, ctx, gamma, b);
     store_prim(q, s.N, c.y, out);
 }
 
@@ -204,7 +208,7 @@ struct Props {
 // time scale; avg = per-instance volume average of the primitive state being differentiated)
 struct Source {
     double p[4];
-    const double *avg;  // [ninst][5]
+    const double *avg;  // [ninst][5] volume averages (bulk forcing), or [5][C] values (device source)
 };
 
 // R += S(q) as teal's finalize_derivative adds source[j] to -sum / V (derivative.c:260-265)
@@ -313,7 +317,14 @@ __global__ void __launch_bounds__(CELL_BLOCK, CELL_MINB) k_cell(Sizes s, const i
             r[v] = -acc[v] / vol;
         }
     }
-    if (SRC != 0) {
+    if (SRC == 3) {
+        // device source function: its values for this residual, [5][C] (derivative.c:262)
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+            r[v] += src.avg[(size_t)v * C + c];
+        }
+    }
+    else if (SRC != 0) {
         // the state being differentiated (plain loads: this kernel writes q afterwards)
         Prim<double> qc{q[c], v3(q[N + c], q[2 * N + c], q[3 * N + c]), q[4 * N + c]};
         add_source<SRC>(src, qc, __ldg(seg.cell_inst + c), r);

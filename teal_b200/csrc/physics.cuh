@@ -575,7 +575,8 @@ enum BcKind {
     BC_SUBSONIC_OUTFLOW = 5,
     BC_PRESSURE_OUTFLOW = 6,
     BC_FARFIELD = 7,
-    BC_ADIABATIC_WALL = 8
+    BC_ADIABATIC_WALL = 8,
+    BC_CUSTOM = 9  // a device function writes the ghost rows
 };
 
 // characteristic far-field state (boundary.c:134-271)
