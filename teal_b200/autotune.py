@@ -38,6 +38,9 @@ CELL_BLOCKS = [256]
 CELL_SHAPES = [(256, 1), (128, 8), (128, 12), (64, 24)]
 # then gradient blocks (160 threads) resident per SM: 9 leaves the registers free, 12 caps them at 32
 GRAD_MINB = [9, 12]
+# last, on the ramp: resident face threads per SM of the Euler face kernel (fewer registers than the
+# Navier-Stokes one needs)
+EULER_FACE_THREADS = [640, 768, 896, 1024]
 
 TIMER = r"""
 import json, math, sys, time
@@ -112,7 +115,8 @@ def write_header(path, best):
              "// time wins.",
              "#pragma once", ""]
     notes = {"TG_FACE_BLOCK": "threads per face-flux block",
-             "TG_FACE_MINB": "face-flux blocks kept resident per SM (caps registers per thread)",
+             "TG_FACE_MINB": "Navier-Stokes face-flux blocks kept resident per SM (caps registers per thread)",
+             "TG_FACE_MINB_EULER": "Euler face-flux blocks kept resident per SM (caps registers per thread)",
              "TG_CELL_BLOCK": "threads per cell-gather block",
              "TG_CELL_MINB": "cell-gather blocks kept resident per SM (caps registers per thread)",
              "TG_FACE_STAGED_NS": "Navier-Stokes face kernel: geometry staged by bulk copies (1) or loaded (0)",
@@ -165,6 +169,8 @@ def main():
         ms, best = sweep(grads, "tgv", args.n, work, per)
         euler = [dict(best, TG_FACE_STAGED_EULER=st) for st in STAGED]
         ms_e, best = sweep(euler, "ramp", args.ramp_n, work, per)
+        occ = [dict(best, TG_FACE_MINB_EULER=t // best["TG_FACE_BLOCK"]) for t in EULER_FACE_THREADS]
+        ms_e, best = sweep(occ, "ramp", args.ramp_n, work, per)
     write_header(os.path.join(CSRC, "tuned.h"), best)
     if args.out:
         write_header(args.out, best)

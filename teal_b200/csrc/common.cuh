@@ -15,6 +15,12 @@ enum DeviceError { ERR_NONFINITE = 1, ERR_TIMEOUT = 2 };
 constexpr int BLOCK = 256;
 constexpr int FACE_BLOCK = TG_FACE_BLOCK;
 constexpr int FACE_MINB = TG_FACE_MINB;
+constexpr int FACE_MINB_EULER = TG_FACE_MINB_EULER;
+// resident face blocks per SM: Navier-Stokes (more registers: the viscous flux) or Euler
+__host__ __device__ constexpr int face_minb(bool ns)
+{
+    return ns ? FACE_MINB : FACE_MINB_EULER;
+}
 constexpr int CELL_BLOCK = TG_CELL_BLOCK;
 constexpr int CELL_MINB = TG_CELL_MINB;
 constexpr int GRAD_MINB = TG_GRAD_MINB;
