@@ -117,6 +117,7 @@ def write_header(path, best):
     notes = {"TG_FACE_BLOCK": "threads per face-flux block",
              "TG_FACE_MINB": "Navier-Stokes face-flux blocks kept resident per SM (caps registers per thread)",
              "TG_FACE_MINB_EULER": "Euler face-flux blocks kept resident per SM (caps registers per thread)",
+             "TG_FACE_MINB_FP32": "FP32-flux face-flux blocks kept resident per SM (caps registers per thread)",
              "TG_CELL_BLOCK": "threads per cell-gather block",
              "TG_CELL_MINB": "cell-gather blocks kept resident per SM (caps registers per thread)",
              "TG_FACE_STAGED_NS": "Navier-Stokes face kernel: geometry staged by bulk copies (1) or loaded (0)",

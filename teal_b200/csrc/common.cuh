@@ -16,10 +16,13 @@ constexpr int BLOCK = 256;
 constexpr int FACE_BLOCK = TG_FACE_BLOCK;
 constexpr int FACE_MINB = TG_FACE_MINB;
 constexpr int FACE_MINB_EULER = TG_FACE_MINB_EULER;
-// resident face blocks per SM: Navier-Stokes (more registers: the viscous flux) or Euler
+constexpr int FACE_MINB_FP32 = TG_FACE_MINB_FP32;
+// resident face blocks per SM: FP64 Navier-Stokes (more registers: the viscous flux), FP64 Euler,
+// or the FP32-flux form
+template <typename R>
 __host__ __device__ constexpr int face_minb(bool ns)
 {
-    return ns ? FACE_MINB : FACE_MINB_EULER;
+    return sizeof(R) == sizeof(float) ? FACE_MINB_FP32 : ns ? FACE_MINB : FACE_MINB_EULER;
 }
 constexpr int CELL_BLOCK = TG_CELL_BLOCK;
 constexpr int CELL_MINB = TG_CELL_MINB;

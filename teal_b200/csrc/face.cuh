@@ -228,7 +228,7 @@ __device__ __forceinline__ void face_flux(const Geo &geo, int i, int f, const Si
 // One thread per face, geometry loaded by the threads. face_minb caps the registers so that
 // several blocks stay resident per SM.
 template <typename R, int FK, bool NS, int ORDER, bool FOLD>
-__global__ void __launch_bounds__(FACE_BLOCK, face_minb(NS)) k_face(Sizes s, Geometry<R> g, const double *__restrict__ q,
+__global__ void __launch_bounds__(FACE_BLOCK, face_minb<R>(NS)) k_face(Sizes s, Geometry<R> g, const double *__restrict__ q,
                                                    const R *__restrict__ rec, R gamma, R mu, R prandtl,
                                                    R *__restrict__ G)
 {
@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(FACE_BLOCK, face_minb(NS)) k_face(Sizes s, Geo
 // before the threads (one face each) start. A wait that gives up sets ERR_TIMEOUT in the error
 // word and ends the block.
 template <typename R, int FK, bool NS, int ORDER, bool FOLD>
-__global__ void __launch_bounds__(FACE_BLOCK, face_minb(NS)) k_face_staged(Sizes s, Geometry<R> g,
+__global__ void __launch_bounds__(FACE_BLOCK, face_minb<R>(NS)) k_face_staged(Sizes s, Geometry<R> g,
                                                           const double *__restrict__ q,
                                                           const R *__restrict__ rec, R gamma, R mu,
                                                           R prandtl, R *__restrict__ G, int *err)

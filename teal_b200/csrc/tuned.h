@@ -3,8 +3,8 @@
 // for the Euler staging switch and the Euler face occupancy; times within 0.5 % of the fastest
 // count as ties, resolved to fewer resident face blocks, i.e. more registers per thread). From the
 // later sweeps: cell 0.113 vs 0.133 ms per TGV 128^3 launch, gradient 0.264 vs 0.280 ms, Euler face
-// 0.271 ms at 28 blocks against 0.290 at 24 and 0.318 at 20 (ramp 80^3). A value given with -D at
-// build time wins.
+// 0.271 ms at 28 blocks against 0.290 at 24 and 0.318 at 20 (ramp 80^3), FP32-flux face 0.309 ms at
+// 32 blocks against 0.326 at 20 (TGV 128^3). A value given with -D at build time wins.
 #pragma once
 
 #ifndef TG_FACE_BLOCK
@@ -12,6 +12,9 @@
 #endif
 #ifndef TG_FACE_MINB
 #define TG_FACE_MINB 20  // Navier-Stokes face-flux blocks kept resident per SM (caps registers per thread)
+#endif
+#ifndef TG_FACE_MINB_FP32
+#define TG_FACE_MINB_FP32 32  // FP32-flux face-flux blocks kept resident per SM (caps registers per thread)
 #endif
 #ifndef TG_FACE_MINB_EULER
 #define TG_FACE_MINB_EULER 28  // Euler face-flux blocks kept resident per SM (caps registers per thread)
