@@ -194,11 +194,11 @@ __device__ __forceinline__ void face_flux(const Geo &geo, int i, int f, const Si
             }
         }
         V3<R> unit = geo.corr(i);
-        R norm = geo.corr_norm(i);
+        R inv_norm = R(1) / geo.corr_norm(i);
 #pragma unroll
         for (int v = 0; v < 5; v++) {
             V3<R> gv = v3(gm[3 * v], gm[3 * v + 1], gm[3 * v + 2]);
-            R adjust = dot(gv, unit) - ((qrv[v] - qlv[v]) / norm);
+            R adjust = dot(gv, unit) - ((qrv[v] - qlv[v]) * inv_norm);
             gv = sub(gv, mul(adjust, unit));
             gm[3 * v] = gv.x;
             gm[3 * v + 1] = gv.y;

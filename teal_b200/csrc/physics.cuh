@@ -146,7 +146,7 @@ __device__ __forceinline__ Local<R> make_local(const Prim<R> &g, R gamma, const 
     s.u = to_local(b, g.u);
     s.p = g.p;
     s.m = mul(s.rho, s.u);
-    s.e = (s.p / (gamma - R(1))) + (dot(s.m, s.u) / R(2));
+    s.e = (s.p * (R(1) / (gamma - R(1)))) + (dot(s.m, s.u) / R(2));
     return s;
 }
 
@@ -185,8 +185,9 @@ template <typename R>
 __device__ __forceinline__ Cons<R> flux_roe(const Local<R> &l, const Local<R> &r, R gamma)
 {
     R gm1 = gamma - R(1);
-    R hl = (l.e + l.p) / l.rho;
-    R hr = (r.e + r.p) / r.rho;
+    const R il = R(1) / l.rho, ir = R(1) / r.rho;
+    R hl = (l.e + l.p) * il;
+    R hr = (r.e + r.p) * ir;
     R sl = sqrt(l.rho);
     R sr = sqrt(r.rho);
     R w = R(1) / (sl + sr);
@@ -198,8 +199,8 @@ __device__ __forceinline__ Cons<R> flux_roe(const Local<R> &l, const Local<R> &r
 
     R eig[3] = {u.x - a, u.x, u.x + a};
     {
-        R al = sqrt(gamma * l.p / l.rho);
-        R ar = sqrt(gamma * r.p / r.rho);
+        R al = sqrt((gamma * l.p) * il);
+        R ar = sqrt((gamma * r.p) * ir);
         R el[3] = {l.u.x - al, l.u.x, l.u.x + al};
         R er[3] = {r.u.x - ar, r.u.x, r.u.x + ar};
 #pragma unroll
@@ -270,8 +271,9 @@ template <typename R>
 __device__ __forceinline__ void einfeldt_speeds(const Local<R> &l, const Local<R> &r, R gamma,
                                                 R &sl_out, R &sr_out)
 {
-    R hl = (l.e + l.p) / l.rho;
-    R hr = (r.e + r.p) / r.rho;
+    const R il = R(1) / l.rho, ir = R(1) / r.rho;
+    R hl = (l.e + l.p) * il;
+    R hr = (r.e + r.p) * ir;
     R sl = sqrt(l.rho);
     R sr = sqrt(r.rho);
     R w = R(1) / (sl + sr);
@@ -279,8 +281,8 @@ __device__ __forceinline__ void einfeldt_speeds(const Local<R> &l, const Local<R
     R h = w * ((sl * hl) + (sr * hr));
     R u2 = dot(u, u);
     R a = sqrt((gamma - R(1)) * (h - (u2 / R(2))));
-    R al = sqrt(gamma * l.p / l.rho);
-    R ar = sqrt(gamma * r.p / r.rho);
+    R al = sqrt((gamma * l.p) * il);
+    R ar = sqrt((gamma * r.p) * ir);
     sl_out = fmin(l.u.x - al, u.x - a);
     sr_out = fmax(r.u.x + ar, u.x + a);
 }
@@ -346,8 +348,8 @@ __device__ __forceinline__ Cons<R> flux_hlle(const Local<R> &l, const Local<R> &
     R sr = sqrt(r.rho);
     R w = R(1) / (sl + sr);
     R ux = w * ((sl * l.u.x) + (sr * r.u.x));
-    R a2l = gamma * l.p / l.rho;
-    R a2r = gamma * r.p / r.rho;
+    R a2l = (gamma * l.p) * (R(1) / l.rho);
+    R a2r = (gamma * r.p) * (R(1) / r.rho);
     R al = sqrt(a2l);
     R ar = sqrt(a2r);
     R a2 = w * ((sl * a2l) + (sr * a2r));
@@ -371,14 +373,16 @@ template <typename R, bool DV>
 __device__ __forceinline__ void ausm_split(const Local<R> &l, const Local<R> &r, R gamma, R &vpl,
                                            R &ppl, R &vmr, R &pmr)
 {
-    R al = sqrt(gamma * l.p / l.rho);
-    R ar = sqrt(gamma * r.p / r.rho);
+    const R il = R(1) / l.rho, ir = R(1) / r.rho;
+    R al = sqrt((gamma * l.p) * il);
+    R ar = sqrt((gamma * r.p) * ir);
     R a = fmax(al, ar);
-    R pdl = l.p / l.rho;
-    R pdr = r.p / r.rho;
+    const R ia = R(1) / a;
+    R pdl = l.p * il;
+    R pdr = r.p * ir;
     R pds = pdl + pdr;
-    R ml = l.u.x / a;
-    R mr = r.u.x / a;
+    R ml = l.u.x * ia;
+    R mr = r.u.x * ia;
     if (fabs(l.u.x) <= a) {
         R alpha = R(2) * pdl / pds;
         R f = l.u.x + a;
@@ -412,8 +416,8 @@ __device__ __forceinline__ Cons<R> flux_ausmd(const Local<R> &l, const Local<R> 
     R mf = (vpl * l.rho) + (vmr * r.rho);
     R amf = fabs(mf);
     R pf = ppl + pmr;
-    R hl = (l.e + l.p) / l.rho;
-    R hr = (r.e + r.p) / r.rho;
+    R hl = (l.e + l.p) * (R(1) / l.rho);
+    R hr = (r.e + r.p) * (R(1) / r.rho);
     Cons<R> f;
     f.rho = mf;
     f.m.x = (((mf * (l.u.x + r.u.x)) - (amf * (r.u.x - l.u.x))) / R(2)) + pf;
@@ -437,8 +441,8 @@ __device__ __forceinline__ Cons<R> flux_ausmdv(const Local<R> &l, const Local<R>
     R pmin = fmin(l.p, r.p);
     R sw = fmin(R(1) / R(2), fmin(R(1), (R(10) * fabs(r.p - l.p)) / pmin));
     R nm = (((R(1) + sw) * nv) + ((R(1) - sw) * nd)) / R(2);
-    R hl = (l.e + l.p) / l.rho;
-    R hr = (r.e + r.p) / r.rho;
+    R hl = (l.e + l.p) * (R(1) / l.rho);
+    R hr = (r.e + r.p) * (R(1) / r.rho);
     Cons<R> f;
     f.rho = mf;
     f.m.x = nm + pf;
@@ -542,9 +546,10 @@ __device__ __forceinline__ Cons<R> viscous_central(const Prim<R> &q, const Grad<
                                                    R mu, R prandtl, const Basis<R> &b)
 {
     R div_u = (g.ux.x + g.uy.y) + g.uz.z;
-    R txx = R(2) * mu * (g.ux.x - (div_u / R(3)));
-    R tyy = R(2) * mu * (g.uy.y - (div_u / R(3)));
-    R tzz = R(2) * mu * (g.uz.z - (div_u / R(3)));
+    const R div3 = div_u * (R(1) / R(3));
+    R txx = R(2) * mu * (g.ux.x - div3);
+    R tyy = R(2) * mu * (g.uy.y - div3);
+    R tzz = R(2) * mu * (g.uz.z - div3);
     R txy = mu * (g.ux.y + g.uy.x);
     R txz = mu * (g.ux.z + g.uz.x);
     R tyz = mu * (g.uy.z + g.uz.y);
