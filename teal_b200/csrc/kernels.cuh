@@ -311,10 +311,10 @@ __global__ void __launch_bounds__(CELL_BLOCK, CELL_MINB) k_cell(Sizes s, const i
                 }
             }
         }
-        double vol = __ldg(cd.volume + c);
+        const double ivol = 1.0 / __ldg(cd.volume + c);  // one reciprocal for the five components
 #pragma unroll
         for (int v = 0; v < 5; v++) {
-            r[v] = -acc[v] / vol;
+            r[v] = -acc[v] * ivol;
         }
     }
     if (SRC == 3) {

@@ -86,19 +86,24 @@ __device__ __forceinline__ Prim<R> cons_to_prim(const Cons<R> &c, R gamma)
 {
     Prim<R> q;
     q.rho = fmax(R(1e-8), c.rho);
-    q.u = div(c.m, q.rho);
+    q.u = mul(R(1) / q.rho, c.m);  // one reciprocal for the three velocities
     q.p = fmax(R(1e-8), (gamma - R(1)) * (c.e - (dot(c.m, q.u) / R(2))));
     return q;
 }
 
-// primitive -> conserved (src/euler/create.c:34-44)
+// a product the compiler may not fuse into a following addition: the same bits in every kernel
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+
+// primitive -> conserved (src/euler/create.c:34-44); several kernels form U0 with it (the step's
+// last stage, the preparation of a loaded state), which must agree bit for bit
 template <typename R>
 __device__ __forceinline__ Cons<R> prim_to_cons(const Prim<R> &q, R gamma)
 {
     Cons<R> c;
     c.rho = q.rho;
     c.m = mul(c.rho, q.u);
-    c.e = (q.p / (gamma - R(1))) + (dot(c.m, q.u) / R(2));
+    c.e = mul_rn(q.p, R(1) / (gamma - R(1))) + (dot(c.m, q.u) / R(2));
     return c;
 }
 
