@@ -220,9 +220,10 @@ __device__ __forceinline__ Cons<R> flux_roe(const Local<R> &l, const Local<R> &r
     R ws[5];
     ws[2] = j.m.y - (u.y * j.rho);
     ws[3] = j.m.z - (u.z * j.rho);
-    ws[1] = gm1 / a2 *
+    const R ia = R(1) / a;  // one reciprocal for the two quotients by a and a^2
+    ws[1] = (gm1 * (ia * ia)) *
             (((((j.rho * (h - (u.x * u.x))) + (u.x * j.m.x)) - j.e) + (ws[2] * u.y)) + (ws[3] * u.z));
-    ws[0] = (((j.rho * (u.x + a)) - j.m.x) - (a * ws[1])) / (R(2) * a);
+    ws[0] = (((j.rho * (u.x + a)) - j.m.x) - (a * ws[1])) * (ia / R(2));
     ws[4] = j.rho - (ws[0] + ws[1]);
 
     R ch[5] = {ws[0] * eig[0], ws[1] * eig[1], ws[2] * eig[1], ws[3] * eig[1], ws[4] * eig[2]};
@@ -386,13 +387,14 @@ __device__ __forceinline__ void ausm_split(const Local<R> &l, const Local<R> &r,
     R pdl = l.p * il;
     R pdr = r.p * ir;
     R pds = pdl + pdr;
+    const R ips = R(1) / pds;
     R ml = l.u.x * ia;
     R mr = r.u.x * ia;
     if (fabs(l.u.x) <= a) {
-        R alpha = R(2) * pdl / pds;
+        R alpha = (R(2) * pdl) * ips;
         R f = l.u.x + a;
-        vpl = ((alpha * (f * f)) / (R(4) * a)) + (((R(1) - alpha) * (l.u.x + fabs(l.u.x))) / R(2));
-        ppl = ((l.p * (f * f)) / (R(4) * (a * a))) * (R(2) - ml);
+        vpl = ((alpha * (f * f)) * (ia / R(4))) + (((R(1) - alpha) * (l.u.x + fabs(l.u.x))) / R(2));
+        ppl = ((l.p * (f * f)) * ((ia * ia) / R(4))) * (R(2) - ml);
     }
     else {
         vpl = (l.u.x + fabs(l.u.x)) / R(2);
@@ -400,10 +402,10 @@ __device__ __forceinline__ void ausm_split(const Local<R> &l, const Local<R> &r,
                  : (((l.p * (l.u.x + fabs(l.u.x))) / R(2)) / l.u.x);
     }
     if (fabs(r.u.x) <= a) {
-        R alpha = R(2) * pdr / pds;
+        R alpha = (R(2) * pdr) * ips;
         R f = r.u.x - a;
-        vmr = ((-alpha * (f * f)) / (R(4) * a)) + (((R(1) - alpha) * (r.u.x - fabs(r.u.x))) / R(2));
-        pmr = ((r.p * (f * f)) / (R(4) * (a * a))) * (R(2) + mr);
+        vmr = ((-alpha * (f * f)) * (ia / R(4))) + (((R(1) - alpha) * (r.u.x - fabs(r.u.x))) / R(2));
+        pmr = ((r.p * (f * f)) * ((ia * ia) / R(4))) * (R(2) + mr);
     }
     else {
         vmr = (r.u.x - fabs(r.u.x)) / R(2);
