@@ -134,7 +134,7 @@ __global__ void __launch_bounds__(GRAD_THREADS, GRAD_MINB) k_gradient(Sizes s, G
     //                    (d1 (d1 + 2 d2) + eps2) / (d1 (d1 + d2) + 2 d2^2 + eps2), every term >= 0.
     // In FP64 the running minimum stays a fraction compared by cross multiplication and is divided
     // once: one division per thread instead of one or two per face, within a few ulps of teal's
-    // per-face quotients. FP32 divides per face (its products could underflow), approximately.
+    // per-face quotients. FP32 divides per face (its products could underflow).
     R psi = R(1);
     if (LIM != 0) {
         const R e2 = (LIM == 2) ? R(__ldg(eps2 + c)) : R(0);
@@ -163,10 +163,7 @@ __global__ void __launch_bounds__(GRAD_THREADS, GRAD_MINB) k_gradient(Sizes s, G
                         }
                     }
                     else {
-                        // the FP32 form's candidates: an approximate quotient (x * rcp(y), two
-                        // ulps), well inside the form's 1e-6 accuracy (it reads 0 for den beyond
-                        // 2^126, where the FP32 fluxes would have overflowed already)
-                        psi = fmin(psi, __fdividef(num, den));
+                        psi = fmin(psi, num / den);
                     }
                 }
             }
