@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cfloat>
+#include <type_traits>
 
 #include "device.cuh"
 #include "tuned.h"
@@ -51,6 +52,32 @@ __device__ __forceinline__ void store_prim(double *__restrict__ q, int ld, int i
     q[3 * ld + i] = p.u.z;
     q[4 * ld + i] = p.p;
 }
+
+// The state of cell i with the pressure taken relative to pref (in FP64, then converted)
+template <typename R>
+__device__ __forceinline__ Prim<R> load_prim_rel(const double *__restrict__ q, int ld, int i, double pref)
+{
+    Prim<R> p;
+    p.rho = R(__ldg(q + i));
+    p.u = v3(R(__ldg(q + ld + i)), R(__ldg(q + 2 * ld + i)), R(__ldg(q + 3 * ld + i)));
+    p.p = R(__ldg(q + 4 * ld + i) - pref);
+    return p;
+}
+
+// no reference pressure (FP64 kernels)
+struct NoPressureRef {
+};
+
+// Reference pressure of the FP32-flux form, per instance (null: none)
+struct PressureRef {
+    const double *pref;     // [ninst]
+    const int *cell_inst;   // [C]
+    __device__ __forceinline__ double of(int c) const { return pref ? __ldg(pref + __ldg(cell_inst + c)) : 0.0; }
+};
+
+// the reference-pressure argument of a face kernel in precision R
+template <typename R>
+using PressureRefOf = typename std::conditional<sizeof(R) == sizeof(float), PressureRef, NoPressureRef>::type;
 
 template <typename R>
 __device__ __forceinline__ Basis<R> load_basis(const R *__restrict__ b, int ld, int f)

@@ -255,6 +255,8 @@ struct tg_ctx {
     double *bcenter = nullptr;  // [F_bd - F_in][3] ghost cell centres of the boundary faces
     double *ccenter = nullptr;  // [C][3] cell centres (device source)
     double *S = nullptr;        // [5][C] device source values of the residual being evaluated
+    double *pref = nullptr;     // [ninst] reference pressure of the FP32-flux form (Local::dp)
+    std::vector<double> h_pref; // its host copy (the source of each upload stays alive)
     double *dprop = nullptr;    // [3] properties
     const void *src_kernel = nullptr;
     // time of the residual being evaluated: time[0] + coef * step[0] on the device (inside step
@@ -311,7 +313,7 @@ static void free_ctx(tg_ctx *c)
         cudaEventDestroy(p.second.second);
     }
     if (c->graph) cudaGraphExecDestroy(c->graph);
-    void *ptrs[] = {c->bcenter, c->ccenter, c->S, c->dprop,
+    void *ptrs[] = {c->bcenter, c->ccenter, c->S, c->dprop, c->pref,
                     c->lr, c->slot_nbr, c->slot_face, c->slot_cnt, c->owner, c->bface_ent, c->bkind, c->bctx,
                     c->volume, c->proj, c->eps2, c->gb.area, c->gb.basis, c->gb.offl, c->gb.offr, c->gb.corr,
                     c->gb.slot_w, c->gb.slot_off, c->gb.area32, c->gb.basis32, c->gb.offl32, c->gb.offr32,
@@ -892,6 +894,11 @@ static int create_ctx(MeshInput &in, const tg_equations *e, int precision, tg_ct
         }
         CU(cudaMalloc(&c->G, FLUX_REC * rsz * s.F));
         TRY(dalloc(&c->dtc, s.C));
+        if (precision == TG_PRECISION_FP32_FLUX) {
+            TRY(dalloc(&c->pref, c->ninst));
+            CU(cudaMemsetAsync(c->pref, 0, sizeof(double) * c->ninst, st));
+            c->h_pref.assign(c->ninst, 0.0);
+        }
         CU(cudaMemsetAsync(c->dtc, 0, sizeof(double) * s.C, st));
         TRY(dalloc(&c->part_min, c->npieces));
         TRY(dalloc(&c->part_sum, 5 * (size_t)c->npieces));
@@ -1133,6 +1140,13 @@ static int set_rows(tg_ctx *c, int inst, const double *prim, double *q)
     TRY(h2d(c, c->aos, prim, 5 * (size_t)n));
     k_rows_aos_to_soa<<<grid_of(n), BLOCK, 0, c->stream>>>(n, row0, c->s.N, c->aos, q);
     CU(cudaGetLastError());
+    if (q == c->q && c->pref && n > 0) {
+        // the FP32-flux form's reference pressure: the instance's first cell (any constant cancels
+        // over closed cells; a representative one keeps the relative pressures small)
+        double p0 = prim[4];
+        c->h_pref[inst] = std::isfinite(p0) ? p0 : 0.0;
+        CU(cudaMemcpyAsync(c->pref + inst, &c->h_pref[inst], sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    }
     return TG_OK;
 }
 
@@ -1275,6 +1289,7 @@ static int run_face(tg_ctx *c, const double *q)
     a.prandtl = c->prop[2];
     a.G = c->G;
     a.err = c->st.error;
+    a.pr_ref = PressureRef{c->precision == TG_PRECISION_FP32_FLUX ? c->pref : nullptr, c->cell_inst};
     bool ns = c->viscous == TG_VISCOUS_CENTRAL;
     bool fold = fold_psi(c);
     Launch l(c, TG_PROF_FACE);

@@ -132,11 +132,18 @@ struct FaceTile {
 // gradient re-reads the unlimited gradients, which are still in L1).
 template <typename R, int FK, bool NS, int ORDER, bool FOLD, typename Geo>
 __device__ __forceinline__ void face_flux(const Geo &geo, int i, int f, const Sizes &s, const double *__restrict__ q,
-                                          const R *__restrict__ rec, R gamma, R mu, R prandtl, R *__restrict__ G)
+                                          const R *__restrict__ rec, R gamma, R mu, R prandtl, R *__restrict__ G,
+                                          const PressureRefOf<R> &pr_ref)
 {
     const int N = s.N;
     const bool boundary = (f >= s.F_in) && (f < s.F_bd);
     const int2 c = geo.cells(i);
+    // FP32 fluxes work with the pressure relative to the instance's reference (Local::dp); the
+    // difference is taken in FP64, before the rounding to FP32
+    double pref = 0.0;
+    if constexpr (sizeof(R) == sizeof(float)) {
+        pref = pr_ref.of(c.x);
+    }
 
     // convective flux: the basis and the cell states are dead while the flux runs in the face frame
     // and are re-read afterwards
@@ -144,12 +151,19 @@ __device__ __forceinline__ void face_flux(const Geo &geo, int i, int f, const Si
     if (FK != FK_NONE) {
         Local<R> l, r;
         {
-            Prim<R> ql = load_prim<R>(q, N, c.x);
-            Prim<R> qr = load_prim<R>(q, N, c.y);
+            Prim<R> ql, qr;
+            if constexpr (sizeof(R) == sizeof(float)) {
+                ql = load_prim_rel<R>(q, N, c.x, pref);
+                qr = load_prim_rel<R>(q, N, c.y, pref);
+            }
+            else {
+                ql = load_prim<R>(q, N, c.x);
+                qr = load_prim<R>(q, N, c.y);
+            }
             Basis<R> b = geo.basis(i);
             if (ORDER == 1) {
-                l = make_local(ql, gamma, b);
-                r = make_local(qr, gamma, b);
+                l = make_local(ql, gamma, b, R(pref));
+                r = make_local(qr, gamma, b, R(pref));
             }
             else {
                 R pl[5], pr[5];
@@ -160,8 +174,8 @@ __device__ __forceinline__ void face_flux(const Geo &geo, int i, int f, const Si
                 else {
                     reconstruct<R, FOLD>(qr, rec, c.y, geo.offr(i), pr);
                 }
-                l = make_local(prim_from(pl), gamma, b);
-                r = make_local(prim_from(pr), gamma, b);
+                l = make_local(prim_from(pl), gamma, b, R(pref));
+                r = make_local(prim_from(pr), gamma, b, R(pref));
             }
         }
         fc = convective_flux_local<FK>(l, r, gamma);
@@ -230,14 +244,14 @@ __device__ __forceinline__ void face_flux(const Geo &geo, int i, int f, const Si
 template <typename R, int FK, bool NS, int ORDER, bool FOLD>
 __global__ void __launch_bounds__(FACE_BLOCK, face_minb<R>(NS)) k_face(Sizes s, Geometry<R> g, const double *__restrict__ q,
                                                    const R *__restrict__ rec, R gamma, R mu, R prandtl,
-                                                   R *__restrict__ G)
+                                                   R *__restrict__ G, PressureRefOf<R> pr_ref)
 {
     const int f = blockIdx.x * FACE_BLOCK + threadIdx.x;
     if (f >= s.F) {
         return;
     }
     DirectGeo<R> geo{g, s.F, f};
-    face_flux<R, FK, NS, ORDER, FOLD>(geo, 0, f, s, q, rec, gamma, mu, prandtl, G);
+    face_flux<R, FK, NS, ORDER, FOLD>(geo, 0, f, s, q, rec, gamma, mu, prandtl, G, pr_ref);
 }
 
 // One tile of FACE_BLOCK faces per block, its geometry staged in shared memory by bulk copies
@@ -247,7 +261,8 @@ template <typename R, int FK, bool NS, int ORDER, bool FOLD>
 __global__ void __launch_bounds__(FACE_BLOCK, face_minb<R>(NS)) k_face_staged(Sizes s, Geometry<R> g,
                                                           const double *__restrict__ q,
                                                           const R *__restrict__ rec, R gamma, R mu,
-                                                          R prandtl, R *__restrict__ G, int *err)
+                                                          R prandtl, R *__restrict__ G, int *err,
+                                                          PressureRefOf<R> pr_ref)
 {
     __shared__ __align__(16) FaceTile<R, ORDER, NS> t;
     const int f0 = blockIdx.x * FACE_BLOCK;
@@ -256,7 +271,8 @@ __global__ void __launch_bounds__(FACE_BLOCK, face_minb<R>(NS)) k_face_staged(Si
         return;
     }
     if (threadIdx.x < n) {
-        face_flux<R, FK, NS, ORDER, FOLD>(t, threadIdx.x, f0 + threadIdx.x, s, q, rec, gamma, mu, prandtl, G);
+        face_flux<R, FK, NS, ORDER, FOLD>(t, threadIdx.x, f0 + threadIdx.x, s, q, rec, gamma, mu, prandtl, G,
+                                          pr_ref);
     }
 }
 

@@ -16,6 +16,7 @@ struct FaceLaunch {
     double gamma, mu, prandtl;
     void *G;
     int *err;  // device error word (bounded waits that give up set ERR_TIMEOUT)
+    PressureRef pr_ref;  // FP32-flux form: reference pressure per instance
 };
 
 template <typename R, int FK, bool NS, int ORDER, bool FOLD>
@@ -23,11 +24,16 @@ inline void launch_face_v(bool staged, const FaceLaunch &a, const Geometry<R> &g
 {
     dim3 grid((a.s.F + FACE_BLOCK - 1) / FACE_BLOCK);
     R gm = R(a.gamma), mu = R(a.mu), pr = R(a.prandtl);
+    PressureRefOf<R> pref{};
+    if constexpr (sizeof(R) == sizeof(float)) {
+        pref = a.pr_ref;
+    }
     if (staged) {
-        k_face_staged<R, FK, NS, ORDER, FOLD><<<grid, FACE_BLOCK, 0, st>>>(a.s, g, a.q, rec, gm, mu, pr, G, a.err);
+        k_face_staged<R, FK, NS, ORDER, FOLD>
+            <<<grid, FACE_BLOCK, 0, st>>>(a.s, g, a.q, rec, gm, mu, pr, G, a.err, pref);
     }
     else {
-        k_face<R, FK, NS, ORDER, FOLD><<<grid, FACE_BLOCK, 0, st>>>(a.s, g, a.q, rec, gm, mu, pr, G);
+        k_face<R, FK, NS, ORDER, FOLD><<<grid, FACE_BLOCK, 0, st>>>(a.s, g, a.q, rec, gm, mu, pr, G, pref);
     }
 }
 

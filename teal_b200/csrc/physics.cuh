@@ -134,8 +134,22 @@ __device__ __forceinline__ R navierstokes_timestep(const Prim<R> &q, R gamma, R 
 // ---- convective fluxes (src/euler/convective.c) ------------------------------------------------
 
 // state in the face frame (convective.c:7-25 `Euler`, global_to_local)
+// FP32 fluxes: pressure and energy relative to a reference pressure p_ref, dp = p - p_ref and
+// de = dp / (gamma - 1) + rho |u|^2 / 2. The normal momentum flux carries dp and the state jumps use
+// de, which shifts every face's momentum flux by the constant -p_ref n A; that cancels over each
+// closed cell in exact arithmetic, while FP32 no longer rounds p_ref (~1/(gamma Ma^2)) into the
+// cancelling fluxes (the FP32-flux form of low-Mach flows). FP64 fluxes use p and e themselves.
 template <typename R>
-struct Local {
+struct LocalRel {
+    R dp;
+    R de;
+};
+template <>
+struct LocalRel<double> {
+};
+
+template <typename R>
+struct Local : LocalRel<R> {
     R rho;
     V3<R> u;
     R p;
@@ -143,15 +157,27 @@ struct Local {
     R e;
 };
 
+// g.p is the pressure relative to pref (FP32-flux form) or the pressure itself (pref = 0)
 template <typename R>
-__device__ __forceinline__ Local<R> make_local(const Prim<R> &g, R gamma, const Basis<R> &b)
+__device__ __forceinline__ Local<R> make_local(const Prim<R> &g, R gamma, const Basis<R> &b, R pref = R(0))
 {
     Local<R> s;
     s.rho = g.rho;
     s.u = to_local(b, g.u);
-    s.p = g.p;
-    s.m = mul(s.rho, s.u);
-    s.e = (s.p * (R(1) / (gamma - R(1)))) + (dot(s.m, s.u) / R(2));
+    if constexpr (sizeof(R) == sizeof(double)) {  // FP64: no reference pressure
+        (void)pref;
+        s.p = g.p;
+        s.m = mul(s.rho, s.u);
+        s.e = (s.p * (R(1) / (gamma - R(1)))) + (dot(s.m, s.u) / R(2));
+    }
+    else {
+        s.dp = g.p;
+        s.p = g.p + pref;
+        s.m = mul(s.rho, s.u);
+        const R kinetic = dot(s.m, s.u) / R(2);
+        s.e = (s.p * (R(1) / (gamma - R(1)))) + kinetic;
+        s.de = (s.dp * (R(1) / (gamma - R(1)))) + kinetic;
+    }
     return s;
 }
 
@@ -161,7 +187,12 @@ __device__ __forceinline__ Cons<R> physical_flux(const Local<R> &s)
 {
     Cons<R> f;
     f.rho = s.m.x;
-    f.m.x = (s.m.x * s.u.x) + s.p;
+    if constexpr (sizeof(R) == sizeof(double)) {
+        f.m.x = (s.m.x * s.u.x) + s.p;
+    }
+    else {
+        f.m.x = (s.m.x * s.u.x) + s.dp;
+    }
     f.m.y = s.m.x * s.u.y;
     f.m.z = s.m.x * s.u.z;
     f.e = (s.e + s.p) * s.u.x;
@@ -174,7 +205,12 @@ __device__ __forceinline__ Cons<R> jump_of(const Local<R> &l, const Local<R> &r)
     Cons<R> j;
     j.rho = r.rho - l.rho;
     j.m = sub(r.m, l.m);
-    j.e = r.e - l.e;
+    if constexpr (sizeof(R) == sizeof(double)) {
+        j.e = r.e - l.e;
+    }
+    else {
+        j.e = r.de - l.de;
+    }
     return j;
 }
 
