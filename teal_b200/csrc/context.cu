@@ -252,6 +252,7 @@ struct tg_ctx {
     // device functions in place of teal's Compute callbacks (one-mesh contexts)
     std::vector<std::pair<int, int>> bd_range;  // boundary index -> teal face range [beg, end)
     std::vector<const void *> bd_kernel;        // boundary index -> bound kernel (custom kinds)
+    std::vector<int> bd_kind;                   // boundary index -> TG_BC_* (host copy)
     double *bcenter = nullptr;  // [F_bd - F_in][3] ghost cell centres of the boundary faces
     double *ccenter = nullptr;  // [C][3] cell centres (device source)
     double *S = nullptr;        // [5][C] device source values of the residual being evaluated
@@ -949,6 +950,7 @@ static int setup_functions(tg_ctx *c, const tg_mesh *m, const tg_equations *e)
     int nb = e->num_boundaries;
     c->bd_range.resize(nb);
     c->bd_kernel.assign(nb, nullptr);
+    c->bd_kind.assign(e->boundary_kind, e->boundary_kind + nb);
     bool custom = false;
     for (int i = 0; i < nb; i++) {
         int ent = m->num_inner_entities + i;
@@ -1000,9 +1002,8 @@ extern "C" int tg_bind_boundary_function(tg_ctx *c, int boundary, const char *na
     if (c->ninst != 1) return fail(TG_ERR_INVALID, "device functions need a one-mesh context");
     if (boundary < 0 || boundary >= (int)c->bd_range.size())
         return fail(TG_ERR_INVALID, "boundary %d out of range", boundary);
-    int kind = 0;
-    CU(cudaMemcpy(&kind, c->bkind + boundary, sizeof(int), cudaMemcpyDeviceToHost));
-    if (kind != TG_BC_CUSTOM) return fail(TG_ERR_INVALID, "boundary %d is not a custom boundary", boundary);
+    if (c->bd_kind[boundary] != TG_BC_CUSTOM)
+        return fail(TG_ERR_INVALID, "boundary %d is not a custom boundary", boundary);
     std::string error;
     const void *k = nullptr;
     int rc = function_kernel(name, FUNCTION_BOUNDARY, &k, error);
@@ -1356,13 +1357,9 @@ static int launch_cell(tg_ctx *c, double alpha, int last, double *q, double *Rou
 static int run_fluxes(tg_ctx *c, double *q, bool masked = false)
 {
     for (size_t b = 0; b < c->bd_kernel.size(); b++) {
-        if (!c->bd_kernel[b] && c->bcenter) {
-            int kind = 0;
-            CU(cudaMemcpy(&kind, c->bkind + b, sizeof(int), cudaMemcpyDeviceToHost));
-            if (kind == TG_BC_CUSTOM)
-                return fail(TG_ERR_INVALID, "custom boundary %d has no device function (tg_bind_boundary_function)",
-                            (int)b);
-        }
+        if (!c->bd_kernel[b] && c->bd_kind[b] == TG_BC_CUSTOM)
+            return fail(TG_ERR_INVALID, "custom boundary %d has no device function (tg_bind_boundary_function)",
+                        (int)b);
     }
     if (c->source == TG_SOURCE_DEVICE) {
         if (!c->src_kernel)

@@ -35,19 +35,14 @@ struct Nvrtc {
     decltype(&nvrtcDestroyProgram) destroy = nullptr;
 };
 
-// NVRTC of the CUDA installation, else whichever libnvrtc the loader finds
-const Nvrtc *nvrtc()
+void load_nvrtc(Nvrtc &n)
 {
-    static Nvrtc n;
-    static bool tried = false;
-    if (tried) return n.handle ? &n : nullptr;
-    tried = true;
     const char *paths[] = {"/usr/local/cuda/lib64/libnvrtc.so.12", "libnvrtc.so.12", "libnvrtc.so"};
     for (const char *p : paths) {
         n.handle = dlopen(p, RTLD_NOW | RTLD_LOCAL);
         if (n.handle) break;
     }
-    if (!n.handle) return nullptr;
+    if (!n.handle) return;
     n.create = (decltype(n.create))dlsym(n.handle, "nvrtcCreateProgram");
     n.compile = (decltype(n.compile))dlsym(n.handle, "nvrtcCompileProgram");
     n.log_size = (decltype(n.log_size))dlsym(n.handle, "nvrtcGetProgramLogSize");
@@ -58,9 +53,16 @@ const Nvrtc *nvrtc()
     if (!n.create || !n.compile || !n.log_size || !n.log || !n.cubin_size || !n.cubin || !n.destroy) {
         dlclose(n.handle);
         n.handle = nullptr;
-        return nullptr;
     }
-    return &n;
+}
+
+// NVRTC of the CUDA installation, else whichever libnvrtc the loader finds (looked up once)
+const Nvrtc *nvrtc()
+{
+    static Nvrtc n;
+    static std::once_flag once;
+    std::call_once(once, [] { load_nvrtc(n); });
+    return n.handle ? &n : nullptr;
 }
 
 struct Entry {
@@ -200,12 +202,8 @@ int function_register(const char *name, int kind, const char *source, char *log,
     rt->cubin(prog, e.cubin.data());
     rt->destroy(&prog);
     std::lock_guard<std::mutex> lock(registry_mutex);
-    auto &r = registry();
-    auto it = r.find(name);
-    if (it != r.end() && it->second.library) {
-        cudaLibraryUnload(it->second.library);
-    }
-    r[name] = std::move(e);
+    // a replaced function's code stays loaded: contexts bound to it keep launching its kernel
+    registry()[name] = std::move(e);
     return 0;
 }
 

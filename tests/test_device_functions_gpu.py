@@ -183,3 +183,24 @@ def test_batches_refuse_device_functions():
     _, de = inflow_channel()
     with pytest.raises(tb.TealError):
         tb.Batch([de])
+
+
+def test_reregistration_keeps_bound_code():
+    """A context keeps the code it was bound to; later bindings take the replacement."""
+    src = """
+__device__ void swap_src(double *source, const double *property, const double *center, double time,
+                         const double *state)
+{{ source[1] = {value}; }}
+"""
+    tb.register_function("swap_src", "source", src.format(value="1.0"))
+    _, de = inflow_channel()
+    de.set_source("device function", compute="swap_src")
+    prim = random_state(de.mesh.num_cells, seed=70, mach=0.8)
+    old_ctx = tb.Context(de.mesh, de)
+    d1 = old_ctx.derivative(prim)
+    tb.register_function("swap_src", "source", src.format(value="3.0"))
+    np.testing.assert_array_equal(old_ctx.derivative(prim), d1)
+    new_ctx = tb.Context(de.mesh, de)
+    d2 = new_ctx.derivative(prim)
+    np.testing.assert_allclose(d2[:, 1] - d1[:, 1], 2.0, rtol=0, atol=1e-9)
+    np.testing.assert_array_equal(d2[:, [0, 2, 3, 4]], d1[:, [0, 2, 3, 4]])
