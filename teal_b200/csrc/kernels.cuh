@@ -107,15 +107,20 @@ __global__ void __launch_bounds__(GRAD_THREADS, GRAD_MINB) k_gradient(Sizes s, G
     // on meshes of hexahedra only (not MIXED) every cell has MAX_SLOTS slots: the slot tests below
     // fold away
     const int cnt = MIXED ? s_cnt[l] : MAX_SLOTS;
+    // the warp's largest slot count: slots beyond it are skipped by the whole warp (a warp of
+    // tetrahedra stops after 4)
+    const int jmax = MIXED ? __reduce_max_sync(__activemask(), cnt) : MAX_SLOTS;
     double qn[MAX_SLOTS];
 #pragma unroll
     for (int j = 0; j < MAX_SLOTS; j++) {
+        if (j >= jmax) break;
         qn[j] = __ldg(qv + ((j < cnt) ? s_nbr[j][l] : c));
     }
     R gx = R(0), gy = R(0), gz = R(0);
     double mn = qc, mx = qc;
 #pragma unroll
     for (int j = 0; j < MAX_SLOTS; j++) {
+        if (j >= jmax) break;
         if (j < cnt) {
             R d = R(qn[j] - qc);
             gx += d * s_w[0 * MAX_SLOTS + j][l];
@@ -142,6 +147,7 @@ __global__ void __launch_bounds__(GRAD_THREADS, GRAD_MINB) k_gradient(Sizes s, G
         R best_n = R(1), best_d = R(1);
 #pragma unroll
         for (int j = 0; j < MAX_SLOTS; j++) {
+            if (j >= jmax) break;
             if (j < cnt) {
                 R d2 = ((gx * s_off[0 * MAX_SLOTS + j][l]) + (gy * s_off[1 * MAX_SLOTS + j][l])) +
                        (gz * s_off[2 * MAX_SLOTS + j][l]);
