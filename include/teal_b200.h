@@ -284,6 +284,11 @@ int tg_host_mesh_view(const tg_host_mesh *mesh, tg_mesh *view);
 /* Entity names (teal's: "domain", "left", "right", ...) and their cell ranges. */
 int tg_host_mesh_entity(const tg_host_mesh *mesh, int index, const char **name, int *cell_beg,
                         int *cell_end);
+/* Nodes and cell node lists (pointers stay owned by the host mesh): coord [num_nodes][3], the node
+ * list of cell i at cell_node_idx[cell_node_off[i] .. cell_node_off[i + 1]) in teal's cell order
+ * (Gmsh node order), inner cells first; what teal's VTKHDF writer outputs (src/mesh/write.c). */
+int tg_host_mesh_nodes(const tg_host_mesh *mesh, int *num_nodes, const double **coord,
+                       const int **cell_node_off, const int **cell_node_idx);
 int tg_host_mesh_destroy(tg_host_mesh *mesh);
 
 /* ---- measurement -------------------------------------------------------------------------------

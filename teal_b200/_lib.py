@@ -147,6 +147,8 @@ SIGNATURES = [
     ("tg_host_mesh_view", ctypes.c_int, [_vp, ctypes.POINTER(TgMesh)]),
     ("tg_host_mesh_entity", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), _int_p,
                                            _int_p]),
+    ("tg_host_mesh_nodes", ctypes.c_int, [_vp, _int_p, ctypes.POINTER(_dbl_p), ctypes.POINTER(_int_p),
+                                          ctypes.POINTER(_int_p)]),
     ("tg_host_mesh_destroy", ctypes.c_int, [_vp]),
     ("tg_profile", ctypes.c_int, [_vp, ctypes.c_int]),
     ("tg_profile_read", ctypes.c_int, [_vp, _vp, _vp]),

@@ -910,6 +910,17 @@ extern "C" int tg_host_mesh_entity(const tg_host_mesh *m, int index, const char 
     return TG_OK;
 }
 
+extern "C" int tg_host_mesh_nodes(const tg_host_mesh *m, int *num_nodes, const double **coord,
+                                  const int **cell_node_off, const int **cell_node_idx)
+{
+    if (!m || !num_nodes || !coord || !cell_node_off || !cell_node_idx) return TG_ERR_INVALID;
+    *num_nodes = (int)m->coord.size();
+    *coord = m->coord.empty() ? nullptr : &m->coord[0].x;
+    *cell_node_off = m->node_off.data();
+    *cell_node_idx = m->node_idx.data();
+    return TG_OK;
+}
+
 extern "C" int tg_host_mesh_destroy(tg_host_mesh *m)
 {
     delete m;

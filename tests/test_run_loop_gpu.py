@@ -111,3 +111,21 @@ def test_runs_are_deterministic():
         ctx.close()
     assert out[0][0] == out[1][0]
     assert np.array_equal(out[0][1], out[1][1]) and np.array_equal(out[0][2], out[1][2])
+
+
+def test_run_writes_vtu_at_output_points(tmp_path):
+    from teal_b200 import output
+
+    _, e = vortex_pair()
+    sim = tb.Simulation(e)
+    sim.set_max_iter(4)
+    sim.set_out_iter(2)
+    prefix = os.path.join(tmp_path, "vortex")
+    sim.run(prefix=prefix, vtu=True)
+    names = sorted(f for f in os.listdir(tmp_path) if f.endswith(".vtu"))
+    assert names == [f"vortex_{i:05d}.vtu" for i in range(3)]
+    d = output.read_vtu(os.path.join(tmp_path, names[-1]))
+    C = e.mesh.num_inner_cells
+    np.testing.assert_array_equal(d["density"], e.primitive[:C, 0])
+    np.testing.assert_array_equal(d["pressure"], e.primitive[:C, 4])
+    assert d["time"][0] > 0
