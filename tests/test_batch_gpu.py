@@ -62,6 +62,23 @@ def test_batch_instances_are_bit_identical_to_solo_runs():
         assert np.array_equal(got, p1)  # ghost rows too
 
 
+def test_batch_fp32_flux_instances_are_bit_identical_to_solo_runs():
+    """The FP32-flux form too: each instance's reference pressure is its own (its first cell), the
+    same in the arena as alone."""
+    fp32 = tb.TG_PRECISION_FP32_FLUX
+    ps = problems()
+    steps = [6, 4, 5, 3]
+    b = tb.Batch(ps, precision=fp32)
+    t, it, res = b.run(tb.TG_ADVANCE_LSERK, 0.5, steps, context=(3, 3))
+    for i, e in enumerate(ps):
+        ctx = tb.Context(e.mesh, e, precision=fp32)
+        ctx.set_primitive(e.primitive)
+        t1, it1, res1 = ctx.run(tb.TG_ADVANCE_LSERK, 0.5, steps[i], context=(3, 3))
+        assert t[i] == t1
+        assert np.array_equal(res[i], res1)
+        assert np.array_equal(b.get_primitive(i), ctx.get_primitive())
+
+
 def test_batch_stops_each_instance_on_its_own_limits():
     ps = problems()
     b = tb.Batch(ps)
