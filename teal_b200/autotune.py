@@ -7,7 +7,7 @@ per build, selected with TEAL_B200_LIBRARY), and writes the fastest shape to
 teal_b200/csrc/tuned.h (and to --out when given). Shapes and the Navier-Stokes staging switch are
 tuned on the Taylor-Green vortex, the Euler staging switch on the unstructured ramp.
 
-    python -m teal_b200.autotune [--n 96] [--ramp-n 64] [--steps 10] [--precision fp64] [--out gpurun_out/tuned.h]
+    python -m teal_b200.autotune [--n 96] [--ramp-n 64] [--steps 10] [--precision fp64] [--out tuned_candidate.h]
 
 Needs nvcc and a GPU. Every candidate computes the same results; only speed differs.
 """
