@@ -4,9 +4,11 @@
 // Floating-point expressions keep teal's evaluation order; this file is compiled without
 // floating-point contraction so the geometry is bit-identical to teal's (-std=c99) build.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/teal_b200.h"
@@ -32,6 +34,41 @@ inline Vec vcross(Vec a, Vec b)
 inline bool is_close(double a, double b)  // src/core/utils.c:29-34
 {
     return std::fabs(a - b) <= std::fmax(1e-8, 1e-5 * std::fmax(std::fabs(a), std::fabs(b)));
+}
+
+// Host threads for the loops of mesh generation whose iterations are independent: every element
+// gets the same arithmetic as in a serial loop, so results do not depend on the split.
+
+// parts for n items: at most 16 and the host's cores, at least 32768 items each
+int num_parts(int n)
+{
+    unsigned hw = std::thread::hardware_concurrency();
+    return std::max(1, std::min<int>(hw ? (int)hw : 1, std::min(16, n / 32768)));
+}
+
+// body(p) for p in [0, parts), part 0 on the calling thread
+template <class Body>
+void run_parts(int parts, const Body &body)
+{
+    std::vector<std::thread> pool;
+    for (int p = 1; p < parts; p++) {
+        try {
+            pool.emplace_back([&body, p] { body(p); });
+        }
+        catch (...) {
+            body(p);  // no thread to be had: this part runs here
+        }
+    }
+    body(0);
+    for (auto &th : pool) th.join();
+}
+
+// body(beg, end) over [0, n) in contiguous chunks
+template <class Body>
+void parallel_for(int n, const Body &body)
+{
+    int parts = num_parts(n), chunk = (n + parts - 1) / parts;
+    run_parts(parts, [&](int p) { body(std::min(n, p * chunk), std::min(n, (p + 1) * chunk)); });
 }
 
 struct Entity {
@@ -297,30 +334,42 @@ void connect_cells(tg_host_mesh &m)
     for (int e = 0; e < ne; e++)
         for (int k = eoff[e]; k < eoff[e + 1]; k++) nind[cur[eind[k]]++] = e;
 
-    std::vector<int> mark(ne, 0), nbrs;
+    // each cell's neighbour list depends only on the node lists: chunks of cells are listed
+    // independently and concatenated in cell order
     m.cell_off.assign(ne + 1, 0);
-    m.cell_idx.clear();
-    for (int e = 0; e < ne; e++) {
-        nbrs.clear();
-        int len_e = eoff[e + 1] - eoff[e];
-        for (int k = eoff[e]; k < eoff[e + 1]; k++) {
-            int v = eind[k];
-            for (int t = noff[v]; t < noff[v + 1]; t++) {
-                int o = nind[t];
-                if (o == e) continue;
-                if (mark[o] == 0) nbrs.push_back(o);
-                mark[o]++;
+    int parts = num_parts(ne), chunk = (ne + parts - 1) / parts;
+    std::vector<std::vector<int>> part(parts);
+    run_parts(parts, [&](int p) {
+        std::vector<int> mark(ne, 0), nbrs;
+        std::vector<int> &out = part[p];
+        for (int e = p * chunk; e < std::min(ne, (p + 1) * chunk); e++) {
+            nbrs.clear();
+            int len_e = eoff[e + 1] - eoff[e];
+            for (int k = eoff[e]; k < eoff[e + 1]; k++) {
+                int v = eind[k];
+                for (int t = noff[v]; t < noff[v + 1]; t++) {
+                    int o = nind[t];
+                    if (o == e) continue;
+                    if (mark[o] == 0) nbrs.push_back(o);
+                    mark[o]++;
+                }
             }
+            for (int o : nbrs) {
+                int overlap = mark[o];
+                int len_o = eoff[o + 1] - eoff[o];
+                bool adj = overlap >= 3 || overlap >= len_e - 1 || overlap >= len_o - 1;
+                // inner cells keep every neighbour, face cells only their inner neighbour
+                if (adj && (e < m.num_inner || o < m.num_inner)) out.push_back(o);
+                mark[o] = 0;
+            }
+            m.cell_off[e + 1] = (int)out.size();  // within the part; offset below
         }
-        for (int o : nbrs) {
-            int overlap = mark[o];
-            int len_o = eoff[o + 1] - eoff[o];
-            bool adj = overlap >= 3 || overlap >= len_e - 1 || overlap >= len_o - 1;
-            // inner cells keep every neighbour, face cells only their inner neighbour
-            if (adj && (e < m.num_inner || o < m.num_inner)) m.cell_idx.push_back(o);
-            mark[o] = 0;
-        }
-        m.cell_off[e + 1] = (int)m.cell_idx.size();
+    });
+    m.cell_idx.clear();
+    for (int p = 0; p < parts; p++) {
+        int base = (int)m.cell_idx.size();
+        for (int e = p * chunk; e < std::min(ne, (p + 1) * chunk); e++) m.cell_off[e + 1] += base;
+        m.cell_idx.insert(m.cell_idx.end(), part[p].begin(), part[p].end());
     }
 }
 
@@ -424,37 +473,57 @@ bool correct_face_node_order(Face &f, const tg_host_mesh &m)
 
 int create_faces(tg_host_mesh &m)  // generate.c:267-321
 {
-    std::vector<Face> faces;
-    faces.reserve((size_t)m.num_inner * 3 + (size_t)(m.num_cells - m.num_inner));
-    for (int i = 0; i < m.num_inner; i++) {
-        for (int j = m.cell_off[i]; j < m.cell_off[i + 1]; j++) {
-            int l = i, r = m.cell_idx[j];
-            if (l < r) {
-                Face f{};
-                f.inner = r < m.num_inner;
-                f.left = l;
-                f.right = r;
-                for (int a = m.node_off[l]; a < m.node_off[l + 1]; a++)
-                    for (int b = m.node_off[r]; b < m.node_off[r + 1]; b++)
-                        if (m.node_idx[a] == m.node_idx[b]) {
-                            if (f.num_nodes >= 4) return TG_ERR_INVALID;
-                            f.node[f.num_nodes++] = m.node_idx[a];
-                        }
-                if (f.num_nodes < 3) return TG_ERR_INVALID;
-                if (!correct_face_node_order(f, m)) return TG_ERR_INVALID;
-                faces.push_back(f);
+    // the faces of chunks of inner cells, built independently and concatenated in cell order
+    int parts = num_parts(m.num_inner), chunk = (m.num_inner + parts - 1) / parts;
+    std::vector<std::vector<Face>> part(parts);
+    std::vector<char> bad(parts, 0);
+    run_parts(parts, [&](int p) {
+        int beg = std::min(m.num_inner, p * chunk), end = std::min(m.num_inner, (p + 1) * chunk);
+        part[p].reserve((size_t)(end - beg) * 3);
+        for (int i = beg; i < end && !bad[p]; i++) {
+            for (int j = m.cell_off[i]; j < m.cell_off[i + 1]; j++) {
+                int l = i, r = m.cell_idx[j];
+                if (l < r) {
+                    Face f{};
+                    f.inner = r < m.num_inner;
+                    f.left = l;
+                    f.right = r;
+                    for (int a = m.node_off[l]; a < m.node_off[l + 1]; a++)
+                        for (int b = m.node_off[r]; b < m.node_off[r + 1]; b++)
+                            if (m.node_idx[a] == m.node_idx[b]) {
+                                if (f.num_nodes >= 4) bad[p] = 1;
+                                else f.node[f.num_nodes++] = m.node_idx[a];
+                            }
+                    if (bad[p] || f.num_nodes < 3 || !correct_face_node_order(f, m)) {
+                        bad[p] = 1;
+                        break;
+                    }
+                    part[p].push_back(f);
+                }
             }
         }
-    }
-    std::stable_sort(faces.begin(), faces.end(), [](const Face &a, const Face &b) {
-        if (a.inner != b.inner) return a.inner > b.inner;
-        if (a.inner) return a.left < b.left;
-        return a.right < b.right;
     });
+    std::vector<Face> faces;
+    size_t total = 0;
+    for (int p = 0; p < parts; p++) {
+        if (bad[p]) return TG_ERR_INVALID;
+        total += part[p].size();
+    }
+    faces.reserve(total);
+    for (int p = 0; p < parts; p++) {
+        faces.insert(faces.end(), part[p].begin(), part[p].end());
+        std::vector<Face>().swap(part[p]);
+    }
+    // teal's order: inner faces by left cell, then the others by right cell, ties in creation order
+    // (a stable sort). Faces are created by ascending left cell, so the inner ones already stand in
+    // that order and only the (few) others need sorting.
+    auto outer = std::stable_partition(faces.begin(), faces.end(), [](const Face &f) { return f.inner != 0; });
+    std::stable_sort(outer, faces.end(), [](const Face &a, const Face &b) { return a.right < b.right; });
     int F = (int)faces.size();
     m.num_faces = F;
     m.fnode_off.assign(F + 1, 0);
     m.fnode_idx.clear();
+    m.fnode_idx.reserve(4 * (size_t)F);
     m.face_cell.resize(2 * (size_t)F);
     int ni = 0, nb = 0;
     for (int i = 0; i < F; i++) {
@@ -573,7 +642,7 @@ Vec cell_center(const Vec *c, int n)  // generate.c:517-557
     return vdiv(vadd(mm[0], mm[1]), v[0] + v[1]);
 }
 
-void geometry(tg_host_mesh &m)
+int geometry(tg_host_mesh &m)
 {
     int F = m.num_faces;
     auto fcoords = [&](int f, Vec *c) {
@@ -585,58 +654,59 @@ void geometry(tg_host_mesh &m)
     m.area.resize(F);
     m.fcenter.resize(F);
     m.basis.resize(9 * (size_t)F);
-    for (int f = 0; f < F; f++) {
-        Vec c[4];
-        int n = fcoords(f, c);
-        m.area[f] = face_area(c, n);
-        m.fcenter[f] = face_center(c, n);
-    }
-    for (int f = 0; f < F; f++) {
-        Vec c[4];
-        int n = fcoords(f, c);
-        Vec nx = face_normal(c, n), ny, nz;
-        double nqz = std::hypot(nx.x, nx.y);
-        double nqy = std::hypot(nx.x, nx.z);
-        if (nqz > nqy) {
-            ny = {-nx.y / nqz, nx.x / nqz, 0};
-            nz = {(-nx.x * nx.z) / nqz, (-nx.y * nx.z) / nqz, nqz};
+    parallel_for(F, [&](int beg, int end) {
+        for (int f = beg; f < end; f++) {
+            Vec c[4];
+            int n = fcoords(f, c);
+            m.area[f] = face_area(c, n);
+            m.fcenter[f] = face_center(c, n);
         }
-        else {
-            ny = {(-nx.x * nx.y) / nqy, nqy, (-nx.y * nx.z) / nqy};
-            nz = {-nx.z / nqy, 0, nx.x / nqy};
+    });
+    parallel_for(F, [&](int beg, int end) {
+        for (int f = beg; f < end; f++) {
+            Vec c[4];
+            int n = fcoords(f, c);
+            Vec nx = face_normal(c, n), ny, nz;
+            double nqz = std::hypot(nx.x, nx.y);
+            double nqy = std::hypot(nx.x, nx.z);
+            if (nqz > nqy) {
+                ny = {-nx.y / nqz, nx.x / nqz, 0};
+                nz = {(-nx.x * nx.z) / nqz, (-nx.y * nx.z) / nqz, nqz};
+            }
+            else {
+                ny = {(-nx.x * nx.y) / nqy, nqy, (-nx.y * nx.z) / nqy};
+                nz = {-nx.z / nqy, 0, nx.x / nqy};
+            }
+            int left = m.face_cell[2 * f];
+            Vec mean = {0, 0, 0};
+            for (int j = m.node_off[left]; j < m.node_off[left + 1]; j++) mean = vadd(mean, m.coord[m.node_idx[j]]);
+            mean = vdiv(mean, (double)(m.node_off[left + 1] - m.node_off[left]));
+            if (vdot(vsub(mean, m.fcenter[f]), nx) > 0) {
+                nx = vmul(-1, nx);
+                ny = vmul(-1, ny);
+            }
+            double *b = &m.basis[9 * (size_t)f];
+            b[0] = nx.x, b[1] = nx.y, b[2] = nx.z;
+            b[3] = ny.x, b[4] = ny.y, b[5] = ny.z;
+            b[6] = nz.x, b[7] = nz.y, b[8] = nz.z;
         }
-        int left = m.face_cell[2 * f];
-        Vec mean = {0, 0, 0};
-        for (int j = m.node_off[left]; j < m.node_off[left + 1]; j++) mean = vadd(mean, m.coord[m.node_idx[j]]);
-        mean = vdiv(mean, (double)(m.node_off[left + 1] - m.node_off[left]));
-        if (vdot(vsub(mean, m.fcenter[f]), nx) > 0) {
-            nx = vmul(-1, nx);
-            ny = vmul(-1, ny);
-        }
-        double *b = &m.basis[9 * (size_t)f];
-        b[0] = nx.x, b[1] = nx.y, b[2] = nx.z;
-        b[3] = ny.x, b[4] = ny.y, b[5] = ny.z;
-        b[6] = nz.x, b[7] = nz.y, b[8] = nz.z;
-    }
+    });
     auto normal = [&](int f) { return Vec{m.basis[9 * (size_t)f], m.basis[9 * (size_t)f + 1], m.basis[9 * (size_t)f + 2]}; };
 
     // cell volumes and centres (generate.c:496-630)
     m.volume.assign(m.num_cells, 0.0);
     m.sum_volume = 0;
     m.center.assign(m.num_cells, Vec{0, 0, 0});
-    for (int i = 0; i < m.num_inner; i++) {
-        Vec c[8];
-        int n = 0;
-        for (int j = m.node_off[i]; j < m.node_off[i + 1]; j++) c[n++] = m.coord[m.node_idx[j]];
-        m.volume[i] = cell_volume(c, n);
-        m.sum_volume += m.volume[i];
-    }
-    for (int i = 0; i < m.num_inner; i++) {
-        Vec c[8];
-        int n = 0;
-        for (int j = m.node_off[i]; j < m.node_off[i + 1]; j++) c[n++] = m.coord[m.node_idx[j]];
-        m.center[i] = cell_center(c, n);
-    }
+    parallel_for(m.num_inner, [&](int beg, int end) {
+        for (int i = beg; i < end; i++) {
+            Vec c[8];
+            int n = 0;
+            for (int j = m.node_off[i]; j < m.node_off[i + 1]; j++) c[n++] = m.coord[m.node_idx[j]];
+            m.volume[i] = cell_volume(c, n);
+            m.center[i] = cell_center(c, n);
+        }
+    });
+    for (int i = 0; i < m.num_inner; i++) m.sum_volume += m.volume[i];  // in cell order
     for (int f = m.num_inner_faces; f < m.off_boundary_faces; f++) {  // mirrored boundary ghosts
         int l = m.face_cell[2 * f], r = m.face_cell[2 * f + 1];
         Vec nrm = normal(f);
@@ -679,30 +749,50 @@ void geometry(tg_host_mesh &m)
         if (r < m.num_inner) m.projection[r] = vadd(m.projection[r], inc);
     }
 
-    // cell offsets to the faces of each neighbour (generate.c:648-667)
-    struct Key {
-        int l, r, f;
-    };
-    std::vector<Key> keys(F);
-    for (int f = 0; f < F; f++) keys[f] = {m.face_cell[2 * f], m.face_cell[2 * f + 1], f};
-    std::sort(keys.begin(), keys.end(), [](const Key &a, const Key &b) {
-        return a.l != b.l ? a.l < b.l : a.r < b.r;
-    });
+    // cell offsets to the faces of each neighbour (generate.c:648-667). teal finds the face of the
+    // pair (min, max) by binary search over the faces sorted by cell pair; a pair has exactly one
+    // face (one per neighbour-list entry with left < right), so the face lists of each inner cell
+    // find the same face.
     int nnz = m.cell_off[m.num_inner];
     m.offset.assign(nnz, Vec{0, 0, 0});
-    for (int i = 0; i < m.num_inner; i++) {
-        for (int j = m.cell_off[i]; j < m.cell_off[i + 1]; j++) {
-            int o = m.cell_idx[j];
-            Key key{std::min(i, o), std::max(i, o), 0};
-            auto it = std::lower_bound(keys.begin(), keys.end(), key, [](const Key &a, const Key &b) {
-                return a.l != b.l ? a.l < b.l : a.r < b.r;
-            });
-            m.offset[j] = vsub(m.fcenter[it->f], m.center[i]);
+    int C = m.num_inner;
+    std::vector<int> cf_off(C + 1, 0), cf_idx;
+    for (int f = 0; f < F; f++) {
+        cf_off[m.face_cell[2 * f] + 1]++;
+        if (m.face_cell[2 * f + 1] < C) cf_off[m.face_cell[2 * f + 1] + 1]++;
+    }
+    for (int i = 0; i < C; i++) cf_off[i + 1] += cf_off[i];
+    cf_idx.resize(cf_off[C]);
+    {
+        std::vector<int> cur(cf_off.begin(), cf_off.end() - 1);
+        for (int f = 0; f < F; f++) {
+            cf_idx[cur[m.face_cell[2 * f]]++] = f;
+            if (m.face_cell[2 * f + 1] < C) cf_idx[cur[m.face_cell[2 * f + 1]]++] = f;
         }
     }
+    std::atomic<bool> missing{false};
+    parallel_for(C, [&](int beg, int end) {
+        for (int i = beg; i < end; i++) {
+            for (int j = m.cell_off[i]; j < m.cell_off[i + 1]; j++) {
+                int o = m.cell_idx[j], l = std::min(i, o), r = std::max(i, o), face = -1;
+                for (int k = cf_off[i]; k < cf_off[i + 1]; k++) {
+                    int f = cf_idx[k];
+                    if (m.face_cell[2 * f] == l && m.face_cell[2 * f + 1] == r) {
+                        face = f;
+                        break;
+                    }
+                }
+                if (face < 0) {
+                    missing.store(true, std::memory_order_relaxed);
+                    continue;
+                }
+                m.offset[j] = vsub(m.fcenter[face], m.center[i]);
+            }
+        }
+    });
+    if (missing.load()) return TG_ERR_INVALID;
 
     // least-squares weights (generate.c:669-752)
-    int C = m.num_inner;
     std::vector<double> r11(C, 0), r12(C, 0), r22(C, 0), r13(C, 0), r23(C, 0), r33(C, 0);
     for (int f = 0; f < F; f++) {
         int l = m.face_cell[2 * f], r = m.face_cell[2 * f + 1];
@@ -754,25 +844,28 @@ void geometry(tg_host_mesh &m)
     m.weight.assign(6 * (size_t)F, 0.0);
     m.foffset.resize(6 * (size_t)F);
     m.correction.resize(4 * (size_t)F);
-    for (int f = 0; f < F; f++) {
-        int l = m.face_cell[2 * f], r = m.face_cell[2 * f + 1];
-        Vec d = vsub(m.center[r], m.center[l]);
-        Vec wl = face_weight(d, l);
-        double *w = &m.weight[6 * (size_t)f];
-        w[0] = wl.x, w[1] = wl.y, w[2] = wl.z;
-        if (r < C) {
-            Vec wr = face_weight(vmul(-1, d), r);
-            w[3] = wr.x, w[4] = wr.y, w[5] = wr.z;
+    parallel_for(F, [&](int beg, int end) {
+        for (int f = beg; f < end; f++) {
+            int l = m.face_cell[2 * f], r = m.face_cell[2 * f + 1];
+            Vec d = vsub(m.center[r], m.center[l]);
+            Vec wl = face_weight(d, l);
+            double *w = &m.weight[6 * (size_t)f];
+            w[0] = wl.x, w[1] = wl.y, w[2] = wl.z;
+            if (r < C) {
+                Vec wr = face_weight(vmul(-1, d), r);
+                w[3] = wr.x, w[4] = wr.y, w[5] = wr.z;
+            }
+            // offsets and corrections (generate.c:754-777)
+            Vec ol = vsub(m.fcenter[f], m.center[l]), orr = vsub(m.fcenter[f], m.center[r]);
+            double *o = &m.foffset[6 * (size_t)f];
+            o[0] = ol.x, o[1] = ol.y, o[2] = ol.z, o[3] = orr.x, o[4] = orr.y, o[5] = orr.z;
+            double nrm = vnorm(d);
+            Vec unit = vdiv(d, nrm);
+            double *cr = &m.correction[4 * (size_t)f];
+            cr[0] = unit.x, cr[1] = unit.y, cr[2] = unit.z, cr[3] = nrm;
         }
-        // offsets and corrections (generate.c:754-777)
-        Vec ol = vsub(m.fcenter[f], m.center[l]), orr = vsub(m.fcenter[f], m.center[r]);
-        double *o = &m.foffset[6 * (size_t)f];
-        o[0] = ol.x, o[1] = ol.y, o[2] = ol.z, o[3] = orr.x, o[4] = orr.y, o[5] = orr.z;
-        double nrm = vnorm(d);
-        Vec unit = vdiv(d, nrm);
-        double *cr = &m.correction[4 * (size_t)f];
-        cr[0] = unit.x, cr[1] = unit.y, cr[2] = unit.z, cr[3] = nrm;
-    }
+    });
+    return TG_OK;
 }
 
 int generate(tg_host_mesh &m)
@@ -785,8 +878,7 @@ int generate(tg_host_mesh &m)
     reorder_nodes(m);
     int rc = create_faces(m);
     if (rc != TG_OK) return rc;
-    geometry(m);
-    return TG_OK;
+    return geometry(m);
 }
 
 }  // namespace

@@ -19,6 +19,7 @@ CASES = [
     ((0, 0, 0), (1, 1, 1), (8, 6, 5), (1, 0, 1)),                # walls in y
     ((0, 0, 0), (2, 1, 1), (12, 7, 1), (0, 0, 0)),               # 2D, all boundary
     ((-1, -2, 0), (3, 1, 0.5), (5, 4, 3), (0, 0, 0)),            # 3D, all boundary
+    ((0, 0, 0), (2 * np.pi,) * 3, (48, 48, 48), (1, 1, 1)),      # large enough for threaded geometry
 ]
 
 needs_ref = pytest.mark.skipif(not ref.available(), reason="reference oracle not built")
@@ -56,7 +57,8 @@ def test_mesh_invariants(case):
 
 
 RAMPS = [dict(n=(10, 8, 6), block=4, seed=1), dict(n=(16, 12, 10), block=4, seed=2),
-         dict(n=(20, 16, 12), block=8, seed=5)]
+         dict(n=(20, 16, 12), block=8, seed=5),
+         dict(n=(48, 40, 32), block=8, seed=9)]  # threaded geometry (more than 32768 cells per thread)
 
 
 @needs_ref
