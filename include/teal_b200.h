@@ -356,7 +356,8 @@ enum { TG_FUNCTION_BOUNDARY = 1, TG_FUNCTION_SOURCE = 2 };
  * properties (heat capacity ratio, then dynamic viscosity and Prandtl number for Navier-Stokes);
  * center = the ghost cell's centre (boundary) or the cell's centre (source), 3 doubles; time = the
  * time of the residual being evaluated (teal's stage time); context = the inner cell's primitive
- * state (boundary) or the cell's primitive state (source), 5 doubles. The function is compiled at
+ * state (boundary) or the cell's primitive state (source), 5 doubles; a source bound with
+ * TG_PREPARE_AVERAGE finds 5 more after them (tg_bind_source_prepare). The function is compiled at
  * once with NVRTC for sm_100a without FMA contraction (libnvrtc is loaded at run time, no device
  * needed); a compile error returns TG_ERR_INVALID with the compiler log in `log` (`log_size` bytes,
  * may be null). A second registration of a name replaces the first for later bindings. */
@@ -370,6 +371,15 @@ int tg_bind_boundary_function(tg_ctx *ctx, int boundary, const char *name);
 /* Use the registered source function `name` (tg_equations.source must be TG_SOURCE_DEVICE). One-mesh
  * contexts only. */
 int tg_bind_source_function(tg_ctx *ctx, const char *name);
+
+/* teal's source Prepare (src/equations.h:40-41, called before the source of every cell,
+ * src/equations/derivative.c:248-250) for a device source: TG_PREPARE_NONE (the default) or
+ * TG_PREPARE_AVERAGE, the pass of run/periodic_hill/run.c:8-11, equations_average over the inner
+ * cells (src/equations/average.c:8-40): the volume average of the primitive state being
+ * differentiated, sum of V_c q_c over the inner cells / their volume, summed in a fixed order. The
+ * source function reads it as context[5..9], after the cell's own state (zeros without it). */
+enum { TG_PREPARE_NONE = 0, TG_PREPARE_AVERAGE = 1 };
+int tg_bind_source_prepare(tg_ctx *ctx, int prepare);
 
 #ifdef __cplusplus
 }

@@ -28,6 +28,7 @@ TG_PRECISION_FP64, TG_PRECISION_FP32_FLUX = 0, 1
 TG_SOURCE_NONE, TG_SOURCE_BODY_FORCE, TG_SOURCE_BULK_FORCING, TG_SOURCE_DEVICE = 0, 1, 2, 3
 TG_BC_CUSTOM = 9
 TG_FUNCTION_BOUNDARY, TG_FUNCTION_SOURCE = 1, 2
+TG_PREPARE_NONE, TG_PREPARE_AVERAGE = 0, 1
 TG_NOALLOC_MAX_CELLS = 67108864  # cell limit of tg_residual_noalloc (its fixed scratch array)
 
 _int_p = ctypes.POINTER(ctypes.c_int)
@@ -159,6 +160,7 @@ SIGNATURES = [
                                             ctypes.c_long]),
     ("tg_bind_boundary_function", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_char_p]),
     ("tg_bind_source_function", ctypes.c_int, [_vp, ctypes.c_char_p]),
+    ("tg_bind_source_prepare", ctypes.c_int, [_vp, ctypes.c_int]),
     ("tg_build_info", ctypes.c_char_p, []),
 ]
 

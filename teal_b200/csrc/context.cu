@@ -260,6 +260,7 @@ struct tg_ctx {
     std::vector<double> h_pref; // its host copy (the source of each upload stays alive)
     double *dprop = nullptr;    // [3] properties
     const void *src_kernel = nullptr;
+    int src_prepare = TG_PREPARE_NONE;
     // time of the residual being evaluated: time[0] + coef * step[0] on the device (inside step
     // sequences), else host
     const double *t_time = nullptr, *t_step = nullptr;
@@ -1031,6 +1032,18 @@ extern "C" int tg_bind_source_function(tg_ctx *c, const char *name)
     return TG_OK;
 }
 
+extern "C" int tg_bind_source_prepare(tg_ctx *c, int prepare)
+{
+    if (!c) return fail(TG_ERR_INVALID, "null argument");
+    if (c->source != TG_SOURCE_DEVICE) return fail(TG_ERR_INVALID, "the equations' source is not a device function");
+    if (prepare != TG_PREPARE_NONE && prepare != TG_PREPARE_AVERAGE)
+        return fail(TG_ERR_INVALID, "unknown source prepare %d", prepare);
+    CU(cudaStreamSynchronize(c->stream));
+    c->src_prepare = prepare;
+    drop_graph(c);
+    return TG_OK;
+}
+
 extern "C" int tg_create(const tg_mesh *m, const tg_equations *e, int precision, tg_ctx **out)
 {
     if (!out) return fail(TG_ERR_INVALID, "null output pointer");
@@ -1361,23 +1374,27 @@ static int run_fluxes(tg_ctx *c, double *q, bool masked = false)
             return fail(TG_ERR_INVALID, "custom boundary %d has no device function (tg_bind_boundary_function)",
                         (int)b);
     }
-    if (c->source == TG_SOURCE_DEVICE) {
-        if (!c->src_kernel)
-            return fail(TG_ERR_INVALID, "the device source has no function (tg_bind_source_function)");
-        // the source of every cell from the state being differentiated, added by the cell gather
-        Launch l(c, TG_PROF_CELL);
-        int C = c->s.C;
-        long N = c->s.N;
-        const double *qc = q;
-        void *args[] = {&C, &c->ccenter, &qc, &N, &c->dprop, &c->t_time, &c->t_step, &c->t_coef, &c->t_host, &c->S};
-        CU(cudaLaunchKernel(c->src_kernel, dim3((C + 127) / 128), dim3(128), args, 0, c->stream));
-    }
-    if (c->source == TG_SOURCE_BULK_FORCING) {
+    bool prepare_average = c->source == TG_SOURCE_BULK_FORCING ||
+                           (c->source == TG_SOURCE_DEVICE && c->src_prepare == TG_PREPARE_AVERAGE);
+    if (c->source == TG_SOURCE_DEVICE && !c->src_kernel)
+        return fail(TG_ERR_INVALID, "the device source has no function (tg_bind_source_function)");
+    if (prepare_average) {
         // the Prepare pass: volume averages of the state being differentiated, per instance
         Launch l(c, TG_PROF_REDUCE);
         k_piece_average<<<c->npieces, BLOCK, 0, c->stream>>>(c->seg, c->s.N, q, c->volume, c->part_sum);
         k_inst_average<<<(c->ninst + 127) / 128, 128, 0, c->stream>>>(c->seg, c->part_sum, c->src_avg);
         CU(cudaGetLastError());
+    }
+    if (c->source == TG_SOURCE_DEVICE) {
+        // the source of every cell from the state being differentiated, added by the cell gather
+        Launch l(c, TG_PROF_CELL);
+        int C = c->s.C;
+        long N = c->s.N;
+        const double *qc = q;
+        const double *avg = prepare_average ? c->src_avg : nullptr;
+        void *args[] = {&C,         &c->ccenter, &qc,       &N,     &c->dprop, &c->t_time,
+                        &c->t_step, &c->t_coef,  &c->t_host, &c->S, &avg};
+        CU(cudaLaunchKernel(c->src_kernel, dim3((C + 127) / 128), dim3(128), args, 0, c->stream));
     }
     TRY(run_boundary(c, q, masked));
     if (c->order == 2) TRY(run_gradient(c, q));

@@ -93,8 +93,9 @@ bool valid_name(const char *name)
 // The wrapper kernels (the user's source comes first). Boundary: for the faces [f0, f0 + n) of one
 // boundary, outer = the ghost row as it stands (teal's Compute writes into it in place), context =
 // the inner cell's primitive state, center = the ghost cell's centre. Source: S[v][c] for every
-// inner cell, from a zeroed source vector. The stage time is time[0] + coef * step[0] on the device
-// inside step sequences, else host_time. A stopped instance (active[0] == 0) is left as it is.
+// inner cell, from a zeroed source vector; its context is the cell's state followed by the Prepare
+// pass's volume average (avg; zeros without one). The stage time is time[0] + coef * step[0] on the
+// device inside step sequences, else host_time. A stopped instance (active[0] == 0) is left as it is.
 const char *boundary_wrapper = R"(
 extern "C" __global__ void tg_function_kernel(int n, int f0, const int *lr, const double *center, double *q,
                                               long N, const double *property, const double *time,
@@ -124,15 +125,16 @@ const char *source_wrapper = R"(
 extern "C" __global__ void tg_function_kernel(int C, const double *center, const double *q, long N,
                                               const double *property, const double *time,
                                               const double *step, double coef, double host_time,
-                                              double *S)
+                                              double *S, const double *avg)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= C) {
         return;
     }
-    double state[5], s[5] = {0, 0, 0, 0, 0};
+    double state[10], s[5] = {0, 0, 0, 0, 0};
     for (int v = 0; v < 5; v++) {
         state[v] = q[v * N + c];
+        state[5 + v] = avg ? avg[v] : 0.0;
     }
     const double t = time ? time[0] + coef * step[0] : host_time;
     TG_USER_FUNCTION(s, property, center + 3 * (long)c, t, state);

@@ -40,3 +40,31 @@ __device__ void unsteady_source(double *source, const double *property, const do
     source[4] = (state[1] * fx) + (state[2] * fy);
 }
 """
+
+
+
+def hill_forcing(name="hill_forcing", tau="0.001"):
+    """The periodic hill's forcing (run/periodic_hill/run.c:13-21: target bulk velocity 1, time
+    scale 0.001) with its Prepare, the volume average of the state, read from context[5..9]."""
+    return """
+__device__ void NAME(double *source, const double *property, const double *center, double time,
+                     const double *context)
+{
+    const double *state = context, *average = context + 5;
+    double s1 = state[0] * (1.0 - average[1]) / TAU;
+    source[1] = s1;
+    source[4] = state[1] * s1;
+}
+""".replace("NAME", name).replace("TAU", tau)
+
+
+HILL_FORCING = hill_forcing()
+
+# writes the context's average slots into the source, to show what a source without Prepare sees
+AVERAGE_PROBE = """
+__device__ void average_probe(double *source, const double *property, const double *center, double time,
+                              const double *context)
+{
+    for (int k = 0; k < 5; k++) source[k] = context[5 + k];
+}
+"""

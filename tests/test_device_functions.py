@@ -8,13 +8,15 @@ import pytest
 
 import teal_b200 as tb
 from teal_b200 import _lib
-from tests.device_functions import MOVING_WALL, UNSTEADY_INFLOW, UNSTEADY_SOURCE
+from tests.device_functions import AVERAGE_PROBE, HILL_FORCING, MOVING_WALL, UNSTEADY_INFLOW, UNSTEADY_SOURCE
 
 
 def test_register_compiles():
     tb.register_function("lid_wall", "boundary", MOVING_WALL)
     tb.register_function("unsteady_inflow", "boundary", UNSTEADY_INFLOW)
     tb.register_function("unsteady_source", "source", UNSTEADY_SOURCE)
+    tb.register_function("hill_forcing", "source", HILL_FORCING)
+    tb.register_function("average_probe", "source", AVERAGE_PROBE)
 
 
 def test_compile_error_carries_the_log():
@@ -66,3 +68,12 @@ def test_equations_api_requires_a_function_for_custom_kinds():
     assert e.source_function == "unsteady_source"
     e.set_source(None)
     assert e.source is None and e.source_function is None
+
+    with pytest.raises(tb.TealError):
+        e.set_source("device function", compute="hill_forcing", prepare="sum")
+    with pytest.raises(tb.TealError):
+        e.set_source("bulk forcing", (1.0, 0.001), prepare="average")
+    e.set_source("device function", compute="hill_forcing", prepare="average")
+    assert e.source_prepare == "average"
+    e.set_source(None)
+    assert e.source_prepare is None

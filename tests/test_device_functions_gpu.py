@@ -14,7 +14,8 @@ import teal_b200 as tb
 from oracle import ref
 from teal_b200 import _lib
 from tests.cases import random_state, rel_l2
-from tests.device_functions import MOVING_WALL, UNSTEADY_INFLOW, UNSTEADY_SOURCE
+from tests.device_functions import (AVERAGE_PROBE, HILL_FORCING, MOVING_WALL, UNSTEADY_INFLOW, UNSTEADY_SOURCE,
+                                   hill_forcing)
 
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not ref.available(), reason="reference oracle not built")]
 
@@ -26,6 +27,9 @@ def registered():
     tb.register_function("lid_wall", "boundary", MOVING_WALL)
     tb.register_function("unsteady_inflow", "boundary", UNSTEADY_INFLOW)
     tb.register_function("unsteady_source", "source", UNSTEADY_SOURCE)
+    tb.register_function("hill_forcing", "source", HILL_FORCING)
+    tb.register_function("average_probe", "source", AVERAGE_PROBE)
+    tb.register_function("hill_forcing_mild", "source", hill_forcing("hill_forcing_mild", "1.0"))
 
 
 def run_both(re, de, prim, method, courant, steps, rk=None, nk=None):
@@ -204,3 +208,73 @@ __device__ void swap_src(double *source, const double *property, const double *c
     d2 = new_ctx.derivative(prim)
     np.testing.assert_allclose(d2[:, 1] - d1[:, 1], 2.0, rtol=0, atol=1e-9)
     np.testing.assert_array_equal(d2[:, [0, 2, 3, 4]], d1[:, [0, 2, 3, 4]])
+
+
+def hill_channel(tau=0.001):
+    """The periodic hill's walled channel (run/periodic_hill/run.c, coarse and without the hill):
+    teal's bulk forcing with its Prepare in the reference, the device function with the average
+    Prepare here (time scale 0.001 as in the run case, or 1)."""
+    lo, hi, n = (0, 0, 0), (9, 3, 0.3), (18, 10, 2)
+    rm = ref.RefMesh(lo, hi, n, (1, 0, 1))
+    re = ref.RefEquations(rm, True)
+    dm = tb.Mesh.create(lo, hi, n, (1, 0, 1))
+    de = tb.Equations.navierstokes(dm)
+    for e in (re, de):
+        e.set_convective_flux("roe")
+        e.set_limiter("venkatakrishnan", 1.0)
+        e.set_property("dynamic viscosity", 0.01)
+        e.set_boundary_condition("bottom", "wall")
+        e.set_boundary_condition("top", "wall")
+    re.set_source("bulk forcing", (1.0, tau))
+    de.set_source("device function", compute="hill_forcing" if tau == 0.001 else "hill_forcing_mild",
+                  prepare="average")
+    return re, de
+
+
+def test_prepare_average_matches_teals_prepare():
+    re, de = hill_channel()
+    prim = random_state(de.mesh.num_cells, seed=71, mach=0.4)
+    for time in (0.0, 0.5):
+        assert rel_l2(de.derivative(prim, time), re.derivative(prim, time)).max() <= TOL
+    (tr, rr, pr), (td, rd, pd) = run_both(re, de, prim, "lserk", 0.3, 5, rk=(3, 3))
+    assert rel_l2(pd, pr).max() <= TOL
+
+
+def test_prepare_average_implicit():
+    # the run case's time scale 0.001 makes the Newton systems stiff enough that the loose Krylov
+    # tolerance amplifies last-bit differences of the average (teal sums it serially, the device by
+    # pieces) above the implicit bar; time scale 1 keeps the systems as well conditioned as the
+    # other implicit parity cases
+    re, de = hill_channel(tau=1.0)
+    for e in (re, de):
+        e.set_limiter(None, 0.0)
+    prim = random_state(de.mesh.num_cells, seed=72, mach=0.4)
+    (tr, rr, pr), (td, rd, pd) = run_both(re, de, prim, "implicit euler", 2.0, 2, nk=(0.1, 0.3, 30))
+    assert rel_l2(pd, pr).max() <= 1e-7
+
+
+def test_prepare_average_values_and_default_zeros():
+    """context[5..9] holds the volume average of the primitive state with the average Prepare and
+    zeros without it; the source's conserved-variable residual contribution is S itself."""
+    _, de = inflow_channel()
+    prim = random_state(de.mesh.num_cells, seed=73, mach=0.8)
+    C = de.mesh.num_inner_cells
+    vol = np.asarray(de.mesh.cell_volume[:C])
+    want = (vol[:, None] * prim[:C]).sum(axis=0) / vol.sum()
+    base = de.derivative(prim)
+    de.set_source("device function", compute="average_probe")
+    assert np.array_equal(de.derivative(prim), base)
+    de.set_source("device function", compute="average_probe", prepare="average")
+    got = de.derivative(prim) - base
+    # got = (R + S) - R: exact up to the rounding of R + S
+    np.testing.assert_allclose(got, np.broadcast_to(want, got.shape), rtol=0,
+                               atol=1e-12 * (1 + np.abs(base).max()))
+
+
+def test_prepare_needs_a_device_source():
+    _, de = inflow_channel(source=True)
+    ctx = de.context()
+    assert _lib.lib.tg_bind_source_prepare(ctx.handle, 7) == _lib.TG_ERR_INVALID
+    _, de2 = inflow_channel()
+    ctx2 = de2.context()
+    assert _lib.lib.tg_bind_source_prepare(ctx2.handle, _lib.TG_PREPARE_AVERAGE) == _lib.TG_ERR_INVALID
