@@ -115,22 +115,28 @@ class ClockSampler:
         self.proc = None
         self.lines = []
         self.thread = None
+        self.first = threading.Event()
 
     def start(self):
+        """Start sampling every 100 ms and return once the first sample is in (at most 3 s), so the
+        timed region that follows is covered from its start."""
         q = "clocks.sm,clocks.max.sm," + ",".join(self.REASONS.values())
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200",
+                ["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "100",
                  "-i", str(self.index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except (OSError, ValueError):
             self.proc = None
             return
         self.thread = threading.Thread(target=self._read, daemon=True)
         self.thread.start()
+        self.first.wait(timeout=3.0)
 
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
+            self.first.set()
+        self.first.set()
 
     def stop(self):
         if not self.proc:
