@@ -556,7 +556,8 @@ def main():
     ap.add_argument("--rate", type=float, default=8.0, help="serve: arrivals per second")
     ap.add_argument("--max-active", type=int, default=8, help="serve: concurrent solves")
     ap.add_argument("--n", type=int, default=None, help="mesh cells per axis (tgv 128, ramp 80)")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "exact"],
+                    help="fp64: plain FP64; fp32: FP32-flux form; exact: FP64 with teal's exact arithmetic")
     ap.add_argument("--ref-n", type=int, default=None, help="mesh size of the CPU reference sample (tgv 48, ramp 32)")
     ap.add_argument("--ref-steps", type=int, default=None,
                     help="steps of the CPU baseline sample (tgv: the all-core MPI run, 10; ramp: 20)")
@@ -610,7 +611,8 @@ def main():
     t_mesh = time.perf_counter() - t0
     configure(eqns, args.workload)
     eqns.set_initial_condition("domain", tgv_state if ns else ramp_state)
-    precision = tb.TG_PRECISION_FP64 if args.precision == "fp64" else tb.TG_PRECISION_FP32_FLUX
+    precision = {"fp64": tb.TG_PRECISION_FP64, "fp32": tb.TG_PRECISION_FP32_FLUX,
+                 "exact": tb.TG_PRECISION_FP64_EXACT}[args.precision]
     t0 = time.perf_counter()
     ctx = eqns.context(precision)
     t_upload = time.perf_counter() - t0
@@ -673,6 +675,30 @@ def main():
     e2e_s = max_over_ranks(time.perf_counter() - t0, pg)
     e2e_value = whole_job_rate(C, e2e_steps, world, e2e_s)
 
+    # the exact FP64 form (teal's arithmetic, bit-identical results) on the same workload: its rate
+    # beside the plain form's, from the same state, timed the same way
+    exact_form = None
+    if args.precision == "fp64":
+        xctx = eqns.context(tb.TG_PRECISION_FP64_EXACT)
+        xctx.set_stream(stream.cuda_stream)
+        xctx.set_primitive(ctx.get_primitive())
+        xsteps = min(args.steps, 10)
+        xctx.run(LSERK, 0.99, 2, context=rk)
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        ev0.record(stream)
+        xctx.run(LSERK, 0.99, xsteps, context=rk)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        xms = max_over_ranks(ev0.elapsed_time(ev1), pg)
+        xval = whole_job_rate(C, xsteps, world, xms / 1000.0)
+        exact_form = {"value": xval, "unit": "cell-updates/s", "ms_per_step": xms / xsteps, "steps": xsteps,
+                      "plain_over_exact": value / xval,
+                      "parity": "bit-identical to the reference's residual and explicit steps"}
+        xctx.close()
+        eqns._ctx.pop(tb.TG_PRECISION_FP64_EXACT, None)
+
     # roofline of one RK stage (boundary + gradient + face + cell kernels)
     peak, peak_kind = read_peaks()
     stages = ksteps * rk[1]
@@ -700,7 +726,7 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32-flux/f64-accumulate",
+        "vs_baseline": None, "dtype": "f32-flux/f64-accumulate" if args.precision == "fp32" else "f64",
         "data": "synthetic",
         "config": {"workload": workload_name("tgv" if ns else "ramp", n), "cells": C, "faces": F, "mesh": f"{n}^3",
                    "global_batch": world, "parallelism": f"replicas x{world}" if world > 1 else "1 gpu",
@@ -716,6 +742,8 @@ def main():
         "gpu_launches": launches,
         "setup_s": {"mesh": t_mesh, "upload": t_upload},
     }
+    if exact_form:
+        line["exact_form"] = exact_form
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:

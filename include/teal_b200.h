@@ -93,9 +93,17 @@ enum { TG_SOURCE_NONE = 0, TG_SOURCE_BODY_FORCE = 1, TG_SOURCE_BULK_FORCING = 2,
 /* time integrators of simulation_set_advance (src/simulation/set.c:74-131) */
 enum { TG_ADVANCE_EULER = 0, TG_ADVANCE_LSERK = 1, TG_ADVANCE_IMPLICIT_EULER = 2 };
 
-/* arithmetic of the face-flux path: plain FP64, or FP32 gradients/limiter/fluxes with FP64
- * accumulation, state update and Krylov arithmetic */
-enum { TG_PRECISION_FP64 = 0, TG_PRECISION_FP32_FLUX = 1 };
+/* arithmetic of the face-flux path:
+ *   TG_PRECISION_FP64        plain FP64; quotients that share a denominator take one reciprocal and
+ *                            multiply-adds are contracted: within a few ulps of teal per operation
+ *   TG_PRECISION_FP32_FLUX   FP32 gradients/limiter/fluxes with FP64 accumulation, state update and
+ *                            Krylov arithmetic
+ *   TG_PRECISION_FP64_EXACT  FP64 with teal's own operations in teal's order (every quotient a
+ *                            division, no contraction, the viscous face terms of a cell summed before
+ *                            the convective ones as in derivative.c:279-292): residuals, gradients,
+ *                            time steps and explicit steps equal teal's bit for bit; slower than
+ *                            TG_PRECISION_FP64 (two flux records per face with a viscous flux) */
+enum { TG_PRECISION_FP64 = 0, TG_PRECISION_FP32_FLUX = 1, TG_PRECISION_FP64_EXACT = 2 };
 
 /* Return the kind for a teal plugin name, or -1 when teal has no such name or this library does not
  * run it on the device (then teal would call teal_error). */
@@ -187,6 +195,14 @@ const char *tg_last_error(void);
 
 /* Run all device work of this context on `stream` (a cudaStream_t; null = the context's own). */
 int tg_set_stream(tg_ctx *ctx, void *stream);
+
+/* Failure-detection control, no counterpart in teal. Every device-side wait of this context (the
+ * staged face kernel's wait for its bulk copies of face geometry) polls at most `polls` times before
+ * it gives up; the call then returns TG_ERR_TIMEOUT, the blocks that gave up first let their copies
+ * land, and the context stays usable. Default and maximum 16777216 polls (about a second);
+ * 0 makes every such wait give up at once, which is how the timeout path is tested without a
+ * fault. */
+int tg_set_wait_limit(tg_ctx *ctx, int polls);
 
 /* Resident primitive state: [num_cells][5] in teal's cell order (density, velocity, pressure).
  * set: reads inner cells (ghost rows are ignored). get: writes inner cells, boundary ghosts as the
@@ -327,13 +343,16 @@ int tg_layout(tg_ctx *ctx, const char *name, void *out, long count);
  * can synchronise it).
  *   derivative  device double[num_cells][5] (teal's row layout)
  *   volume      device double[num_cells]
- *   sum_volume  the divisor (teal's mesh->cell.sum_volume)
+ *   sum_volume  the divisor (teal's mesh->cell.sum_volume), finite and > 0, else TG_ERR_INVALID
  *   residual    device double[5], written on `stream` (a cudaStream_t; null = legacy default)
- * All three buffers must be 8-byte aligned device or managed memory, else TG_ERR_INVALID.
+ * All three buffers must be 8-byte aligned memory of the current device, or managed memory, else
+ * TG_ERR_INVALID (memory of another GPU is refused before any launch).
  * The partial sums go to a fixed 640 KiB array compiled into the library, one per device, which
  * limits num_cells to TG_NOALLOC_MAX_CELLS; a larger num_cells returns TG_ERR_INVALID.
  * The first call on each device does a set-up (it looks up that array's device address, which can
- * initialise the device's CUDA context); make that first call before any stream capture.
+ * initialise the device's CUDA context); make that first call before any stream capture. The
+ * address is kept for the life of the process: do not cudaDeviceReset a device after calling this
+ * on it.
  * Calls that overlap in time on the same device (other streams, other host threads) share the
  * array and race: serialise them. The result equals tg_residual's on the same derivative. */
 #define TG_NOALLOC_MAX_CELLS 67108864

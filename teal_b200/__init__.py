@@ -14,6 +14,7 @@ from ._lib import (  # noqa: F401
     TG_NAVIERSTOKES,
     TG_PRECISION_FP32_FLUX,
     TG_PRECISION_FP64,
+    TG_PRECISION_FP64_EXACT,
 )
 from .api import (  # noqa: F401
     Batch,

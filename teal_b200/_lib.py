@@ -24,7 +24,8 @@ TG_EULER, TG_NAVIERSTOKES = 0, 1
 TG_VISCOUS_NONE, TG_VISCOUS_CENTRAL = 0, 1
 TG_LIMITER_NONE, TG_LIMITER_BARTH_JESPERSEN, TG_LIMITER_VENKATAKRISHNAN = 0, 1, 2
 TG_ADVANCE_EULER, TG_ADVANCE_LSERK, TG_ADVANCE_IMPLICIT_EULER = 0, 1, 2
-TG_PRECISION_FP64, TG_PRECISION_FP32_FLUX = 0, 1
+TG_PRECISION_FP64, TG_PRECISION_FP32_FLUX, TG_PRECISION_FP64_EXACT = 0, 1, 2
+TG_WAIT_POLLS = 1 << 24  # default (and maximum) polls of a device-side bounded wait
 TG_SOURCE_NONE, TG_SOURCE_BODY_FORCE, TG_SOURCE_BULK_FORCING, TG_SOURCE_DEVICE = 0, 1, 2, 3
 TG_BC_CUSTOM = 9
 TG_FUNCTION_BOUNDARY, TG_FUNCTION_SOURCE = 1, 2
@@ -117,6 +118,7 @@ SIGNATURES = [
     ("tg_destroy", ctypes.c_int, [_vp]),
     ("tg_last_error", ctypes.c_char_p, []),
     ("tg_set_stream", ctypes.c_int, [_vp, _vp]),
+    ("tg_set_wait_limit", ctypes.c_int, [_vp, ctypes.c_int]),
     ("tg_set_primitive", ctypes.c_int, [_vp, _vp]),
     ("tg_get_primitive", ctypes.c_int, [_vp, _vp]),
     ("tg_derivative", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double]),

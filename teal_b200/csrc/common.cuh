@@ -197,6 +197,14 @@ __device__ __forceinline__ void grad_rec_load(const float *rec, int c, int v, fl
 // access in FP64, two 2-vector accesses in FP32), component 4 as [F] after them.
 constexpr int FLUX_REC = 5;
 
+// Element offset of a second set of flux records (the exact form's viscous records) behind the
+// first: 5 F rounded up to a multiple of 4, so that its [F][4] part starts on a 32-byte boundary as
+// the 256-bit record accesses require.
+__host__ __device__ constexpr size_t flux_rec2_offset(int F)
+{
+    return ((size_t)FLUX_REC * (size_t)F + 3) & ~(size_t)3;
+}
+
 __device__ __forceinline__ void flux_rec_store(double *G, int F, int f, const double (&v)[5])
 {
     asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(G + (size_t)f * 4), "d"(v[0]), "d"(v[1]),

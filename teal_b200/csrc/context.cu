@@ -15,7 +15,7 @@
 #include "../../include/teal_b200.h"
 #include "functions.h"
 #include "gmres.cuh"
-#include "kernels.cuh"
+#include "aux_kernels.cuh"
 #include "launch.cuh"
 
 using namespace tg;
@@ -271,6 +271,9 @@ struct tg_ctx {
     int graph_method = -1, graph_stages = 0;
     double graph_courant = 0;
     int graph_use_max_time = -1;
+
+    // polls of the staged face kernel's first bounded wait (lowered only by tg_set_wait_limit)
+    int wait_polls = MBAR_POLLS;
 };
 
 static double &hd_at(tg_ctx *c, int field, int i) { return c->hd[(size_t)field * c->ninst + i]; }
@@ -724,7 +727,7 @@ static int upload_soa(double **dst, const double *src, size_t n, int k, double *
 static int create_ctx(MeshInput &in, const tg_equations *e, int precision, tg_ctx **out)
 {
     *out = nullptr;
-    if (precision != TG_PRECISION_FP64 && precision != TG_PRECISION_FP32_FLUX)
+    if (precision != TG_PRECISION_FP64 && precision != TG_PRECISION_FP32_FLUX && precision != TG_PRECISION_FP64_EXACT)
         return fail(TG_ERR_INVALID, "invalid precision %d", precision);
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
@@ -885,7 +888,7 @@ static int create_ctx(MeshInput &in, const tg_equations *e, int precision, tg_ct
                                  c->gb.slot_off32};
 
         // state
-        size_t rsz = precision == TG_PRECISION_FP64 ? sizeof(double) : sizeof(float);
+        size_t rsz = precision == TG_PRECISION_FP32_FLUX ? sizeof(float) : sizeof(double);
         TRY(dalloc(&c->q, 5 * (size_t)s.N));
         CU(cudaMemsetAsync(c->q, 0, 5 * sizeof(double) * s.N, st));
         TRY(dalloc(&c->U0, 5 * (size_t)s.C));
@@ -894,7 +897,10 @@ static int create_ctx(MeshInput &in, const tg_equations *e, int precision, tg_ct
         if (c->order == 2) {
             CU(cudaMalloc(&c->grad, 20 * rsz * s.C));
         }
-        CU(cudaMalloc(&c->G, FLUX_REC * rsz * s.F));
+        // the exact form with a viscous flux keeps the viscous records apart (face.cuh)
+        const bool two = precision == TG_PRECISION_FP64_EXACT && c->viscous == TG_VISCOUS_CENTRAL;
+        const size_t nrec_elems = two ? flux_rec2_offset(s.F) + (size_t)FLUX_REC * s.F : (size_t)FLUX_REC * s.F;
+        CU(cudaMalloc(&c->G, nrec_elems * rsz));
         TRY(dalloc(&c->dtc, s.C));
         if (precision == TG_PRECISION_FP32_FLUX) {
             TRY(dalloc(&c->pref, c->ninst));
@@ -1099,6 +1105,15 @@ extern "C" int tg_set_stream(tg_ctx *c, void *stream)
     return TG_OK;
 }
 
+extern "C" int tg_set_wait_limit(tg_ctx *c, int polls)
+{
+    if (!c) return fail(TG_ERR_INVALID, "null context");
+    if (polls < 0) return fail(TG_ERR_INVALID, "the poll limit must be >= 0");
+    c->wait_polls = polls > MBAR_POLLS ? MBAR_POLLS : polls;
+    drop_graph(c);  // the limit is a kernel argument baked into the step graph
+    return TG_OK;
+}
+
 // ---- host transfers --------------------------------------------------------------------------
 
 static int ensure_pinned(tg_ctx *c, size_t n)
@@ -1210,6 +1225,17 @@ static bool is_ns(const tg_ctx *c)
     return c->physics == TG_NAVIERSTOKES;
 }
 
+// FP64 records and geometry (the plain and the exact FP64 forms)
+static bool is_fp64(const tg_ctx *c)
+{
+    return c->precision != TG_PRECISION_FP32_FLUX;
+}
+
+static bool is_exact(const tg_ctx *c)
+{
+    return c->precision == TG_PRECISION_FP64_EXACT;
+}
+
 // teal's O2 path keeps the unlimited gradient only when a viscous flux needs it
 static bool fold_psi(const tg_ctx *c)
 {
@@ -1222,8 +1248,16 @@ static int run_boundary(tg_ctx *c, double *q, bool masked = false)
     int nbf = c->s.F_bd - c->s.F_in;
     if (nbf <= 0) return TG_OK;
     Launch l(c, TG_PROF_BOUNDARY);
-    k_boundary<<<grid_of(nbf), BLOCK, 0, c->stream>>>(c->s, c->lr, c->gb.basis, c->bface_ent, c->bkind, c->bctx, q,
-                                                      c->prop[0], c->cell_inst, masked ? c->st.active : nullptr);
+    if (is_exact(c)) {
+        BoundaryLaunch a{c->s,   c->lr,      c->gb.basis, c->bface_ent, c->bkind, c->bctx, q,
+                         c->prop[0], c->cell_inst, masked ? c->st.active : nullptr};
+        CU(launch_boundary_exact(a, c->stream));
+    }
+    else {
+        k_boundary<false><<<grid_of(nbf), BLOCK, 0, c->stream>>>(c->s, c->lr, c->gb.basis, c->bface_ent, c->bkind,
+                                                                 c->bctx, q, c->prop[0], c->cell_inst,
+                                                                 masked ? c->st.active : nullptr);
+    }
     CU(cudaGetLastError());
     // custom boundaries: their device functions, face by face of each boundary
     for (size_t b = 0; b < c->bd_kernel.size(); b++) {
@@ -1249,19 +1283,19 @@ static void launch_gradient_s(tg_ctx *c, const Geometry<R> &g, bool fold, const 
     R *rec = (R *)c->grad;
     switch (c->limiter) {
         case TG_LIMITER_NONE:
-            k_gradient<R, 0, true, MIXED><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
+            k_gradient<R, 0, true, MIXED, false><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
             break;
         case TG_LIMITER_BARTH_JESPERSEN:
             if (fold)
-                k_gradient<R, 1, true, MIXED><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
+                k_gradient<R, 1, true, MIXED, false><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
             else
-                k_gradient<R, 1, false, MIXED><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
+                k_gradient<R, 1, false, MIXED, false><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
             break;
         default:
             if (fold)
-                k_gradient<R, 2, true, MIXED><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
+                k_gradient<R, 2, true, MIXED, false><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
             else
-                k_gradient<R, 2, false, MIXED><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
+                k_gradient<R, 2, false, MIXED, false><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
             break;
     }
 }
@@ -1282,6 +1316,13 @@ static int run_gradient(tg_ctx *c, const double *q, int limiter_override = -1)
     if (limiter_override >= 0) c->limiter = limiter_override;
     bool fold = fold_psi(c);
     Launch l(c, TG_PROF_GRADIENT);
+    if (is_exact(c)) {
+        GradientLaunch a{c->s, c->g64, c->eps2, q, (double *)c->grad, c->limiter, fold, !c->full_slots};
+        cudaError_t e = launch_gradient_exact(a, c->stream);
+        c->limiter = saved;
+        CU(e);
+        return TG_OK;
+    }
     if (c->precision == TG_PRECISION_FP64)
         launch_gradient<double>(c, c->g64, fold, q);
     else
@@ -1295,7 +1336,7 @@ static int run_face(tg_ctx *c, const double *q)
 {
     FaceLaunch a;
     a.s = c->s;
-    a.geom = c->precision == TG_PRECISION_FP64 ? (const void *)&c->g64 : (const void *)&c->g32;
+    a.geom = is_fp64(c) ? (const void *)&c->g64 : (const void *)&c->g32;
     a.q = q;
     a.rec = c->grad;
     a.gamma = c->prop[0];
@@ -1304,10 +1345,26 @@ static int run_face(tg_ctx *c, const double *q)
     a.G = c->G;
     a.err = c->st.error;
     a.pr_ref = PressureRef{c->precision == TG_PRECISION_FP32_FLUX ? c->pref : nullptr, c->cell_inst};
+    a.polls = c->wait_polls;
     bool ns = c->viscous == TG_VISCOUS_CENTRAL;
     bool fold = fold_psi(c);
     Launch l(c, TG_PROF_FACE);
     cudaError_t e;
+    if (is_exact(c)) {
+        switch (c->flux) {
+            case TG_FLUX_ROE: e = launch_face_exact<FK_ROE>(ns, c->order, fold, a, c->stream); break;
+            case TG_FLUX_HLL: e = launch_face_exact<FK_HLL>(ns, c->order, fold, a, c->stream); break;
+            case TG_FLUX_HLLC: e = launch_face_exact<FK_HLLC>(ns, c->order, fold, a, c->stream); break;
+            case TG_FLUX_HLLE: e = launch_face_exact<FK_HLLE>(ns, c->order, fold, a, c->stream); break;
+            case TG_FLUX_AUSMD: e = launch_face_exact<FK_AUSMD>(ns, c->order, fold, a, c->stream); break;
+            case TG_FLUX_AUSMDV: e = launch_face_exact<FK_AUSMDV>(ns, c->order, fold, a, c->stream); break;
+            case TG_FLUX_LXF: e = launch_face_exact<FK_LXF>(ns, c->order, fold, a, c->stream); break;
+            case TG_FLUX_CENTRAL: e = launch_face_exact<FK_CENTRAL>(ns, c->order, fold, a, c->stream); break;
+            default: e = launch_face_exact<FK_NONE>(ns, c->order, fold, a, c->stream); break;
+        }
+        CU(e);
+        return TG_OK;
+    }
     switch (c->flux) {
         case TG_FLUX_ROE: e = launch_face<FK_ROE>(c->precision, ns, c->order, fold, a, c->stream); break;
         case TG_FLUX_HLL: e = launch_face<FK_HLL>(c->precision, ns, c->order, fold, a, c->stream); break;
@@ -1329,9 +1386,9 @@ static void launch_cell_s(tg_ctx *c, double alpha, int last, double *q, double *
     CellData cd{c->volume, c->proj, c->eps2};
     Source src{{c->src_par[0], c->src_par[1], c->src_par[2], c->src_par[3]},
                c->source == TG_SOURCE_DEVICE ? c->S : c->src_avg};
-    k_cell<MODE, NS, GT, SRC><<<(c->s.C + CELL_BLOCK - 1) / CELL_BLOCK, CELL_BLOCK, 0, c->stream>>>(
+    k_cell<MODE, NS, GT, SRC, false><<<(c->s.C + CELL_BLOCK - 1) / CELL_BLOCK, CELL_BLOCK, 0, c->stream>>>(
         c->s, c->slot_face, c->slot_cnt, cd, (const GT *)c->G, c->U0, q, Rout, c->seg, c->st, alpha, last,
-        props_of(c), c->dtc, src);
+        props_of(c), c->dtc, src, 0);
 }
 
 template <int MODE, bool NS, typename GT>
@@ -1350,6 +1407,31 @@ static int launch_cell(tg_ctx *c, double alpha, int last, double *q, double *Rou
 {
     Launch l(c, TG_PROF_CELL);
     bool ns = is_ns(c);
+    if (is_exact(c)) {
+        CellLaunch a;
+        a.mode = MODE;
+        a.ns = ns;
+        a.source = c->source;
+        a.two = (c->viscous == TG_VISCOUS_CENTRAL && c->order == 2) ? 1 : 0;
+        a.s = c->s;
+        a.slot_face = c->slot_face;
+        a.slot_cnt = c->slot_cnt;
+        a.cd = CellData{c->volume, c->proj, c->eps2};
+        a.G = (const double *)c->G;
+        a.U0 = c->U0;
+        a.q = q;
+        a.Rout = Rout;
+        a.seg = c->seg;
+        a.st = c->st;
+        a.alpha = alpha;
+        a.last = last;
+        a.prop = props_of(c);
+        a.dtc = c->dtc;
+        a.src = Source{{c->src_par[0], c->src_par[1], c->src_par[2], c->src_par[3]},
+                       c->source == TG_SOURCE_DEVICE ? c->S : c->src_avg};
+        CU(launch_cell_exact(a, c->stream));
+        return TG_OK;
+    }
     if (c->precision == TG_PRECISION_FP64) {
         if (ns)
             launch_cell_t<MODE, true, double>(c, alpha, last, q, Rout);
@@ -1415,10 +1497,12 @@ static int run_pieces(tg_ctx *c, int res)
 static int run_prepare(tg_ctx *c)
 {
     CellData cd{c->volume, c->proj, c->eps2};
-    if (is_ns(c))
-        k_prepare<true><<<grid_of(c->s.C), BLOCK, 0, c->stream>>>(c->s, cd, c->q, c->U0, props_of(c), c->dtc);
+    if (is_exact(c))
+        CU(launch_prepare_exact(is_ns(c), c->s, cd, c->q, c->U0, props_of(c), c->dtc, c->stream));
+    else if (is_ns(c))
+        k_prepare<true, false><<<grid_of(c->s.C), BLOCK, 0, c->stream>>>(c->s, cd, c->q, c->U0, props_of(c), c->dtc);
     else
-        k_prepare<false><<<grid_of(c->s.C), BLOCK, 0, c->stream>>>(c->s, cd, c->q, c->U0, props_of(c), c->dtc);
+        k_prepare<false, false><<<grid_of(c->s.C), BLOCK, 0, c->stream>>>(c->s, cd, c->q, c->U0, props_of(c), c->dtc);
     CU(cudaGetLastError());
     TRY(run_pieces(c, 0));
     c->prepared = true;
@@ -1498,7 +1582,7 @@ extern "C" int tg_gradient(tg_ctx *c, double time, int limited, double *gradient
     // multiplied in here
     const bool folded = lim == TG_LIMITER_NONE || c->viscous != TG_VISCOUS_CENTRAL;
     int limit = (limited && lim != TG_LIMITER_NONE && !folded) ? 1 : 0;
-    if (c->precision == TG_PRECISION_FP64)
+    if (is_fp64(c))
         k_grad_to_aos<double><<<grid_of(c->s.C), BLOCK, 0, c->stream>>>(c->s.C, (const double *)c->grad, limit,
                                                                         c->aos);
     else
@@ -1950,7 +2034,7 @@ static int implicit_step_all(tg_ctx *c, const void *context, double courant)
     const size_t n = 5 * (size_t)C;
     // finite-difference perturbation relative to the state: teal's 1e-6 (advance.c:157) in FP64;
     // the FP32-flux form's residual carries ~1e-7 relative rounding, so it perturbs by 3e-4
-    const double fd_rel = (c->precision == TG_PRECISION_FP64) ? 1e-6 : 3e-4;
+    const double fd_rel = is_fp64(c) ? 1e-6 : 3e-4;
 
     // step from the CFL condition; U = cons(q) (advance.c:136-143)
     TRY(run_prepare(c));

@@ -81,7 +81,9 @@ struct FaceTile {
     // thread 0 issues the copies of faces [f0, f0 + n); every thread then waits (bounded).
     // Returns false after a wait that gave up (the error word then has the timeout bit); the
     // decision is the same in every thread of the block.
-    __device__ __forceinline__ bool stage(const Geometry<R> &g, int F, int f0, int n, int *err)
+    // `polls` bounds the first wait (MBAR_POLLS normally; a smaller value lets a test make it give up);
+    // the drain after a wait that gave up always uses the full MBAR_POLLS.
+    __device__ __forceinline__ bool stage(const Geometry<R> &g, int F, int f0, int n, int *err, int polls)
     {
         if (threadIdx.x == 0) {
             mbar_init(&bar, 1);
@@ -96,12 +98,12 @@ struct FaceTile {
             }
         }
         __syncthreads();
-        const bool ok = mbar_wait_bounded(&bar, 0);
+        const bool ok = mbar_wait_bounded(&bar, 0, polls);
         if (__syncthreads_or(!ok)) {
             if (threadIdx.x == 0) {
                 atomicOr(err, ERR_TIMEOUT);
             }
-            mbar_wait_bounded(&bar, 0);  // let copies still in flight land before the block exits
+            mbar_wait_bounded(&bar, 0, MBAR_POLLS);  // let copies still in flight land before the block exits
             return false;
         }
         return true;
@@ -130,6 +132,10 @@ struct FaceTile {
 // The flux record of face f (element i of its tile). The convective flux comes first (its
 // reconstruction streams the limited gradients), the viscous flux second (its face-averaged
 // gradient re-reads the unlimited gradients, which are still in L1).
+// Records: G[f] = (convective - viscous) * area; in the exact translation units with a viscous
+// flux, G[f] = convective * area and G[flux_rec2_offset(F) + f] = viscous * area instead, because teal adds all of a
+// cell's viscous terms before its convective ones (derivative.c:279-292) and the cell gather must
+// repeat that order.
 template <typename R, int FK, bool NS, int ORDER, bool FOLD, typename Geo>
 __device__ __forceinline__ void face_flux(const Geo &geo, int i, int f, const Sizes &s, const double *__restrict__ q,
                                           const R *__restrict__ rec, R gamma, R mu, R prandtl, R *__restrict__ G,
@@ -208,11 +214,13 @@ __device__ __forceinline__ void face_flux(const Geo &geo, int i, int f, const Si
             }
         }
         V3<R> unit = geo.corr(i);
-        R inv_norm = R(1) / geo.corr_norm(i);
+        const R cnorm = geo.corr_norm(i);
+        const R inv_norm = R(1) / cnorm;
 #pragma unroll
         for (int v = 0; v < 5; v++) {
             V3<R> gv = v3(gm[3 * v], gm[3 * v + 1], gm[3 * v + 2]);
-            R adjust = dot(gv, unit) - ((qrv[v] - qlv[v]) * inv_norm);
+            const R dq = qrv[v] - qlv[v];
+            R adjust = dot(gv, unit) - (kExact ? (dq / cnorm) : (dq * inv_norm));
             gv = sub(gv, mul(adjust, unit));
             gm[3 * v] = gv.x;
             gm[3 * v + 1] = gv.y;
@@ -230,22 +238,30 @@ __device__ __forceinline__ void face_flux(const Geo &geo, int i, int f, const Si
         nb.y = nb.x;
         nb.z = nb.x;
         Cons<R> fv = viscous_central(prim_from(qm), gg, gamma, mu, prandtl, nb);
-        gf[0] -= fv.rho * area;
-        gf[1] -= fv.m.x * area;
-        gf[2] -= fv.m.y * area;
-        gf[3] -= fv.m.z * area;
-        gf[4] -= fv.e * area;
+        if constexpr (kExact) {
+            const R gv[5] = {fv.rho * area, fv.m.x * area, fv.m.y * area, fv.m.z * area, fv.e * area};
+            flux_rec_store(G + flux_rec2_offset(s.F), s.F, f, gv);
+        }
+        else {
+            gf[0] -= fv.rho * area;
+            gf[1] -= fv.m.x * area;
+            gf[2] -= fv.m.y * area;
+            gf[3] -= fv.m.z * area;
+            gf[4] -= fv.e * area;
+        }
     }
     flux_rec_store(G, s.F, f, gf);
 }
 
 // One thread per face, geometry loaded by the threads. face_minb caps the registers so that
 // several blocks stay resident per SM.
-template <typename R, int FK, bool NS, int ORDER, bool FOLD>
+// X: this is the exact translation unit's instantiation (a distinct kernel name per arithmetic).
+template <typename R, int FK, bool NS, int ORDER, bool FOLD, bool X>
 __global__ void __launch_bounds__(FACE_BLOCK, face_minb<R>(NS)) k_face(Sizes s, Geometry<R> g, const double *__restrict__ q,
                                                    const R *__restrict__ rec, R gamma, R mu, R prandtl,
                                                    R *__restrict__ G, PressureRefOf<R> pr_ref)
 {
+    static_assert(X == kExact, "exact kernels live in the exact translation units only");
     const int f = blockIdx.x * FACE_BLOCK + threadIdx.x;
     if (f >= s.F) {
         return;
@@ -257,17 +273,18 @@ __global__ void __launch_bounds__(FACE_BLOCK, face_minb<R>(NS)) k_face(Sizes s, 
 // One tile of FACE_BLOCK faces per block, its geometry staged in shared memory by bulk copies
 // before the threads (one face each) start. A wait that gives up sets ERR_TIMEOUT in the error
 // word and ends the block.
-template <typename R, int FK, bool NS, int ORDER, bool FOLD>
+template <typename R, int FK, bool NS, int ORDER, bool FOLD, bool X>
 __global__ void __launch_bounds__(FACE_BLOCK, face_minb<R>(NS)) k_face_staged(Sizes s, Geometry<R> g,
                                                           const double *__restrict__ q,
                                                           const R *__restrict__ rec, R gamma, R mu,
                                                           R prandtl, R *__restrict__ G, int *err,
-                                                          PressureRefOf<R> pr_ref)
+                                                          PressureRefOf<R> pr_ref, int polls)
 {
+    static_assert(X == kExact, "exact kernels live in the exact translation units only");
     __shared__ __align__(16) FaceTile<R, ORDER, NS> t;
     const int f0 = blockIdx.x * FACE_BLOCK;
     const int n = min(FACE_BLOCK, s.F - f0);
-    if (!t.stage(g, s.F, f0, n, err)) {
+    if (!t.stage(g, s.F, f0, n, err, polls)) {
         return;
     }
     if (threadIdx.x < n) {

@@ -17,11 +17,18 @@ struct FaceLaunch {
     void *G;
     int *err;  // device error word (bounded waits that give up set ERR_TIMEOUT)
     PressureRef pr_ref;  // FP32-flux form: reference pressure per instance
+    int polls;           // limit of the staged kernel's first wait (MBAR_POLLS unless a test lowers it)
 };
+
+// The launchers below are local to each translation unit (unnamed namespace): the exact and the plain
+// face translation units instantiate them with the same template arguments, and one shared
+// definition would launch the other arithmetic's kernels.
+namespace {
 
 template <typename R, int FK, bool NS, int ORDER, bool FOLD>
 inline void launch_face_v(bool staged, const FaceLaunch &a, const Geometry<R> &g, const R *rec, R *G, cudaStream_t st)
 {
+    constexpr bool X = kExact;
     dim3 grid((a.s.F + FACE_BLOCK - 1) / FACE_BLOCK);
     R gm = R(a.gamma), mu = R(a.mu), pr = R(a.prandtl);
     PressureRefOf<R> pref{};
@@ -29,11 +36,11 @@ inline void launch_face_v(bool staged, const FaceLaunch &a, const Geometry<R> &g
         pref = a.pr_ref;
     }
     if (staged) {
-        k_face_staged<R, FK, NS, ORDER, FOLD>
-            <<<grid, FACE_BLOCK, 0, st>>>(a.s, g, a.q, rec, gm, mu, pr, G, a.err, pref);
+        k_face_staged<R, FK, NS, ORDER, FOLD, X>
+            <<<grid, FACE_BLOCK, 0, st>>>(a.s, g, a.q, rec, gm, mu, pr, G, a.err, pref, a.polls);
     }
     else {
-        k_face<R, FK, NS, ORDER, FOLD><<<grid, FACE_BLOCK, 0, st>>>(a.s, g, a.q, rec, gm, mu, pr, G, pref);
+        k_face<R, FK, NS, ORDER, FOLD, X><<<grid, FACE_BLOCK, 0, st>>>(a.s, g, a.q, rec, gm, mu, pr, G, pref);
     }
 }
 
@@ -60,10 +67,17 @@ inline cudaError_t launch_face_r(bool ns, int order, bool fold, const FaceLaunch
     return cudaGetLastError();
 }
 
+}  // namespace
+
 // precision: 0 = FP64, 1 = FP32 flux path
 template <int FK>
 cudaError_t launch_face(int precision, bool ns, int order, bool fold, const FaceLaunch &a,
                         cudaStream_t st);
+
+// FP64 with teal's exact arithmetic (face_*_exact.cu); with a viscous flux, `a.G` holds 2 x 5 F
+// values (convective and viscous records)
+template <int FK>
+cudaError_t launch_face_exact(bool ns, int order, bool fold, const FaceLaunch &a, cudaStream_t st);
 
 #define TG_INSTANTIATE_FACE(FK)                                                                 \
     template <>                                                                                 \
@@ -74,6 +88,14 @@ cudaError_t launch_face(int precision, bool ns, int order, bool fold, const Face
             return launch_face_r<FK, double>(ns, order, fold, a, st);                           \
         }                                                                                       \
         return launch_face_r<FK, float>(ns, order, fold, a, st);                                \
+    }
+
+#define TG_INSTANTIATE_FACE_EXACT(FK)                                                              \
+    static_assert(kExact, "face_*_exact.cu is compiled with TG_EXACT_TU=1");                       \
+    template <>                                                                                 \
+    cudaError_t launch_face_exact<FK>(bool ns, int order, bool fold, const FaceLaunch &a, cudaStream_t st) \
+    {                                                                                           \
+        return launch_face_r<FK, double>(ns, order, fold, a, st);                               \
     }
 
 }  // namespace tg

@@ -12,6 +12,7 @@
 // sqrt(sum / sum_volume)), with the same loop order, so both give the same bits.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdint>
 #include <mutex>
 
@@ -86,7 +87,9 @@ __global__ void __launch_bounds__(NA_FINISH_BLOCK) k_noalloc_residual_finish(int
 }
 
 // Address of this device's scratch array, looked up once per device (with that device current)
-// and kept. Returns null after recording the error.
+// and kept for the life of the process. A cudaDeviceReset after that first lookup unloads the module
+// holding the array, and the kept address would then be stale: resetting a device on which
+// tg_residual_noalloc has run is not supported. Returns null after recording the error.
 static double *noalloc_scratch(int *status)
 {
     static std::mutex lock;
@@ -115,8 +118,10 @@ static double *noalloc_scratch(int *status)
     return addr[dev];
 }
 
-// a buffer the kernels may read or write: device or managed memory, 8-byte aligned
-static bool device_buffer(const void *p)
+// a buffer the kernels may read or write: managed memory, or device memory of device `dev` (the
+// current one: memory of another GPU would be a peer access the kernels are not set up for), 8-byte
+// aligned
+static bool device_buffer(const void *p, int dev)
 {
     if (!p || ((uintptr_t)p & 7u)) {
         return false;
@@ -126,7 +131,10 @@ static bool device_buffer(const void *p)
         cudaGetLastError();
         return false;
     }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+    if (a.type == cudaMemoryTypeManaged) {
+        return true;
+    }
+    return a.type == cudaMemoryTypeDevice && a.device == dev;
 }
 
 extern "C" int tg_residual_noalloc(const double *derivative, const double *volume, int num_cells, double sum_volume,
@@ -137,10 +145,19 @@ extern "C" int tg_residual_noalloc(const double *derivative, const double *volum
                                "tg_residual_noalloc: num_cells must be in [0, TG_NOALLOC_MAX_CELLS = 67108864]; "
                                "use tg_residual through a context for larger meshes");
     }
-    if (!device_buffer(residual) || (num_cells > 0 && (!device_buffer(derivative) || !device_buffer(volume)))) {
+    if (!(sum_volume > 0.0) || !std::isfinite(sum_volume)) {
+        return tg_record_error(TG_ERR_INVALID, "tg_residual_noalloc: sum_volume must be finite and positive");
+    }
+    int dev = -1;
+    cudaError_t de = cudaGetDevice(&dev);
+    if (de != cudaSuccess) {
+        return tg_record_error(TG_ERR_NO_DEVICE, cudaGetErrorString(de));
+    }
+    if (!device_buffer(residual, dev) ||
+        (num_cells > 0 && (!device_buffer(derivative, dev) || !device_buffer(volume, dev)))) {
         return tg_record_error(TG_ERR_INVALID,
                                "tg_residual_noalloc: derivative, volume and residual must be 8-byte aligned "
-                               "device memory");
+                               "memory of the current device (or managed memory)");
     }
     int status = TG_OK;
     double *partials = noalloc_scratch(&status);

@@ -7,7 +7,19 @@
 
 #include <cuda_runtime.h>
 
+// Arithmetic of this translation unit. The translation units named *_exact.cu are compiled with
+// TG_EXACT_TU=1 and -fmad=false: their FP64 kernels evaluate every expression with teal's own
+// operations in teal's order (each quotient a division, no multiply-add contraction), so that with
+// IEEE-rounded + - * / sqrt on both sides they reproduce teal's CPU results bit for bit. The other
+// translation units share one reciprocal between quotients with the same denominator and let the
+// compiler contract multiply-adds, within a few ulps of teal per operation and faster.
+#ifndef TG_EXACT_TU
+#define TG_EXACT_TU 0
+#endif
+
 namespace tg {
+
+constexpr bool kExact = TG_EXACT_TU != 0;
 
 template <typename R>
 struct V3 {
@@ -86,7 +98,12 @@ __device__ __forceinline__ Prim<R> cons_to_prim(const Cons<R> &c, R gamma)
 {
     Prim<R> q;
     q.rho = fmax(R(1e-8), c.rho);
-    q.u = mul(R(1) / q.rho, c.m);  // one reciprocal for the three velocities
+    if constexpr (kExact) {
+        q.u = div(c.m, q.rho);
+    }
+    else {
+        q.u = mul(R(1) / q.rho, c.m);  // one reciprocal for the three velocities
+    }
     q.p = fmax(R(1e-8), (gamma - R(1)) * (c.e - (dot(c.m, q.u) / R(2))));
     return q;
 }
@@ -103,7 +120,12 @@ __device__ __forceinline__ Cons<R> prim_to_cons(const Prim<R> &q, R gamma)
     Cons<R> c;
     c.rho = q.rho;
     c.m = mul(c.rho, q.u);
-    c.e = mul_rn(q.p, R(1) / (gamma - R(1))) + (dot(c.m, q.u) / R(2));
+    if constexpr (kExact) {
+        c.e = (q.p / (gamma - R(1))) + (dot(c.m, q.u) / R(2));
+    }
+    else {
+        c.e = mul_rn(q.p, R(1) / (gamma - R(1))) + (dot(c.m, q.u) / R(2));
+    }
     return c;
 }
 
@@ -168,7 +190,12 @@ __device__ __forceinline__ Local<R> make_local(const Prim<R> &g, R gamma, const 
         (void)pref;
         s.p = g.p;
         s.m = mul(s.rho, s.u);
-        s.e = (s.p * (R(1) / (gamma - R(1)))) + (dot(s.m, s.u) / R(2));
+        if constexpr (kExact) {
+            s.e = (s.p / (gamma - R(1))) + (dot(s.m, s.u) / R(2));
+        }
+        else {
+            s.e = (s.p * (R(1) / (gamma - R(1)))) + (dot(s.m, s.u) / R(2));
+        }
     }
     else {
         s.dp = g.p;
@@ -227,8 +254,8 @@ __device__ __forceinline__ Cons<R> flux_roe(const Local<R> &l, const Local<R> &r
 {
     R gm1 = gamma - R(1);
     const R il = R(1) / l.rho, ir = R(1) / r.rho;
-    R hl = (l.e + l.p) * il;
-    R hr = (r.e + r.p) * ir;
+    R hl = kExact ? ((l.e + l.p) / l.rho) : ((l.e + l.p) * il);
+    R hr = kExact ? ((r.e + r.p) / r.rho) : ((r.e + r.p) * ir);
     R sl = sqrt(l.rho);
     R sr = sqrt(r.rho);
     R w = R(1) / (sl + sr);
@@ -240,8 +267,8 @@ __device__ __forceinline__ Cons<R> flux_roe(const Local<R> &l, const Local<R> &r
 
     R eig[3] = {u.x - a, u.x, u.x + a};
     {
-        R al = sqrt((gamma * l.p) * il);
-        R ar = sqrt((gamma * r.p) * ir);
+        R al = kExact ? sqrt((gamma * l.p) / l.rho) : sqrt((gamma * l.p) * il);
+        R ar = kExact ? sqrt((gamma * r.p) / r.rho) : sqrt((gamma * r.p) * ir);
         R el[3] = {l.u.x - al, l.u.x, l.u.x + al};
         R er[3] = {r.u.x - ar, r.u.x, r.u.x + ar};
 #pragma unroll
@@ -256,10 +283,16 @@ __device__ __forceinline__ Cons<R> flux_roe(const Local<R> &l, const Local<R> &r
     R ws[5];
     ws[2] = j.m.y - (u.y * j.rho);
     ws[3] = j.m.z - (u.z * j.rho);
-    const R ia = R(1) / a;  // one reciprocal for the two quotients by a and a^2
-    ws[1] = (gm1 * (ia * ia)) *
-            (((((j.rho * (h - (u.x * u.x))) + (u.x * j.m.x)) - j.e) + (ws[2] * u.y)) + (ws[3] * u.z));
-    ws[0] = (((j.rho * (u.x + a)) - j.m.x) - (a * ws[1])) * (ia / R(2));
+    const R jw = ((((j.rho * (h - (u.x * u.x))) + (u.x * j.m.x)) - j.e) + (ws[2] * u.y)) + (ws[3] * u.z);
+    if constexpr (kExact) {
+        ws[1] = (gm1 / a2) * jw;
+        ws[0] = (((j.rho * (u.x + a)) - j.m.x) - (a * ws[1])) / (R(2) * a);
+    }
+    else {
+        const R ia = R(1) / a;  // one reciprocal for the two quotients by a and a^2
+        ws[1] = (gm1 * (ia * ia)) * jw;
+        ws[0] = (((j.rho * (u.x + a)) - j.m.x) - (a * ws[1])) * (ia / R(2));
+    }
     ws[4] = j.rho - (ws[0] + ws[1]);
 
     R ch[5] = {ws[0] * eig[0], ws[1] * eig[1], ws[2] * eig[1], ws[3] * eig[1], ws[4] * eig[2]};
@@ -314,8 +347,8 @@ __device__ __forceinline__ void einfeldt_speeds(const Local<R> &l, const Local<R
                                                 R &sl_out, R &sr_out)
 {
     const R il = R(1) / l.rho, ir = R(1) / r.rho;
-    R hl = (l.e + l.p) * il;
-    R hr = (r.e + r.p) * ir;
+    R hl = kExact ? ((l.e + l.p) / l.rho) : ((l.e + l.p) * il);
+    R hr = kExact ? ((r.e + r.p) / r.rho) : ((r.e + r.p) * ir);
     R sl = sqrt(l.rho);
     R sr = sqrt(r.rho);
     R w = R(1) / (sl + sr);
@@ -323,8 +356,8 @@ __device__ __forceinline__ void einfeldt_speeds(const Local<R> &l, const Local<R
     R h = w * ((sl * hl) + (sr * hr));
     R u2 = dot(u, u);
     R a = sqrt((gamma - R(1)) * (h - (u2 / R(2))));
-    R al = sqrt((gamma * l.p) * il);
-    R ar = sqrt((gamma * r.p) * ir);
+    R al = kExact ? sqrt((gamma * l.p) / l.rho) : sqrt((gamma * l.p) * il);
+    R ar = kExact ? sqrt((gamma * r.p) / r.rho) : sqrt((gamma * r.p) * ir);
     sl_out = fmin(l.u.x - al, u.x - a);
     sr_out = fmax(r.u.x + ar, u.x + a);
 }
@@ -390,8 +423,8 @@ __device__ __forceinline__ Cons<R> flux_hlle(const Local<R> &l, const Local<R> &
     R sr = sqrt(r.rho);
     R w = R(1) / (sl + sr);
     R ux = w * ((sl * l.u.x) + (sr * r.u.x));
-    R a2l = (gamma * l.p) * (R(1) / l.rho);
-    R a2r = (gamma * r.p) * (R(1) / r.rho);
+    R a2l = kExact ? ((gamma * l.p) / l.rho) : ((gamma * l.p) * (R(1) / l.rho));
+    R a2r = kExact ? ((gamma * r.p) / r.rho) : ((gamma * r.p) * (R(1) / r.rho));
     R al = sqrt(a2l);
     R ar = sqrt(a2r);
     R a2 = w * ((sl * a2l) + (sr * a2r));
@@ -415,6 +448,39 @@ template <typename R, bool DV>
 __device__ __forceinline__ void ausm_split(const Local<R> &l, const Local<R> &r, R gamma, R &vpl,
                                            R &ppl, R &vmr, R &pmr)
 {
+    if constexpr (kExact) {  // teal's quotients, term by term
+        R al = sqrt((gamma * l.p) / l.rho);
+        R ar = sqrt((gamma * r.p) / r.rho);
+        R a = fmax(al, ar);
+        R pdl = l.p / l.rho;
+        R pdr = r.p / r.rho;
+        R pds = pdl + pdr;
+        R ml = l.u.x / a;
+        R mr = r.u.x / a;
+        if (fabs(l.u.x) <= a) {
+            R alpha = (R(2) * pdl) / pds;
+            R f = l.u.x + a;
+            vpl = ((alpha * (f * f)) / (R(4) * a)) + (((R(1) - alpha) * (l.u.x + fabs(l.u.x))) / R(2));
+            ppl = ((l.p * (f * f)) / (R(4) * (a * a))) * (R(2) - ml);
+        }
+        else {
+            vpl = (l.u.x + fabs(l.u.x)) / R(2);
+            ppl = DV ? ((l.p * (l.u.x + fabs(l.u.x))) / (R(2) * l.u.x))
+                     : (((l.p * (l.u.x + fabs(l.u.x))) / R(2)) / l.u.x);
+        }
+        if (fabs(r.u.x) <= a) {
+            R alpha = (R(2) * pdr) / pds;
+            R f = r.u.x - a;
+            vmr = ((-alpha * (f * f)) / (R(4) * a)) + (((R(1) - alpha) * (r.u.x - fabs(r.u.x))) / R(2));
+            pmr = ((r.p * (f * f)) / (R(4) * (a * a))) * (R(2) + mr);
+        }
+        else {
+            vmr = (r.u.x - fabs(r.u.x)) / R(2);
+            pmr = DV ? ((r.p * (r.u.x - fabs(r.u.x))) / (R(2) * r.u.x))
+                     : (((r.p * (r.u.x - fabs(r.u.x))) / R(2)) / r.u.x);
+        }
+        return;
+    }
     const R il = R(1) / l.rho, ir = R(1) / r.rho;
     R al = sqrt((gamma * l.p) * il);
     R ar = sqrt((gamma * r.p) * ir);
@@ -459,8 +525,8 @@ __device__ __forceinline__ Cons<R> flux_ausmd(const Local<R> &l, const Local<R> 
     R mf = (vpl * l.rho) + (vmr * r.rho);
     R amf = fabs(mf);
     R pf = ppl + pmr;
-    R hl = (l.e + l.p) * (R(1) / l.rho);
-    R hr = (r.e + r.p) * (R(1) / r.rho);
+    R hl = kExact ? ((l.e + l.p) / l.rho) : ((l.e + l.p) * (R(1) / l.rho));
+    R hr = kExact ? ((r.e + r.p) / r.rho) : ((r.e + r.p) * (R(1) / r.rho));
     Cons<R> f;
     f.rho = mf;
     f.m.x = (((mf * (l.u.x + r.u.x)) - (amf * (r.u.x - l.u.x))) / R(2)) + pf;
@@ -484,8 +550,8 @@ __device__ __forceinline__ Cons<R> flux_ausmdv(const Local<R> &l, const Local<R>
     R pmin = fmin(l.p, r.p);
     R sw = fmin(R(1) / R(2), fmin(R(1), (R(10) * fabs(r.p - l.p)) / pmin));
     R nm = (((R(1) + sw) * nv) + ((R(1) - sw) * nd)) / R(2);
-    R hl = (l.e + l.p) * (R(1) / l.rho);
-    R hr = (r.e + r.p) * (R(1) / r.rho);
+    R hl = kExact ? ((l.e + l.p) / l.rho) : ((l.e + l.p) * (R(1) / l.rho));
+    R hr = kExact ? ((r.e + r.p) / r.rho) : ((r.e + r.p) * (R(1) / r.rho));
     Cons<R> f;
     f.rho = mf;
     f.m.x = nm + pf;
@@ -589,7 +655,7 @@ __device__ __forceinline__ Cons<R> viscous_central(const Prim<R> &q, const Grad<
                                                    R mu, R prandtl, const Basis<R> &b)
 {
     R div_u = (g.ux.x + g.uy.y) + g.uz.z;
-    const R div3 = div_u * (R(1) / R(3));
+    const R div3 = kExact ? (div_u / R(3)) : (div_u * (R(1) / R(3)));
     R txx = R(2) * mu * (g.ux.x - div3);
     R tyy = R(2) * mu * (g.uy.y - div3);
     R tzz = R(2) * mu * (g.uz.z - div3);

@@ -48,10 +48,13 @@ __device__ __forceinline__ bool mbar_test_wait(uint64_t *bar, uint32_t phase)
     return done != 0;
 }
 
-// Wait for the barrier's phase with an iteration limit (about a second); false when it gave up.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t phase)
+// polls of a bounded wait: about a second
+constexpr int MBAR_POLLS = 1 << 24;
+
+// Wait for the barrier's phase with an iteration limit; false when it gave up.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t phase, int polls)
 {
-    for (int it = 0; it < (1 << 24); it++) {
+    for (int it = 0; it < polls; it++) {
         if (mbar_test_wait(bar, phase)) {
             return true;
         }

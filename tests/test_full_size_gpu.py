@@ -8,8 +8,11 @@ discrete conservation (every face flux leaves one cell and enters another, so th
 sum of the residual vanishes to rounding and the conserved totals stay put over steps) and
 bit-identical repeated runs.
 
-Parity bar: relative L2 per conserved variable <= 1e-12 for the ramp's residual and state after one
-explicit step. The Taylor-Green residual at 128^3 is the small difference of large,
+The exact FP64 form (TG_PRECISION_FP64_EXACT: teal's operations in teal's order) equals the
+reference bit for bit at both sizes: residual and state after one explicit step.
+
+Parity bar of the plain FP64 form: relative L2 per conserved variable <= 1e-12 for the ramp's
+residual and state after one explicit step. The Taylor-Green residual at 128^3 is the small difference of large,
 nearly equal face fluxes (the pressure flux p0 A, p0 = 71, against residuals of order 1e-2 at
 h = 0.05), so rounding-level differences in the fluxes are amplified by about 1e5: the reference's
 own residual moves by 3.7e-11 (density) and 5.7e-11 (energy) relative L2 when every input moves by
@@ -77,11 +80,11 @@ def conserved_totals(prim, volume):
     return exact_sums(volume[:, None] * cons), exact_sums(volume[:, None] * np.abs(cons))
 
 
-def step_both(re, de, prim, courant, rk):
+def step_both(re, de, prim, courant, rk, precision=tb.TG_PRECISION_FP64):
     re.set_primitive(prim)
     de.primitive[:] = prim
     rsim = ref.RefSimulation(re, "lserk", courant, rk=rk)
-    dsim = tb.Simulation(de)
+    dsim = tb.Simulation(de, precision=precision)
     dsim.set_advance("lserk", courant, rk)
     tr, _, _ = rsim.advance(0.0)
     td, _, _ = dsim.advance(0.0)
@@ -115,6 +118,20 @@ def test_tgv_full_size_matches_reference(tgv):
 
 
 @needs_ref
+def test_tgv_full_size_exact_form_equals_reference(tgv):
+    rm = ref.RefMesh((0, 0, 0), (2 * np.pi,) * 3, (N, N, N), (1, 1, 1))
+    re = ref.RefEquations(rm, True)
+    configure_tgv(re)
+    prim = taylor_green(tgv.mesh.cell_center)
+    d_ref = re.derivative(prim)
+    d_exact = tgv.derivative(prim, precision=tb.TG_PRECISION_FP64_EXACT)
+    assert np.array_equal(d_exact, d_ref), rel_l2(d_exact, d_ref)
+    tr, td, pr, pd = step_both(re, tgv, prim, 0.99, (3, 3), precision=tb.TG_PRECISION_FP64_EXACT)
+    assert td == tr
+    assert np.array_equal(pd, pr), rel_l2(pd, pr)
+
+
+@needs_ref
 def test_ramp_full_size_matches_reference():
     cells = meshes.ramp_mesh(n=(80, 80, 80))
     rm = ref.RefMesh.from_cells(cells)
@@ -124,10 +141,15 @@ def test_ramp_full_size_matches_reference():
     for e in (re, de):
         configure_ramp(e)
     prim = random_state(dm.num_cells, seed=81, mach=2.0)
-    assert rel_l2(de.derivative(prim), re.derivative(prim)).max() <= TOL
+    d_ref = re.derivative(prim)
+    assert rel_l2(de.derivative(prim), d_ref).max() <= TOL
+    assert np.array_equal(de.derivative(prim, precision=tb.TG_PRECISION_FP64_EXACT), d_ref)
     tr, td, pr, pd = step_both(re, de, prim, 0.5, (3, 3))
     assert abs(td - tr) <= 1e-13 * tr
     assert rel_l2(pd, pr).max() <= TOL
+    tr, td, pr, pd = step_both(re, de, prim, 0.5, (3, 3), precision=tb.TG_PRECISION_FP64_EXACT)
+    assert td == tr
+    assert np.array_equal(pd, pr)
 
 
 def test_tgv_full_size_conservation(tgv):

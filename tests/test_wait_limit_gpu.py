@@ -1,0 +1,59 @@
+"""The bounded device-side wait, made to run out without a fault.
+
+The staged face kernel (the Euler form's face-flux kernel, whose geometry tile arrives by bulk copies
+completing on an mbarrier) polls the barrier a bounded number of times. tg_set_wait_limit lowers that
+bound; at 0 every block gives up at once, sets ERR_TIMEOUT in the context's error word, waits (with
+the full bound) for its own copies to land and returns. The call must report TG_ERR_TIMEOUT, and the
+same context must then evaluate the residual exactly as a fresh one does: no hang, no trap, no lost
+context.
+"""
+
+import numpy as np
+import pytest
+
+import teal_b200 as tb
+from teal_b200 import _lib
+from teal_b200 import TealError
+from tests.cases import vortex
+
+pytestmark = pytest.mark.gpu
+
+
+def vortex_context():
+    m = tb.Mesh.create((0, 0, 0), (10, 10, 0.625), (16, 16, 4), (1, 1, 1))
+    e = tb.Equations.euler(m)  # Euler: the face kernel stages its geometry (tuned.h)
+    return m, e, tb.Context(m, e)
+
+
+def test_wait_that_runs_out_reports_timeout_and_leaves_the_context_usable():
+    m, e, ctx = vortex_context()
+    try:
+        prim = vortex(m.cell_center)
+        expect = ctx.derivative(prim)
+        ctx.set_wait_limit(0)
+        with pytest.raises(TealError) as err:
+            ctx.derivative(prim)
+        assert err.value.code == _lib.TG_ERR_TIMEOUT
+        assert b"gave up" in _lib.lib.tg_last_error()
+        # again: the error word was cleared, so the next give-up is reported afresh
+        with pytest.raises(TealError) as err:
+            ctx.derivative(prim)
+        assert err.value.code == _lib.TG_ERR_TIMEOUT
+        ctx.set_wait_limit()  # back to the default bound
+        assert np.array_equal(ctx.derivative(prim), expect)
+        # whole steps replayed from the step graph after the limit changed back
+        ctx.set_primitive(prim)
+        t, it, res = ctx.run(tb.TG_ADVANCE_LSERK, 0.5, 3, context=(3, 3))
+        assert it == 3 and np.all(np.isfinite(res))
+    finally:
+        ctx.close()
+
+
+def test_wait_limit_rejects_negative_polls():
+    m, e, ctx = vortex_context()
+    try:
+        with pytest.raises(TealError) as err:
+            ctx.set_wait_limit(-1)
+        assert err.value.code == _lib.TG_ERR_INVALID
+    finally:
+        ctx.close()

@@ -1,5 +1,6 @@
 """tg_residual_noalloc (the residual norm that allocates no device memory) through the C ABI against
-tg_residual on the same derivative, two calls in a row; and its size limit."""
+tg_residual on the same derivative, two calls in a row, bit for bit; that its calls leave the device's
+free memory unchanged; and the inputs it refuses."""
 
 import ctypes
 
@@ -13,7 +14,8 @@ from tests.cases import taylor_green, vortex
 
 pytestmark = pytest.mark.gpu
 
-RTOL = 1e-12  # the parity bar of the residual; both paths sum in the same order
+# Both paths sum the same products in the same order (pieces of 4096 cells, the same block shapes),
+# so the results are compared bit for bit.
 
 
 def noalloc(deriv, volume, num_cells, sum_volume, out, stream):
@@ -35,7 +37,18 @@ def check_against_context(m, e, prim):
         torch.cuda.synchronize()
         got = out.cpu().numpy()
         assert np.all(np.isfinite(got))
-        np.testing.assert_allclose(got, expect, rtol=RTOL, atol=0)
+        assert np.array_equal(got, expect), (got, expect)
+    # what the entry point exists for: after the first call's set-up, calls allocate nothing
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    held0 = torch.cuda.memory_allocated()
+    for _ in range(20):
+        _lib.check(noalloc(d, v, C, m.sum_volume, out, stream))
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, f"device free memory changed by {free0 - free1} bytes across calls"
+    assert torch.cuda.memory_allocated() == held0
+    assert np.array_equal(out.cpu().numpy(), expect)
 
 
 def test_noalloc_residual_vortex_one_piece():
@@ -65,6 +78,10 @@ def test_noalloc_rejects_sizes_beyond_the_limit():
     status = _lib.lib.tg_residual_noalloc(host.ctypes.data_as(ctypes.c_void_p), host.ctypes.data_as(ctypes.c_void_p),
                                           1, 1.0, out.data_ptr(), stream)
     assert status == _lib.TG_ERR_INVALID  # host memory is refused before any launch
+    # the divisor must be finite and positive
+    for bad in (0.0, -1.0, float("nan"), float("inf")):
+        assert noalloc(d, d, 1, bad, out, stream) == _lib.TG_ERR_INVALID
+        assert b"sum_volume" in _lib.lib.tg_last_error()
     # no cells: the norm of nothing is zero
     out.fill_(float("nan"))
     _lib.check(noalloc(d, d, 0, 1.0, out, stream))
