@@ -40,6 +40,7 @@ struct DirectGeo {
     const Geometry<R> &g;
     int F, f;
     __device__ __forceinline__ int2 cells(int) const { return g.lr[f]; }
+    __device__ __forceinline__ V3<R> normal(int) const { return load_v3(g.basis, F, f); }
     __device__ __forceinline__ Basis<R> basis(int) const { return load_basis(g.basis, F, f); }
     // the basis again later in the thread: re-read (L1) instead of kept live in registers
     __device__ __forceinline__ Basis<R> basis_again(int) const { return reload_basis(g.basis, F, f); }
@@ -57,13 +58,16 @@ struct DirectGeo {
 // Geometry of one tile of FACE_BLOCK consecutive faces in shared memory, staged by bulk
 // asynchronous copies (one per SoA row, all in flight at once, completing on one mbarrier) so the
 // streamed face geometry costs the threads neither registers nor load instructions; rows: area,
-// basis (9), offsets left / right (3 + 3, second order), correction (4, Navier-Stokes).
+// basis (9 in the exact form; the normal's 3 otherwise, see frame_of), offsets left / right
+// (3 + 3, second order), correction (4, Navier-Stokes).
 template <typename R, int ORDER, bool NS>
 struct FaceTile {
     static constexpr int PAD = 16 / int(sizeof(R));
     static constexpr int SROW = FACE_BLOCK + PAD;
-    static constexpr int ROWS = 10 + (ORDER == 2 ? 6 + (NS ? 4 : 0) : 0);
-    static constexpr int R_AREA = 0, R_BASIS = 1, R_OFFL = 10, R_OFFR = 13, R_CORR = (ORDER == 2) ? 16 : 10;
+    static constexpr int NBASIS = kExact ? 9 : 3;
+    static constexpr int ROWS = 1 + NBASIS + (ORDER == 2 ? 6 + (NS ? 4 : 0) : 0);
+    static constexpr int R_AREA = 0, R_BASIS = 1, R_OFFL = 1 + NBASIS, R_OFFR = R_OFFL + 3;
+    static constexpr int R_CORR = (ORDER == 2) ? R_OFFR + 3 : R_OFFL;
     R geo[ROWS][SROW];
     int2 lr[FACE_BLOCK + 2];
     uint64_t bar;
@@ -72,7 +76,7 @@ struct FaceTile {
     __device__ __forceinline__ const R *row_src(const Geometry<R> &g, int F, int r) const
     {
         if (r == R_AREA) return g.area;
-        if (r < R_BASIS + 9) return g.basis + (size_t)(r - R_BASIS) * F;
+        if (r < R_BASIS + NBASIS) return g.basis + (size_t)(r - R_BASIS) * F;
         if (ORDER == 2 && r < R_OFFL + 3) return g.offl + (size_t)(r - R_OFFL) * F;
         if (ORDER == 2 && r < R_OFFR + 3) return g.offr + (size_t)(r - R_OFFR) * F;
         return g.corr + (size_t)(r - R_CORR) * F;
@@ -112,16 +116,20 @@ struct FaceTile {
     __device__ __forceinline__ R at(int r, int i) const { return geo[r][shift[r] + i]; }
     __device__ __forceinline__ V3<R> v3_at(int r, int i) const { return v3(at(r, i), at(r + 1, i), at(r + 2, i)); }
     __device__ __forceinline__ int2 cells(int i) const { return lr[shift[ROWS] + i]; }
+    __device__ __forceinline__ V3<R> normal(int i) const { return v3_at(R_BASIS, i); }
+    template <int NB = NBASIS>
     __device__ __forceinline__ Basis<R> basis(int i) const
     {
+        static_assert(NB == 9, "the full basis is staged in the exact form only");
         Basis<R> b;
         b.x = v3_at(R_BASIS, i);
         b.y = v3_at(R_BASIS + 3, i);
         b.z = v3_at(R_BASIS + 6, i);
         return b;
     }
-    __device__ __forceinline__ Basis<R> basis_again(int i) const { return basis(i); }
-    __device__ __forceinline__ V3<R> normal_again(int i) const { return v3_at(R_BASIS, i); }
+    template <int NB = NBASIS>
+    __device__ __forceinline__ Basis<R> basis_again(int i) const { return basis<NB>(i); }
+    __device__ __forceinline__ V3<R> normal_again(int i) const { return normal(i); }
     __device__ __forceinline__ V3<R> offl(int i) const { return v3_at(R_OFFL, i); }
     __device__ __forceinline__ V3<R> offr(int i) const { return v3_at(R_OFFR, i); }
     __device__ __forceinline__ R area(int i) const { return at(R_AREA, i); }
@@ -166,7 +174,14 @@ __device__ __forceinline__ void face_flux(const Geo &geo, int i, int f, const Si
                 ql = load_prim<R>(q, N, c.x);
                 qr = load_prim<R>(q, N, c.y);
             }
-            Basis<R> b = geo.basis(i);
+            // the stored basis in the exact form; the normal and tangents of its own otherwise
+            Basis<R> b;
+            if constexpr (kExact) {
+                b = geo.basis(i);
+            }
+            else {
+                b = frame_of(geo.normal(i));
+            }
             if (ORDER == 1) {
                 l = make_local(ql, gamma, b, R(pref));
                 r = make_local(qr, gamma, b, R(pref));
@@ -185,7 +200,12 @@ __device__ __forceinline__ void face_flux(const Geo &geo, int i, int f, const Si
             }
         }
         fc = convective_flux_local<FK>(l, r, gamma);
-        fc.m = to_global(geo.basis_again(i), fc.m);
+        if constexpr (kExact) {
+            fc.m = to_global(geo.basis_again(i), fc.m);
+        }
+        else {
+            fc.m = to_global(frame_of(geo.normal_again(i)), fc.m);
+        }
     }
     R area = geo.area(i);
     R gf[5] = {fc.rho * area, fc.m.x * area, fc.m.y * area, fc.m.z * area, fc.e * area};

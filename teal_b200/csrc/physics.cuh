@@ -77,6 +77,25 @@ __device__ __forceinline__ V3<R> to_global(const Basis<R> &b, V3<R> v)
             dot(v3(b.x.z, b.y.z, b.z.z), v)};
 }
 
+// Face frame from the unit normal alone: tangents t1, t2 with (n, t1, t2) orthonormal, branch-free
+// (Duff, Burgess, Christensen, Hart, Kensler, Liani, Villemin: "Building an Orthonormal Basis,
+// Revisited", JCGT 6(1), 2017). The convective fluxes treat the two tangential directions alike and
+// linearly (and the kinetic energy is |u|^2), so they are invariant under a rotation or reflection
+// of the frame about the normal: any such tangents serve in place of the mesh's stored ones, up to
+// rounding, and the plain kernels read only the normal row of the stored basis.
+template <typename R>
+__device__ __forceinline__ Basis<R> frame_of(V3<R> n)
+{
+    const R sg = copysign(R(1), n.z);
+    const R a = R(-1) / (sg + n.z);
+    const R b = (n.x * n.y) * a;
+    Basis<R> f;
+    f.x = n;
+    f.y = v3(R(1) + ((sg * (n.x * n.x)) * a), sg * b, -sg * n.x);
+    f.z = v3(b, sg + ((n.y * n.y) * a), -n.y);
+    return f;
+}
+
 // primitive state: density, velocity, pressure (src/euler.h EulerPrimitive)
 template <typename R>
 struct Prim {
