@@ -11,7 +11,7 @@
 namespace tg {
 
 // bits of the device error word (Steps::error)
-enum DeviceError { ERR_NONFINITE = 1, ERR_TIMEOUT = 2 };
+enum DeviceError { ERR_NONFINITE = 1, ERR_TIMEOUT = 2, ERR_LOOP_LIMIT = 4 };
 
 constexpr int BLOCK = 256;
 constexpr int FACE_BLOCK = TG_FACE_BLOCK;

@@ -171,7 +171,7 @@ struct Gmres {
     double *sc = nullptr;     // per-instance device scalars (GmresScalar)
     int *flag = nullptr;      // per-instance progress (GmresFlag)
     int *count = nullptr;     // [2] instances still iterating (Newton, Arnoldi)
-    int *hcount = nullptr;    // pinned host copy of count
+    int *ctl = nullptr;       // [GC_COUNT] loop counters of the graph-driven loops
 };
 
 // Host mirror of the per-instance step arrays (pinned; one copy per direction moves all of them):
@@ -274,6 +274,13 @@ struct tg_ctx {
 
     // polls of the staged face kernel's first bounded wait (lowered only by tg_set_wait_limit)
     int wait_polls = MBAR_POLLS;
+
+    // implicit step graph (device-driven Newton / Arnoldi / Gram-Schmidt loops) and its key
+    cudaGraphExec_t igraph = nullptr;
+    long igraph_kernels = 0;
+    double ig_courant = 0, ig_newton_tol = 0, ig_krylov_tol = 0;
+    int ig_dim = 0, ig_use_max_time = -1;
+    cudaStream_t cap_stream[3] = {nullptr, nullptr, nullptr};  // body captures of nested loops
 };
 
 static double &hd_at(tg_ctx *c, int field, int i) { return c->hd[(size_t)field * c->ninst + i]; }
@@ -318,6 +325,10 @@ static void free_ctx(tg_ctx *c)
         cudaEventDestroy(p.second.second);
     }
     if (c->graph) cudaGraphExecDestroy(c->graph);
+    if (c->igraph) cudaGraphExecDestroy(c->igraph);
+    for (cudaStream_t s : c->cap_stream) {
+        if (s) cudaStreamDestroy(s);
+    }
     void *ptrs[] = {c->bcenter, c->ccenter, c->S, c->dprop, c->pref,
                     c->lr, c->slot_nbr, c->slot_face, c->slot_cnt, c->owner, c->bface_ent, c->bkind, c->bctx,
                     c->volume, c->proj, c->eps2, c->gb.area, c->gb.basis, c->gb.offl, c->gb.offr, c->gb.corr,
@@ -329,8 +340,7 @@ static void free_ctx(tg_ctx *c)
         if (p) cudaFree(p);
     }
     void *gp[] = {c->gm.U, c->gm.Ustart, c->gm.r, c->gm.delta, c->gm.V, c->gm.w, c->gm.q1, c->gm.R1,
-                  c->gm.part, c->gm.sc, c->gm.flag, c->gm.count};
-    if (c->gm.hcount) cudaFreeHost(c->gm.hcount);
+                  c->gm.part, c->gm.sc, c->gm.flag, c->gm.count, c->gm.ctl};
     for (void *p : gp) {
         if (p) cudaFree(p);
     }
@@ -992,6 +1002,10 @@ static void drop_graph(tg_ctx *c)
         cudaGraphExecDestroy(c->graph);
         c->graph = nullptr;
     }
+    if (c->igraph) {
+        cudaGraphExecDestroy(c->igraph);
+        c->igraph = nullptr;
+    }
 }
 
 extern "C" int tg_function_register(const char *name, int kind, const char *source, char *log, long log_size)
@@ -1097,11 +1111,8 @@ extern "C" int tg_set_stream(tg_ctx *c, void *stream)
     if (!c) return fail(TG_ERR_INVALID, "null context");
     CU(cudaStreamSynchronize(c->stream));
     c->stream = stream ? (cudaStream_t)stream : c->own_stream;
-    if (c->graph) {
-        cudaGraphExecDestroy(c->graph);
-        c->graph = nullptr;
-        c->graph_method = -1;
-    }
+    drop_graph(c);
+    c->graph_method = -1;
     return TG_OK;
 }
 
@@ -1533,6 +1544,9 @@ static int check_error(tg_ctx *c)
         hi_error(c) = 0;
         write_steps(c);
         if (e & ERR_TIMEOUT) return fail(TG_ERR_TIMEOUT, "a device-side wait for staged face geometry gave up");
+        if (e & ERR_LOOP_LIMIT)
+            return fail(TG_ERR_TIMEOUT, "an implicit step reached the device limit of %d Newton iterations",
+                        NEWTON_LOOP_LIMIT);
         return fail(TG_ERR_NONFINITE, "non-finite time step or residual");
     }
     return TG_OK;
@@ -1902,11 +1916,10 @@ static int gm_alloc(tg_ctx *c, int dim)
 {
     Gmres &g = c->gm;
     if (g.V && g.dim >= dim) return TG_OK;
-    void *old[] = {g.U, g.Ustart, g.r, g.delta, g.V, g.w, g.q1, g.R1, g.part, g.sc, g.flag, g.count};
+    void *old[] = {g.U, g.Ustart, g.r, g.delta, g.V, g.w, g.q1, g.R1, g.part, g.sc, g.flag, g.count, g.ctl};
     for (void *p : old) {
         if (p) cudaFree(p);
     }
-    if (g.hcount) cudaFreeHost(g.hcount);
     g = Gmres{};
     size_t n = 5 * (size_t)c->s.C;
     TRY(dalloc(&g.U, n));
@@ -1923,14 +1936,16 @@ static int gm_alloc(tg_ctx *c, int dim)
     TRY(dalloc(&g.flag, (size_t)GF_COUNT * c->ninst));
     CU(cudaMemset(g.flag, 0, sizeof(int) * GF_COUNT * c->ninst));
     TRY(dalloc(&g.count, 2));
-    CU(cudaMallocHost(&g.hcount, 2 * sizeof(int)));
+    TRY(dalloc(&g.ctl, GC_COUNT));
+    CU(cudaMemset(g.ctl, 0, sizeof(int) * GC_COUNT));
     g.dim = dim;
+    drop_graph(c);  // a captured implicit step refers to the old workspace
     return TG_OK;
 }
 
 static GmresBatch gm_batch(tg_ctx *c, int dim)
 {
-    return GmresBatch{dim, gmres_scn(dim), c->ninst, c->cell_inst, c->gm.sc, c->gm.flag, c->gm.count};
+    return GmresBatch{dim, gmres_scn(dim), c->ninst, c->cell_inst, c->gm.sc, c->gm.flag, c->gm.count, c->gm.ctl};
 }
 
 // sc[instance][slot] = x . y (or its square root) for the instances whose flag `which` is set
@@ -1948,12 +1963,58 @@ static int inst_grid(const tg_ctx *c)
     return (c->ninst + 127) / 128;
 }
 
-// instances still iterating, as counted by the kernel just enqueued after a reset of the counter
-static int gm_count(tg_ctx *c, int which, int *out)
+// ---- device-driven loops of a captured graph ---------------------------------------------------
+//
+// A loop whose trip count only the device knows becomes a conditional WHILE node of the graph
+// being captured on c->stream: while_begin creates the node's condition handle in that graph,
+// enqueues `init` (a kernel that sets the condition before the node runs, every time the node is
+// reached), appends the node and captures its body on a side stream until while_end. The body's
+// last kernel sets the condition for the next round.
+
+struct WhileLoop {
+    cudaStream_t outer = nullptr;
+    cudaGraphConditionalHandle h = 0;
+};
+
+template <typename Init>
+static int while_begin(tg_ctx *c, WhileLoop &w, int depth, Init init)
 {
-    CU(cudaMemcpyAsync(c->gm.hcount + which, c->gm.count + which, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    CU(cudaStreamSynchronize(c->stream));
-    *out = c->gm.hcount[which];
+    cudaStreamCaptureStatus status;
+    cudaGraph_t graph = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    CU(cudaStreamGetCaptureInfo(c->stream, &status, nullptr, &graph, &deps, &ndeps));
+    if (status != cudaStreamCaptureStatusActive) return fail(TG_ERR_INVALID, "device loops need a stream capture");
+    CU(cudaGraphConditionalHandleCreate(&w.h, graph, 0, 0));
+    init(w.h);
+    CU(cudaGetLastError());
+    CU(cudaStreamGetCaptureInfo(c->stream, &status, nullptr, &graph, &deps, &ndeps));
+    cudaGraphNodeParams params = {};
+    params.type = cudaGraphNodeTypeConditional;
+    params.conditional.handle = w.h;
+    params.conditional.type = cudaGraphCondTypeWhile;
+    params.conditional.size = 1;
+    cudaGraphNode_t node;
+    CU(cudaGraphAddNode(&node, graph, deps, ndeps, &params));
+    CU(cudaStreamUpdateCaptureDependencies(c->stream, &node, 1, cudaStreamSetCaptureDependencies));
+    if (!c->cap_stream[depth]) CU(cudaStreamCreateWithFlags(&c->cap_stream[depth], cudaStreamNonBlocking));
+    w.outer = c->stream;
+    c->stream = c->cap_stream[depth];
+    cudaError_t e = cudaStreamBeginCaptureToGraph(c->stream, params.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                  cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        c->stream = w.outer;
+        CU(e);
+    }
+    return TG_OK;
+}
+
+static int while_end(tg_ctx *c, WhileLoop &w)
+{
+    cudaGraph_t body = nullptr;
+    cudaError_t e = cudaStreamEndCapture(c->stream, &body);
+    c->stream = w.outer;
+    CU(e);
     return TG_OK;
 }
 
@@ -1967,40 +2028,60 @@ static int gm_derivative(tg_ctx *c, double *q, double *Rout)
     return TG_OK;
 }
 
-// one GMRES cycle for the increment of every Newton instance (gmres.c:52-149)
+// one GMRES cycle for the increment of every Newton instance (gmres.c:52-149): the Arnoldi
+// iterations and each column's Gram-Schmidt rows are device loops (a finished instance is masked
+// out of every vector update); each Gram-Schmidt dot is fused with the update of the row before it
 static int gm_solve(tg_ctx *c, const GmresBatch &gb, double krylov_tol)
 {
     Gmres &g = c->gm;
     const int C = c->s.C, cb = grid_of(C), ib = inst_grid(c);
-    const size_t n = 5 * (size_t)C;
     k_gmres_begin<<<ib, 128, 0, c->stream>>>(gb, krylov_tol);
     k_gmres_start<<<cb, BLOCK, 0, c->stream>>>(C, g.r, gb, g.V, g.delta);
     CU(cudaGetLastError());
-    for (int m = 0; m < gb.dim; m++) {
-        double *Vm = g.V + (size_t)m * n;
+    c->launches += 2;
+    WhileLoop arnoldi;
+    TRY(while_begin(c, arnoldi, 1, [&](cudaGraphConditionalHandle h) {
+        k_arnoldi_enter<<<1, 256, 0, c->stream>>>(gb, h);
+        c->launches += 1;
+    }));
+    {
         // matvec (gmres.c:12-50)
-        TRY(gm_dot(c, gb, Vm, Vm, GF_ARNOLDI, GS_VNORM, 1));
-        k_perturb<<<cb, BLOCK, 0, c->stream>>>(C, c->s.N, g.U, Vm, gb, c->prop[0], g.q1);
+        k_piece_vnorm<<<c->npieces, BLOCK, 0, c->stream>>>(c->seg, C, g.V, gb, g.part);
+        k_inst_dot_at<<<c->ninst, GM_INST_BLOCK, 0, c->stream>>>(c->seg, g.part, gb, 2);
+        k_perturb_at<<<cb, BLOCK, 0, c->stream>>>(C, c->s.N, g.U, g.V, gb, c->prop[0], g.q1);
         CU(cudaGetLastError());
+        c->launches += 3;
         TRY(gm_derivative(c, g.q1, g.R1));
-        k_matvec_finish<<<cb, BLOCK, 0, c->stream>>>(C, Vm, g.R1, c->R, gb, g.w);
-        // modified Gram-Schmidt
-        for (int i = 0; i <= m; i++) {
-            TRY(gm_dot(c, gb, g.V + (size_t)i * n, g.w, GF_ARNOLDI, GS_HEAD + i * gb.dim + m, 0));
-            k_mgs_axpy<<<cb, BLOCK, 0, c->stream>>>(C, g.V + (size_t)i * n, gb, i, m, g.w);
-        }
-        TRY(gm_dot(c, gb, g.w, g.w, GF_ARNOLDI, GS_HEAD + (m + 1) * gb.dim + m, 1));
-        CU(cudaMemsetAsync(g.count + 1, 0, sizeof(int), c->stream));
-        k_givens<<<ib, 128, 0, c->stream>>>(gb, m);
+        k_matvec_finish_at<<<cb, BLOCK, 0, c->stream>>>(C, g.V, g.R1, c->R, gb, g.w);
         CU(cudaGetLastError());
-        int going;
-        TRY(gm_count(c, 1, &going));
-        if (going == 0) break;
-        k_normalize<<<cb, BLOCK, 0, c->stream>>>(C, g.w, gb, m, g.V + (size_t)(m + 1) * n);
+        c->launches += 1;
+        // modified Gram-Schmidt rows 0..k
+        WhileLoop mgs;
+        TRY(while_begin(c, mgs, 2, [&](cudaGraphConditionalHandle h) {
+            k_mgs_enter<<<1, 1, 0, c->stream>>>(gb, h);
+            c->launches += 1;
+        }));
+        k_mgs_piece<<<c->npieces, BLOCK, 0, c->stream>>>(c->seg, C, g.V, gb, 0, g.w, g.part);
+        k_inst_dot_at<<<c->ninst, GM_INST_BLOCK, 0, c->stream>>>(c->seg, g.part, gb, 0);
+        k_mgs_next<<<1, 1, 0, c->stream>>>(gb, mgs.h);
+        CU(cudaGetLastError());
+        c->launches += 3;
+        TRY(while_end(c, mgs));
+        // the last row's update and the norm of w
+        k_mgs_piece<<<c->npieces, BLOCK, 0, c->stream>>>(c->seg, C, g.V, gb, 1, g.w, g.part);
+        k_inst_dot_at<<<c->ninst, GM_INST_BLOCK, 0, c->stream>>>(c->seg, g.part, gb, 1);
+        CU(cudaMemsetAsync(g.count + 1, 0, sizeof(int), c->stream));
+        k_givens_at<<<ib, 128, 0, c->stream>>>(gb);
+        k_normalize_at<<<cb, BLOCK, 0, c->stream>>>(C, g.w, gb, g.V);
+        k_arnoldi_next<<<1, 1, 0, c->stream>>>(gb, arnoldi.h);
+        CU(cudaGetLastError());
+        c->launches += 5;
     }
+    TRY(while_end(c, arnoldi));
     k_backsolve<<<ib, 128, 0, c->stream>>>(gb);
     k_accumulate<<<cb, BLOCK, 0, c->stream>>>(C, g.V, gb, g.delta);
     CU(cudaGetLastError());
+    c->launches += 2;
     return TG_OK;
 }
 
@@ -2019,15 +2100,12 @@ static int newton_params(const void *context, double *newton_tol, double *krylov
     return TG_OK;
 }
 
-// One implicit Euler step of every active instance (advance.c:119-195): CFL step, Newton iterations
-// with a GMRES solve each, then the residual norm and the run loop's time / iteration / stop
-// bookkeeping (k_inst_end). The device step arrays must be current.
-static int implicit_step_all(tg_ctx *c, const void *context, double courant)
+// One implicit Euler step of every active instance (advance.c:119-195), enqueued on a capturing
+// stream: CFL step, Newton iterations (a device loop) with a GMRES solve each, then the residual
+// norm and the run loop's time / iteration / stop bookkeeping (k_inst_end). The device step arrays
+// must be current when the graph runs.
+static int enqueue_implicit_step(tg_ctx *c, double courant, double newton_tol, double krylov_tol, int dim)
 {
-    double newton_tol, krylov_tol;
-    int dim;
-    TRY(newton_params(context, &newton_tol, &krylov_tol, &dim));
-    TRY(gm_alloc(c, dim));
     Gmres &g = c->gm;
     const GmresBatch gb = gm_batch(c, dim);
     const int C = c->s.C, cb = grid_of(C), ib = inst_grid(c);
@@ -2055,13 +2133,16 @@ static int implicit_step_all(tg_ctx *c, const void *context, double courant)
     TRY(gm_dot(c, gb, g.U, g.U, GF_NEWTON, GS_CONS_NORM, 1));
     k_fd_scale<<<ib, 128, 0, c->stream>>>(gb, fd_rel, newton_tol, 1);
     CU(cudaGetLastError());
-    for (;;) {
-        CU(cudaMemsetAsync(g.count, 0, sizeof(int), c->stream));
+    c->launches += 4;
+    auto newton_check = [&](cudaGraphConditionalHandle h, int enter) {
+        cudaMemsetAsync(g.count, 0, sizeof(int), c->stream);
         k_newton_check<<<ib, 128, 0, c->stream>>>(gb, c->seg, c->st.error);
-        CU(cudaGetLastError());
-        int going;
-        TRY(gm_count(c, 0, &going));
-        if (going == 0) break;
+        k_newton_next<<<1, 1, 0, c->stream>>>(gb, h, enter, c->st.error);
+        c->launches += 2;
+    };
+    WhileLoop newton;
+    TRY(while_begin(c, newton, 0, [&](cudaGraphConditionalHandle h) { newton_check(h, 1); }));
+    {
         TRY(gm_solve(c, gb, krylov_tol));
         k_newton_update<<<cb, BLOCK, 0, c->stream>>>(C, c->s.N, g.U, g.delta, gb, c->prop[0], c->q);
         CU(cudaGetLastError());
@@ -2072,7 +2153,11 @@ static int implicit_step_all(tg_ctx *c, const void *context, double courant)
         TRY(gm_dot(c, gb, g.U, g.U, GF_NEWTON, GS_CONS_NORM, 1));
         k_fd_scale<<<ib, 128, 0, c->stream>>>(gb, fd_rel, newton_tol, 0);
         CU(cudaGetLastError());
+        c->launches += 3;
+        newton_check(newton.h, 0);
+        CU(cudaGetLastError());
     }
+    TRY(while_end(c, newton));
     // residual of the last derivative (advance.c:188), time, iteration and the run loop's tests
     TRY(run_pieces(c, 1));
     {
@@ -2081,6 +2166,59 @@ static int implicit_step_all(tg_ctx *c, const void *context, double courant)
         k_count_active<<<1, 256, 0, c->stream>>>(c->ninst, c->st);
     }
     CU(cudaGetLastError());
+    return TG_OK;
+}
+
+// One implicit Euler step of every active instance: a replay of the step's graph, captured on first
+// use for these parameters. The host waits for nothing inside the step.
+static int implicit_step_all(tg_ctx *c, const void *context, double courant)
+{
+    double newton_tol, krylov_tol;
+    int dim;
+    TRY(newton_params(context, &newton_tol, &krylov_tol, &dim));
+    TRY(gm_alloc(c, dim));
+    if (!(c->igraph && c->ig_courant == courant && c->ig_newton_tol == newton_tol &&
+          c->ig_krylov_tol == krylov_tol && c->ig_dim == dim && c->ig_use_max_time == c->st.use_max_time)) {
+        if (c->igraph) {
+            cudaGraphExecDestroy(c->igraph);
+            c->igraph = nullptr;
+        }
+        cudaGraph_t graph;
+        CU(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        const long before = c->launches;
+        const bool prof = c->prof_on;
+        c->prof_on = false;  // no event records inside the graph
+        cudaStream_t outer = c->stream;
+        int rc = enqueue_implicit_step(c, courant, newton_tol, krylov_tol, dim);
+        c->stream = outer;  // restored even when a loop body's capture failed half way
+        c->prof_on = prof;
+        if (rc != TG_OK) {  // close loop-body captures left open by the failure
+            for (cudaStream_t side : c->cap_stream) {
+                cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+                if (side && cudaStreamIsCapturing(side, &st) == cudaSuccess && st != cudaStreamCaptureStatusNone) {
+                    cudaGraph_t body = nullptr;
+                    cudaStreamEndCapture(side, &body);
+                }
+            }
+            cudaGetLastError();
+        }
+        c->igraph_kernels = c->launches - before;
+        c->launches = before;
+        cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+        if (rc != TG_OK) {
+            if (e == cudaSuccess) cudaGraphDestroy(graph);
+            return rc;
+        }
+        CU(e);
+        cudaError_t e2 = cudaGraphInstantiate(&c->igraph, graph, 0);
+        cudaGraphDestroy(graph);
+        CU(e2);
+        c->ig_courant = courant, c->ig_newton_tol = newton_tol, c->ig_krylov_tol = krylov_tol;
+        c->ig_dim = dim, c->ig_use_max_time = c->st.use_max_time;
+    }
+    CU(cudaGraphLaunch(c->igraph, c->stream));
+    c->launches += c->igraph_kernels;
+    c->prepared = false;
     return TG_OK;
 }
 

@@ -1,4 +1,4 @@
-"""The bounded device-side wait, made to run out without a fault.
+"""Bounded device-side waits and loops, made to run out without a fault.
 
 The staged face kernel (the Euler form's face-flux kernel, whose geometry tile arrives by bulk copies
 completing on an mbarrier) polls the barrier a bounded number of times. tg_set_wait_limit lowers that
@@ -55,5 +55,25 @@ def test_wait_limit_rejects_negative_polls():
         with pytest.raises(TealError) as err:
             ctx.set_wait_limit(-1)
         assert err.value.code == _lib.TG_ERR_INVALID
+    finally:
+        ctx.close()
+
+
+def test_newton_loop_of_the_step_graph_is_bounded():
+    """The implicit step's Newton loop runs on the device (a conditional node of the step's graph).
+    With a Newton tolerance no iteration can meet, teal's own bound (128 (cells + 1) iterations)
+    would keep the device busy for a long time; the graph stops after 1000 iterations and the call
+    reports TG_ERR_TIMEOUT. The context then takes a normal implicit step."""
+    m, e, ctx = vortex_context()
+    try:
+        prim = vortex(m.cell_center)
+        ctx.set_primitive(prim)
+        with pytest.raises(TealError) as err:
+            ctx.advance(tb.TG_ADVANCE_IMPLICIT_EULER, 5.0, 0.0, context=(1e-300, 0.3, 2))
+        assert err.value.code == _lib.TG_ERR_TIMEOUT
+        assert b"Newton iterations" in _lib.lib.tg_last_error()
+        ctx.set_primitive(prim)
+        t, s0, res = ctx.advance(tb.TG_ADVANCE_IMPLICIT_EULER, 5.0, 0.0, context=(0.1, 0.3, 10))
+        assert t > 0 and np.all(np.isfinite(res))
     finally:
         ctx.close()
