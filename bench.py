@@ -397,7 +397,7 @@ def batch_specs(count, seed=11, lo=8_000, hi=512_000):
     return out
 
 
-def batch_problem(spec):
+def batch_problem(spec, flux="ausmd", limiter=("minmod", 0.0)):
     """Euler on a mixed-element ramp mesh, far field around, slip walls at the ramp and the sides
     (valid for subsonic and supersonic free streams), starting from the free stream."""
     import teal_b200 as tb
@@ -406,8 +406,8 @@ def batch_problem(spec):
     n, mach, angle, mseed = spec
     m = tb.Mesh.from_cells(meshes.ramp_mesh(n=(n, n, n), seed=mseed))
     e = tb.Equations.euler(m)
-    e.set_convective_flux("ausmd")
-    e.set_limiter("minmod", 0.0)
+    e.set_convective_flux(flux)
+    e.set_limiter(*limiter)
     free = serving.free_stream(mach, angle)
     for side in ("left", "right", "top"):
         e.set_boundary_condition(side, "farfield", free)
@@ -415,6 +415,78 @@ def batch_problem(spec):
         e.set_boundary_condition(side, "slipwall")
     e.primitive[:] = np.tile(free, (m.num_cells, 1))
     return e
+
+
+def run_batch_implicit(args, specs):
+    """Batched steady solves: every instance takes implicit Euler steps until its
+    maximum residual has dropped by `--drop` (1e-8) from its first step's, or `--steps` steps, in
+    FP64 and in the FP32-matvec form (FP64 Newton residuals and Arnoldi, FP32 fluxes in the
+    finite-difference matvec); all instances in one arena, each step one CUDA-graph launch with
+    device-driven Newton / Arnoldi / Gram-Schmidt loops. The scheme is teal's steady airfoil case's
+    (run/airfoil/run.c: hllc, Venkatakrishnan(1), Newton-Krylov {0.1, 0.3, 30}) at CFL 30: from the
+    uniform start CFL 100 ends in non-finite residuals in the first step on some instances, and with
+    teal's global time step (the minimum over a mesh's cells) the drop per step is slow on these
+    mixed meshes, so the run reports how far each instance got. cell-updates/s = sum over instances
+    of cells x steps taken / device time."""
+    import torch
+
+    import teal_b200 as tb
+
+    t0 = time.perf_counter()
+    problems = [batch_problem(sp, flux="hllc", limiter=("venkatakrishnan", 1.0)) for sp in specs]
+    t_setup = time.perf_counter() - t0
+    method = tb.TG_ADVANCE_IMPLICIT_EULER
+    courant = args.courant if args.courant else 30.0
+    context = (0.1, 0.3, 30)
+    n = len(problems)
+    cells = np.array([e.mesh.num_inner_cells for e in problems], dtype=np.float64)
+    stream = torch.cuda.Stream()
+    out, states = {}, {}
+    for name, prec in (("fp64", tb.TG_PRECISION_FP64), ("fp32_matvec", tb.TG_PRECISION_FP32_FLUX)):
+        b = tb.Batch(problems, precision=prec)
+        b.set_stream(stream.cuda_stream)
+        torch.cuda.synchronize()
+        # the first step sets each instance's reference residual (and captures the step graph)
+        t, it, res = b.run(method, courant, 1, context=context)
+        first = res.max(axis=1)
+        thr = np.where(first > 0, args.drop * first, 0.0)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        t, it, res = b.run(method, courant, args.steps, variable=-1, threshold=thr, context=context, time=t)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        secs = ev0.elapsed_time(ev1) / 1000.0
+        steps = it.astype(np.float64)
+        drop = res.max(axis=1) / np.maximum(first, 1e-300)
+        out[name] = {"value": float((cells * steps).sum() / secs), "seconds": secs,
+                     "converged": int((drop <= args.drop).sum()), "instances": n,
+                     "steps_taken_max": int(steps.max()), "drop_p50": float(np.percentile(drop, 50)),
+                     "drop_max": float(drop.max()), "drop_min": float(drop.min())}
+        states[name] = [b.get_primitive(i)[: e.mesh.num_inner_cells].copy() for i, e in enumerate(problems)]
+        b.close()
+    err_var = np.zeros(5)
+    for a, f in zip(states["fp64"], states["fp32_matvec"]):
+        d = np.sqrt(((f - a) ** 2).sum(axis=0)) / np.maximum(np.sqrt((a ** 2).sum(axis=0)), 1e-300)
+        err_var = np.maximum(err_var, d)
+    steps_max = max(1, out["fp32_matvec"]["steps_taken_max"])
+    line = {
+        "metric": "cell-updates/s batched implicit steady solves (FP32-matvec / FP64 Newton-Arnoldi)",
+        "value": out["fp32_matvec"]["value"], "unit": "cell-updates/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": 1, "ms_per_step": 1000 * out["fp32_matvec"]["seconds"] / steps_max,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32-matvec-flux/f64-newton-arnoldi", "data": "synthetic",
+        "config": {"workload": f"{n} euler ramp meshes (tets/prisms/hexes/pyramids), 8k-512k cells log-uniform, "
+                               f"mach 0.3-3.0, angle 0-10 deg, hllc + venkatakrishnan(1), farfield + slip walls, "
+                               f"implicit euler cfl {courant:g}, newton-krylov {{0.1, 0.3, 30}}, until a "
+                               f"{args.drop:g} relative residual drop or {args.steps} steps",
+                   "cells": int(cells.sum()), "instances": n},
+        "fp64": out["fp64"], "fp32_matvec": out["fp32_matvec"],
+        "fp32_matvec_over_fp64": out["fp32_matvec"]["value"] / out["fp64"]["value"],
+        "fp32_matvec_rel_l2_vs_fp64_per_primitive": err_var.tolist(),
+        "setup_s": t_setup,
+    }
+    print(json.dumps(line))
 
 
 def run_batch(args, world, rank):
@@ -429,6 +501,8 @@ def run_batch(args, world, rank):
         return
     torch.cuda.set_device(0)
     specs = batch_specs(args.instances)
+    if args.method == "implicit" and args.drop > 0:
+        return run_batch_implicit(args, specs)
     t0 = time.perf_counter()
     problems = [batch_problem(sp) for sp in specs]
     t_setup = time.perf_counter() - t0
@@ -551,6 +625,9 @@ def main():
                          "serve: the solve server under Poisson arrivals; batch: many meshes in one arena")
     ap.add_argument("--instances", type=int, default=64, help="batch: meshes in the arena")
     ap.add_argument("--method", default="lserk", choices=["lserk", "implicit"], help="batch: time integrator")
+    ap.add_argument("--drop", type=float, default=1e-8,
+                    help="batch implicit: run each instance to this relative residual drop (0: fixed --steps)")
+    ap.add_argument("--courant", type=float, default=None, help="batch implicit: CFL number (default 30)")
     ap.add_argument("--solo-sample", type=int, default=16, help="batch: meshes timed one at a time")
     ap.add_argument("--requests", type=int, default=16, help="serve: number of requests")
     ap.add_argument("--rate", type=float, default=8.0, help="serve: arrivals per second")

@@ -256,10 +256,17 @@ int tg_batch_set_primitive(tg_ctx *ctx, int instance, const double *primitive);
 int tg_batch_get_primitive(tg_ctx *ctx, int instance, double *primitive);
 /* Run every instance until its own limit: max_iter[i] steps, max_time[i] (null: none), or the
  * residual of variable[i] (-1: maximum; null: all -1) below threshold[i] (null or <= 0: none).
- * time[i] is read and updated; iter[i] and residual[i][5] return the end state. Explicit methods. */
+ * time[i] is read and updated; iter[i] and residual[i][5] return the end state. Every method
+ * (explicit, and implicit Euler with each instance's own Newton-GMRES). An instance whose time step
+ * or residual becomes non-finite stops on its own while the others go on (a single-mesh context
+ * returns TG_ERR_NONFINITE instead): tg_batch_status reports it, and it stays stopped until
+ * tg_batch_set_primitive gives it a new state. */
 int tg_batch_run(tg_ctx *ctx, int method, const void *context, double courant, const int *max_iter,
                  const double *max_time, const int *variable, const double *threshold, double *time,
                  int *iter, double *residual);
+/* status[i] = TG_OK, or TG_ERR_NONFINITE for an instance that stopped on a non-finite value. No
+ * counterpart in teal (one mesh per process there). */
+int tg_batch_status(tg_ctx *ctx, int *status);
 
 /* ---- drop-in Advance methods with teal's signature (src/simulation.h:6-7) ----------------------- */
 

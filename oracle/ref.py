@@ -40,6 +40,7 @@ def lib():
             "ref_mesh_validate": (None, [vp]),
             "ref_mesh_destroy": (None, [vp]),
             "ref_mesh_counts": (None, [vp, ctypes.POINTER(ctypes.c_long)]),
+            "ref_kdtree_nearest": (None, [dp, ctypes.c_int, dp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
             "ref_mesh_sum_volume": (ctypes.c_double, [vp]),
             "ref_mesh_array": (vp, [vp, ctypes.c_char_p]),
             "ref_mesh_entity_name": (ctypes.c_char_p, [vp, ctypes.c_int]),
@@ -304,3 +305,12 @@ class RefSimulation:
         res = np.zeros(5)
         step0 = lib().ref_advance(self.ptr, ctypes.byref(t), _d(res), max_step)
         return t.value, step0, res
+
+
+def kdtree_nearest(points, queries):
+    """The reference's kd-tree nearest-point search (src/core/kdtree.c) for every query point."""
+    p = np.ascontiguousarray(points, dtype=np.float64)
+    q = np.ascontiguousarray(queries, dtype=np.float64)
+    out = np.zeros(len(q), dtype=np.int32)
+    lib().ref_kdtree_nearest(_d(p), len(p), _d(q), len(q), out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+    return out

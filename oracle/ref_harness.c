@@ -14,6 +14,7 @@
 #include "navierstokes.h"
 #include "simulation.h"
 #include "teal.h"
+#include "kdtree.h"
 
 int ref_init(void)
 {
@@ -455,4 +456,17 @@ double ref_advance(void *sim_, double *time, double *residual, double max_step)
 void ref_simulation_destroy(void *sim)
 {
     simulation_destroy(sim);
+}
+
+/* Nearest point of `point` [num][3] for each of `query` [num_query][3], with the reference's own kd-tree
+ * (src/core/kdtree.c, the search teal's restart interpolation uses, src/equations/read.c:101-144). */
+void ref_kdtree_nearest(const double *point, int num, const double *query, int num_query, int *index)
+{
+    Kdtree *tree = kdtree_init((const Vector *)point, num);
+    for (int i = 0; i < num_query; i++) {
+        Vector q = {query[3 * i], query[3 * i + 1], query[3 * i + 2]};
+        index[i] = -1;
+        kdtree_nearest(tree, q, &index[i], 1);
+    }
+    kdtree_deinit(tree);
 }

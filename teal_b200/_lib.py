@@ -137,6 +137,7 @@ SIGNATURES = [
     ("tg_batch_get_primitive", ctypes.c_int, [_vp, ctypes.c_int, _vp]),
     ("tg_batch_run", ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_double, _vp, _vp, _vp, _vp, _vp, _vp,
                                     _vp]),
+    ("tg_batch_status", ctypes.c_int, [_vp, _vp]),
     ("tg_bind", ctypes.c_int, [_vp, _vp, _vp]),
     ("tg_unbind", ctypes.c_int, [_vp]),
     ("tg_teal_euler", ctypes.c_double, [_vp, _dbl_p, _vp, ctypes.c_double, ctypes.c_double, _vp]),

@@ -106,8 +106,10 @@ __global__ void __launch_bounds__(INST_BLOCK) k_inst_begin(Segments seg, const d
         double clip = st.use_max_time ? (st.max_time[i] - st.time[i]) : st.max_step[i];
         st.step0[i] = step0;
         st.step[i] = fmin(step0, clip);
-        if (!isfinite(step0) || !(step0 > 0)) {
+        if (!isfinite(step0) || !(step0 > 0)) {  // the instance stops; the others go on
             atomicOr(st.error, ERR_NONFINITE);
+            st.fail[i] = 1;
+            st.active[i] = 0;
         }
     }
 }
@@ -139,16 +141,22 @@ __global__ void __launch_bounds__(INST_BLOCK) k_inst_end(Segments seg, const dou
         return;
     }
     double mx = 0;
+    bool finite = true;
     for (int k = 0; k < 5; k++) {
         res[k] = sqrt(res[k] / seg.sum_volume[i]);
         st.residual[5 * i + k] = res[k];
         mx = (res[k] > mx) ? res[k] : mx;
-        if (!isfinite(res[k])) {
-            atomicOr(st.error, ERR_NONFINITE);
-        }
+        finite = finite && isfinite(res[k]);
+    }
+    if (!finite) {
+        atomicOr(st.error, ERR_NONFINITE);
     }
     if (!advance) {
         return;
+    }
+    if (!finite) {  // the instance stops with its step counted; the others go on
+        st.fail[i] = 1;
+        st.active[i] = 0;
     }
     double t = st.time[i] + st.step[i];
     st.time[i] = t;

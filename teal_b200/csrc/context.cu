@@ -172,13 +172,14 @@ struct Gmres {
     int *flag = nullptr;      // per-instance progress (GmresFlag)
     int *count = nullptr;     // [2] instances still iterating (Newton, Arnoldi)
     int *ctl = nullptr;       // [GC_COUNT] loop counters of the graph-driven loops
+    double *Rm = nullptr;     // [5][C] FP32-flux form: the matvec's base residual, in FP32 fluxes
 };
 
 // Host mirror of the per-instance step arrays (pinned; one copy per direction moves all of them):
 // doubles: time, step, step0, max_step, max_time, threshold, residual[5]; ints: variable, iter,
 // max_iter, active, then num_active and error.
 enum { SD_TIME, SD_STEP, SD_STEP0, SD_MAX_STEP, SD_MAX_TIME, SD_THRESHOLD, SD_RESIDUAL, SD_COUNT = SD_RESIDUAL + 5 };
-enum { SI_VARIABLE, SI_ITER, SI_MAX_ITER, SI_ACTIVE, SI_COUNT };
+enum { SI_VARIABLE, SI_ITER, SI_MAX_ITER, SI_ACTIVE, SI_FAIL, SI_COUNT };
 
 struct tg_ctx {
     int device = 0;
@@ -274,6 +275,8 @@ struct tg_ctx {
 
     // polls of the staged face kernel's first bounded wait (lowered only by tg_set_wait_limit)
     int wait_polls = MBAR_POLLS;
+    // created by tg_batch_create: an instance that goes non-finite stops alone (tg_batch_status)
+    bool batch = false;
 
     // implicit step graph (device-driven Newton / Arnoldi / Gram-Schmidt loops) and its key
     cudaGraphExec_t igraph = nullptr;
@@ -340,7 +343,7 @@ static void free_ctx(tg_ctx *c)
         if (p) cudaFree(p);
     }
     void *gp[] = {c->gm.U, c->gm.Ustart, c->gm.r, c->gm.delta, c->gm.V, c->gm.w, c->gm.q1, c->gm.R1,
-                  c->gm.part, c->gm.sc, c->gm.flag, c->gm.count, c->gm.ctl};
+                  c->gm.part, c->gm.sc, c->gm.flag, c->gm.count, c->gm.ctl, c->gm.Rm};
     for (void *p : gp) {
         if (p) cudaFree(p);
     }
@@ -898,7 +901,9 @@ static int create_ctx(MeshInput &in, const tg_equations *e, int precision, tg_ct
                                  c->gb.slot_off32};
 
         // state
-        size_t rsz = precision == TG_PRECISION_FP32_FLUX ? sizeof(float) : sizeof(double);
+        // FP64 record size in every form: the FP32-flux form's implicit step evaluates its Newton
+        // residuals with the FP64 kernels (enqueue_implicit_step)
+        size_t rsz = sizeof(double);
         TRY(dalloc(&c->q, 5 * (size_t)s.N));
         CU(cudaMemsetAsync(c->q, 0, 5 * sizeof(double) * s.N, st));
         TRY(dalloc(&c->U0, 5 * (size_t)s.C));
@@ -941,7 +946,7 @@ static int create_ctx(MeshInput &in, const tg_equations *e, int precision, tg_ct
         c->st = Steps{c->sd + SD_TIME * n,     c->sd + SD_STEP * n,      c->sd + SD_STEP0 * n,
                       c->sd + SD_MAX_STEP * n, c->sd + SD_MAX_TIME * n,  c->sd + SD_THRESHOLD * n,
                       c->sd + SD_RESIDUAL * n, c->si + SI_VARIABLE * n,  c->si + SI_ITER * n,
-                      c->si + SI_MAX_ITER * n, c->si + SI_ACTIVE * n,    c->si + SI_COUNT * n,
+                      c->si + SI_MAX_ITER * n, c->si + SI_ACTIVE * n,    c->si + SI_FAIL * n, c->si + SI_COUNT * n,
                       c->si + SI_COUNT * n + 1, 0};
         // the residual block is [ninst][5] inside the doubles: SD_RESIDUAL * n .. + 5 n
         c->aos_len = (size_t)15 * ((size_t)m->num_cells > (size_t)s.F ? (size_t)m->num_cells : (size_t)s.F);
@@ -1088,7 +1093,16 @@ extern "C" int tg_batch_create(const tg_mesh *meshes, const tg_equations *eqns, 
     *out = nullptr;
     MeshInput in;
     TRY(merged_input(meshes, eqns, num, in));
-    return create_ctx(in, &eqns[0], precision, out);
+    TRY(create_ctx(in, &eqns[0], precision, out));
+    (*out)->batch = true;
+    return TG_OK;
+}
+
+extern "C" int tg_batch_status(tg_ctx *c, int *status)
+{
+    if (!c || !status) return fail(TG_ERR_INVALID, "null argument");
+    for (int i = 0; i < c->ninst; i++) status[i] = hi_at(c, SI_FAIL, i) ? TG_ERR_NONFINITE : TG_OK;
+    return TG_OK;
 }
 
 extern "C" int tg_batch_size(tg_ctx *c, int *num)
@@ -1194,6 +1208,7 @@ extern "C" int tg_batch_set_primitive(tg_ctx *c, int inst, const double *prim)
 {
     if (!c || !prim) return fail(TG_ERR_INVALID, "null argument");
     TRY(set_rows(c, inst, prim, c->q));
+    hi_at(c, SI_FAIL, inst) = 0;  // a new state: the instance may run again
     c->prepared = false;
     return TG_OK;
 }
@@ -1547,6 +1562,9 @@ static int check_error(tg_ctx *c)
         if (e & ERR_LOOP_LIMIT)
             return fail(TG_ERR_TIMEOUT, "an implicit step reached the device limit of %d Newton iterations",
                         NEWTON_LOOP_LIMIT);
+        // an instance of a batch whose state went non-finite has stopped on its own (tg_batch_status);
+        // the other instances go on
+        if (c->batch) return TG_OK;
         return fail(TG_ERR_NONFINITE, "non-finite time step or residual");
     }
     return TG_OK;
@@ -1885,7 +1903,7 @@ extern "C" int tg_batch_run(tg_ctx *c, int method, const void *context, double c
         hi_at(c, SI_VARIABLE, i) = var;
         hi_at(c, SI_ITER, i) = 0;
         hi_at(c, SI_MAX_ITER, i) = max_iter[i];
-        hi_at(c, SI_ACTIVE, i) = max_iter[i] > 0;
+        hi_at(c, SI_ACTIVE, i) = max_iter[i] > 0 && !hi_at(c, SI_FAIL, i);  // failed instances stay stopped
         most = max_iter[i] > most ? max_iter[i] : most;
         early = early || hd_at(c, SD_THRESHOLD, i) > 0 || hd_at(c, SD_MAX_TIME, i) < DBL_MAX;
     }
@@ -1916,7 +1934,7 @@ static int gm_alloc(tg_ctx *c, int dim)
 {
     Gmres &g = c->gm;
     if (g.V && g.dim >= dim) return TG_OK;
-    void *old[] = {g.U, g.Ustart, g.r, g.delta, g.V, g.w, g.q1, g.R1, g.part, g.sc, g.flag, g.count, g.ctl};
+    void *old[] = {g.U, g.Ustart, g.r, g.delta, g.V, g.w, g.q1, g.R1, g.part, g.sc, g.flag, g.count, g.ctl, g.Rm};
     for (void *p : old) {
         if (p) cudaFree(p);
     }
@@ -1938,6 +1956,7 @@ static int gm_alloc(tg_ctx *c, int dim)
     TRY(dalloc(&g.count, 2));
     TRY(dalloc(&g.ctl, GC_COUNT));
     CU(cudaMemset(g.ctl, 0, sizeof(int) * GC_COUNT));
+    if (c->precision == TG_PRECISION_FP32_FLUX) TRY(dalloc(&g.Rm, n));
     g.dim = dim;
     drop_graph(c);  // a captured implicit step refers to the old workspace
     return TG_OK;
@@ -2018,14 +2037,25 @@ static int while_end(tg_ctx *c, WhileLoop &w)
     return TG_OK;
 }
 
-// derivative of a primitive state q (boundary rows refreshed) into Rout
-static int gm_derivative(tg_ctx *c, double *q, double *Rout)
+// derivative of a primitive state q (boundary rows refreshed) into Rout, with the kernels of
+// `precision` (the context's own, or FP64 for the FP32-flux form's Newton residuals)
+static int gm_derivative(tg_ctx *c, double *q, double *Rout, int precision)
 {
     // implicit Euler evaluates every residual at the end of the step, time + step (advance.c:144)
     c->t_time = c->st.time, c->t_step = c->st.step, c->t_coef = 1.0;
-    TRY(run_fluxes(c, q));
-    TRY(launch_cell<0>(c, 0.0, 0, q, Rout));
-    return TG_OK;
+    const int own = c->precision;
+    c->precision = precision;
+    int rc = run_fluxes(c, q);
+    if (rc == TG_OK) rc = launch_cell<0>(c, 0.0, 0, q, Rout);
+    c->precision = own;
+    return rc;
+}
+
+// the Newton residual's precision: FP64 in the FP32-flux form, whose FP32 fluxes serve the matvec
+// only ("FP64 Arnoldi, FP32 matvec flux": the Newton iteration then converges to the FP64 state)
+static int newton_precision(const tg_ctx *c)
+{
+    return c->precision == TG_PRECISION_FP32_FLUX ? TG_PRECISION_FP64 : c->precision;
 }
 
 // one GMRES cycle for the increment of every Newton instance (gmres.c:52-149): the Arnoldi
@@ -2051,8 +2081,9 @@ static int gm_solve(tg_ctx *c, const GmresBatch &gb, double krylov_tol)
         k_perturb_at<<<cb, BLOCK, 0, c->stream>>>(C, c->s.N, g.U, g.V, gb, c->prop[0], g.q1);
         CU(cudaGetLastError());
         c->launches += 3;
-        TRY(gm_derivative(c, g.q1, g.R1));
-        k_matvec_finish_at<<<cb, BLOCK, 0, c->stream>>>(C, g.V, g.R1, c->R, gb, g.w);
+        TRY(gm_derivative(c, g.q1, g.R1, c->precision));
+        // the matvec differences two residuals of the same precision (gmres.c:41-46)
+        k_matvec_finish_at<<<cb, BLOCK, 0, c->stream>>>(C, g.V, g.R1, g.Rm ? g.Rm : c->R, gb, g.w);
         CU(cudaGetLastError());
         c->launches += 1;
         // modified Gram-Schmidt rows 0..k
@@ -2126,7 +2157,8 @@ static int enqueue_implicit_step(tg_ctx *c, double courant, double newton_tol, d
     CU(cudaMemcpyAsync(g.Ustart, c->U0, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     c->prepared = false;
 
-    TRY(gm_derivative(c, c->q, c->R));
+    TRY(gm_derivative(c, c->q, c->R, newton_precision(c)));
+    if (g.Rm) TRY(gm_derivative(c, c->q, g.Rm, c->precision));
     k_newton_init<<<cb, BLOCK, 0, c->stream>>>(C, c->R, gb, g.r);
     CU(cudaGetLastError());
     TRY(gm_dot(c, gb, g.r, g.r, GF_NEWTON, GS_NORM, 1));
@@ -2136,7 +2168,7 @@ static int enqueue_implicit_step(tg_ctx *c, double courant, double newton_tol, d
     c->launches += 4;
     auto newton_check = [&](cudaGraphConditionalHandle h, int enter) {
         cudaMemsetAsync(g.count, 0, sizeof(int), c->stream);
-        k_newton_check<<<ib, 128, 0, c->stream>>>(gb, c->seg, c->st.error);
+        k_newton_check<<<ib, 128, 0, c->stream>>>(gb, c->seg, c->st);
         k_newton_next<<<1, 1, 0, c->stream>>>(gb, h, enter, c->st.error);
         c->launches += 2;
     };
@@ -2146,7 +2178,8 @@ static int enqueue_implicit_step(tg_ctx *c, double courant, double newton_tol, d
         TRY(gm_solve(c, gb, krylov_tol));
         k_newton_update<<<cb, BLOCK, 0, c->stream>>>(C, c->s.N, g.U, g.delta, gb, c->prop[0], c->q);
         CU(cudaGetLastError());
-        TRY(gm_derivative(c, c->q, c->R));
+        TRY(gm_derivative(c, c->q, c->R, newton_precision(c)));
+        if (g.Rm) TRY(gm_derivative(c, c->q, g.Rm, c->precision));
         k_newton_residual<<<cb, BLOCK, 0, c->stream>>>(C, g.U, g.Ustart, c->R, gb, g.r);
         CU(cudaGetLastError());
         TRY(gm_dot(c, gb, g.r, g.r, GF_NEWTON, GS_NORM, 1));
@@ -2226,8 +2259,12 @@ static int implicit_step_all(tg_ctx *c, const void *context, double courant)
 static int implicit_run(tg_ctx *c, const void *context, double courant, int most)
 {
     TRY(write_steps(c));
-    for (int it = 0; it < most; it++) {
-        TRY(implicit_step_all(c, context, courant));
+    // stopped instances sit out the following steps on the device, so the host looks in only every
+    // 8 steps (and at the end)
+    for (int it = 0; it < most;) {
+        const int n = most - it < 8 ? most - it : 8;
+        for (int k = 0; k < n; k++) TRY(implicit_step_all(c, context, courant));
+        it += n;
         TRY(read_steps(c));
         TRY(check_error(c));
         if (hi_num_active(c) == 0) break;

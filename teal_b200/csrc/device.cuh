@@ -75,6 +75,7 @@ struct Steps {
     int *iter;
     int *max_iter;
     int *active;       // updates and clocks of an inactive instance stand still
+    int *fail;         // nonzero once the instance's time step or residual was non-finite (it stops)
     int *num_active;   // active instances after the last step
     int *error;        // nonzero once a non-finite step or norm was seen
     int use_max_time;  // clip by max_time - time instead of max_step

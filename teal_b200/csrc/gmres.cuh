@@ -175,17 +175,18 @@ __global__ void k_fd_scale(GmresBatch gb, double fd_rel, double newton_tol, int 
 }
 
 // Newton loop test per instance (advance.c:162-165): keep iterating while |r| > tol * |r0| and
-// within 128 (cells + 1) iterations; a non-finite norm sets the error word. count[0] = instances
+// within 128 (cells + 1) iterations; a non-finite norm marks the instance failed. count[0] = instances
 // that go on.
-__global__ void k_newton_check(GmresBatch gb, Segments seg, int *err)
+__global__ void k_newton_check(GmresBatch gb, Segments seg, Steps st)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= gb.ninst || !gb.newton(i)) {
         return;
     }
     const double norm = gb.s(i)[GS_NORM];
-    if (!isfinite(norm)) {
-        atomicOr(err, ERR_NONFINITE);
+    if (!isfinite(norm)) {  // the instance stops (its residual follows as non-finite); the others go on
+        atomicOr(st.error, ERR_NONFINITE);
+        st.fail[i] = 1;
         gb.newton(i) = 0;
         return;
     }

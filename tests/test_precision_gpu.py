@@ -89,3 +89,28 @@ def test_fp32_taylor_green_histories():
     # residual itself stays ~2e-3 off: its p0-sized cancelling parts are compared in FP64 there.
     assert err < 1e-6
     assert max(ke_err) < 1e-7 and max(en_err) < 1e-7
+
+
+def test_fp32_matvec_implicit_step_converges_to_the_fp64_step():
+    """The FP32-flux form's implicit Euler step evaluates its Newton residuals with the FP64 kernels
+    and only the finite-difference matvec with FP32 fluxes ("FP64 Arnoldi, FP32 matvec flux"): with
+    a tight Newton tolerance both forms solve U - U0 - dt R64(U) = 0, so their states agree to the
+    Newton tolerance, not to FP32 rounding."""
+    from tests.test_batch_gpu import farfield_problem
+
+    e = farfield_problem(12, 10, 0.8, 5)
+    prim = e.primitive.copy()
+    C = e.mesh.num_inner_cells
+    out = {}
+    for name, prec in (("fp64", tb.TG_PRECISION_FP64), ("fp32", FP32)):
+        ctx = tb.Context(e.mesh, e, precision=prec)
+        try:
+            ctx.set_primitive(prim)
+            t, s0, res = ctx.advance(tb.TG_ADVANCE_IMPLICIT_EULER, 20.0, 0.0, context=(1e-10, 0.3, 30))
+            out[name] = (t, ctx.get_primitive()[:C].copy())
+        finally:
+            ctx.close()
+    assert out["fp32"][0] == out["fp64"][0]  # the CFL step comes from the same FP64 state
+    err = rel_l2(out["fp32"][1], out["fp64"][1])
+    report("implicit step, FP32 matvec vs FP64, Newton tol 1e-10", err)
+    assert err[[0, 1, 2, 4]].max() <= 1e-9, err
