@@ -458,15 +458,21 @@ def run_batch_implicit(args, specs):
         torch.cuda.synchronize()
         secs = ev0.elapsed_time(ev1) / 1000.0
         steps = it.astype(np.float64)
-        drop = res.max(axis=1) / np.maximum(first, 1e-300)
+        failed = b.status() != 0  # instances that went non-finite stopped alone
+        drop = np.where(failed, np.inf, res.max(axis=1) / np.maximum(first, 1e-300))
         out[name] = {"value": float((cells * steps).sum() / secs), "seconds": secs,
-                     "converged": int((drop <= args.drop).sum()), "instances": n,
-                     "steps_taken_max": int(steps.max()), "drop_p50": float(np.percentile(drop, 50)),
-                     "drop_max": float(drop.max()), "drop_min": float(drop.min())}
-        states[name] = [b.get_primitive(i)[: e.mesh.num_inner_cells].copy() for i, e in enumerate(problems)]
+                     "converged": int((drop <= args.drop).sum()), "instances": n, "failed": int(failed.sum()),
+                     "steps_taken_max": int(steps.max()),
+                     "drop_p50": float(np.percentile(drop[~failed], 50)) if (~failed).any() else None,
+                     "drop_max": float(drop[~failed].max()) if (~failed).any() else None,
+                     "drop_min": float(drop[~failed].min()) if (~failed).any() else None}
+        states[name] = [None if failed[i] else b.get_primitive(i)[: e.mesh.num_inner_cells].copy()
+                        for i, e in enumerate(problems)]
         b.close()
     err_var = np.zeros(5)
     for a, f in zip(states["fp64"], states["fp32_matvec"]):
+        if a is None or f is None:
+            continue
         d = np.sqrt(((f - a) ** 2).sum(axis=0)) / np.maximum(np.sqrt((a ** 2).sum(axis=0)), 1e-300)
         err_var = np.maximum(err_var, d)
     steps_max = max(1, out["fp32_matvec"]["steps_taken_max"])

@@ -1971,7 +1971,7 @@ static GmresBatch gm_batch(tg_ctx *c, int dim)
 static int gm_dot(tg_ctx *c, const GmresBatch &gb, const double *x, const double *y, int which, int slot,
                   int take_sqrt)
 {
-    k_piece_dot<<<c->npieces, BLOCK, 0, c->stream>>>(c->seg, c->s.C, x, y, c->gm.part);
+    k_piece_dot<<<c->npieces, BLOCK, 0, c->stream>>>(c->seg, c->s.C, x, y, gb, which, c->gm.part);
     k_inst_dot<<<c->ninst, GM_INST_BLOCK, 0, c->stream>>>(c->seg, c->gm.part, gb, which, slot, take_sqrt);
     CU(cudaGetLastError());
     return TG_OK;

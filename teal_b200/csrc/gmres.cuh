@@ -63,12 +63,17 @@ __host__ __device__ inline int gmres_scn(int dim)
     return GS_HEAD + (dim + 1) * dim + 4 * dim + 2;
 }
 
-// per-piece partial sums of x . y over the 5 variables of the piece's cells
+// per-piece partial sums of x . y over the 5 variables of the piece's cells; pieces of instances
+// whose flag `which` is off are skipped (their sums are not read)
 __global__ void __launch_bounds__(BLOCK) k_piece_dot(Segments seg, int C, const double *__restrict__ x,
-                                                     const double *__restrict__ y, double *__restrict__ part)
+                                                     const double *__restrict__ y, GmresBatch gb, int which,
+                                                     double *__restrict__ part)
 {
     __shared__ double sh[BLOCK / 32];
     const int beg = seg.piece_beg[blockIdx.x], end = seg.piece_beg[blockIdx.x + 1];
+    if (!gb.flag[which * gb.ninst + gb.cell_inst[beg]]) {
+        return;
+    }
     double t = 0;
     for (int c = beg + threadIdx.x; c < end; c += BLOCK) {
 #pragma unroll
@@ -372,6 +377,9 @@ __global__ void __launch_bounds__(BLOCK) k_piece_vnorm(Segments seg, int C, cons
     __shared__ double sh[BLOCK / 32];
     const double *x = V + (size_t)gb.ctl[GC_K] * 5 * (size_t)C;
     const int beg = seg.piece_beg[blockIdx.x], end = seg.piece_beg[blockIdx.x + 1];
+    if (!gb.arnoldi(gb.cell_inst[beg])) {  // the instance left its Arnoldi loop
+        return;
+    }
     double t = 0;
     for (int c = beg + threadIdx.x; c < end; c += BLOCK) {
 #pragma unroll
@@ -398,7 +406,10 @@ __global__ void __launch_bounds__(BLOCK) k_mgs_piece(Segments seg, int C, const 
     const int i = last ? k + 1 : gb.ctl[GC_I];
     const int beg = seg.piece_beg[blockIdx.x], end = seg.piece_beg[blockIdx.x + 1];
     const int inst = gb.cell_inst[beg];  // a piece lies in one instance
-    const bool update = i > 0 && gb.arnoldi(inst);
+    if (!gb.arnoldi(inst)) {  // the instance left its Arnoldi loop: nothing to update or sum
+        return;
+    }
+    const bool update = i > 0;
     const double h = update ? *gb.H(inst, i - 1, k) : 0.0;
     const double *Vp = V + (size_t)(i > 0 ? i - 1 : 0) * n;
     const double *x = last ? w : V + (size_t)i * n;

@@ -122,6 +122,45 @@ def test_batch_rejects_mixed_lanes():
         tb.Batch([a, c])
 
 
+@pytest.mark.parametrize("method", ["lserk", "implicit"])
+def test_an_instance_that_goes_non_finite_stops_alone(method):
+    """An instance whose state holds a non-finite value stops on its own; the others run to their
+    limits with the same bits as alone, the batch call succeeds, and tg_batch_status names the failed
+    one. A new state lets it run again."""
+    ps = [channel_problem(12, 7, 0.5, 1), channel_problem(9, 9, 2.0, 2), channel_problem(10, 8, 0.8, 3)]
+    bad = ps[1].primitive.copy()
+    bad[5, 0] = np.nan
+    b = tb.Batch(ps)
+    b.set_primitive(1, bad)
+    if method == "lserk":
+        m, cfl, steps, ctx = tb.TG_ADVANCE_LSERK, 0.5, 6, (3, 3)
+    else:
+        m, cfl, steps, ctx = tb.TG_ADVANCE_IMPLICIT_EULER, 20.0, 3, NK
+    t, it, res = b.run(m, cfl, steps, context=ctx)
+    assert b.status().tolist() == [0, 4, 0]  # TG_OK, TG_ERR_NONFINITE, TG_OK
+    for i in (0, 2):
+        e = ps[i]
+        one = tb.Context(e.mesh, e)
+        one.set_primitive(e.primitive)
+        t1, it1, res1 = one.run(m, cfl, steps, context=ctx)
+        assert it[i] == it1 == steps
+        assert t[i] == t1
+        assert np.array_equal(b.get_primitive(i), one.get_primitive())
+        one.close()
+    assert it[1] < steps
+    b.set_primitive(1, ps[1].primitive)
+    t, it, res = b.run(m, cfl, 1, context=ctx)
+    assert b.status().tolist() == [0, 0, 0]
+    assert np.all(np.isfinite(res))
+    # a single-mesh context reports the same condition as an error
+    one = tb.Context(ps[1].mesh, ps[1])
+    one.set_primitive(bad)
+    with pytest.raises(tb.TealError) as err:
+        one.run(m, cfl, 2, context=ctx)
+    assert err.value.code == 4
+    one.close()
+
+
 # ---- batched implicit Euler (Jacobian-free Newton-GMRES per instance) ---------------------------
 
 IMPLICIT_SPECS = [(10, 8, 0.5, 1), (14, 6, 1.5, 2), (7, 9, 0.8, 3)]  # nx, ny, Mach, seed
