@@ -1,15 +1,21 @@
 """Continuous-batching solve server for the teal residual / time-integration path.
 
-Requests (mesh, Mach number, equations, flux scheme, step count or residual tolerance) arrive at any
-time. The server admits a waiting request as soon as its device-memory estimate fits the HBM budget
-and a slot is free, keeps its state resident on the GPU in its own context and CUDA stream, and
-advances all admitted requests concurrently (one host thread per request; the device overlaps their
-kernels). A finished request releases its memory and slot, which admits the next one. Each result
-is the same bits as the request solved alone: contexts share nothing and every kernel is
-deterministic.
+Requests (mesh, Mach number, equations, flux scheme, integrator, step budget or residual tolerance)
+arrive at any time. The server admits a waiting request as soon as its device-memory estimate fits
+the HBM budget, keeps its state resident on the GPU and batches it continuously with the requests
+already running (`Server`): requests that share a scheme (equations, flux, limiter, precision,
+integrator, CFL number) form a lane, and each lane advances all of its requests in one arena (one
+launch per kernel for all of them, the step replayed from a CUDA graph), in rounds of a few steps.
+Between rounds, requests that finished leave and newly admitted ones join: the lane re-packs its
+arena, carrying every running request's state (exact FP64 rows) and clock over. Lanes run on their
+own host threads and CUDA streams, so different schemes overlap on the device. Every result is the
+same bits as the request solved alone: an instance's step depends on its own state only, and every
+kernel is deterministic.
 
-The scheduler (`Scheduler`) is independent of the GPU: it takes an `execute(request)` callable, so
-its admission and failure handling are testable on the host with a fake executor.
+`StreamServer` is the simpler design kept for comparison: one context, CUDA stream and host thread
+per request, overlapping on the device but sharing no launches. Its admission (`Scheduler`) is
+independent of the GPU: it takes an `execute(request)` callable, so admission and failure handling
+are testable on the host with a fake executor.
 """
 
 import dataclasses
@@ -25,11 +31,12 @@ from . import _lib
 
 @dataclasses.dataclass
 class Request:
-    """One solve request. `steps` bounds the explicit RK steps; `tolerance` (> 0) stops earlier once
-    the maximum residual has dropped by that factor from the first step's."""
+    """One solve request. `steps` bounds its steps (explicit RK, or implicit Euler for a steady
+    solve); `tolerance` (> 0) stops it earlier once the maximum residual has dropped by that factor
+    from the first step's."""
 
     id: int
-    cells: tuple                     # (nx, ny, nz) of the channel box
+    cells: tuple                     # (nx, ny, nz) of the channel box; (n, n, n) grid of a ramp
     mach: float = 0.5
     angle: float = 0.0               # flow angle in degrees
     physics: int = _lib.TG_EULER
@@ -41,6 +48,9 @@ class Request:
     courant: float = 0.5
     arrival: float = 0.0             # seconds after the server's start
     precision: int = _lib.TG_PRECISION_FP64
+    method: str = "lserk"            # teal's advance name: "lserk" or "implicit euler" (steady solves)
+    mesh: str = "channel"            # "channel" box, or "ramp": the mixed-element ramp of the batch workload
+    seed: int = 0                    # mesh seed of a ramp
     # filled by the server
     admitted: float = math.nan
     finished: float = math.nan
@@ -52,6 +62,8 @@ class Request:
 
     @property
     def num_cells(self):
+        if self.mesh == "ramp":
+            return int(round(4.64 * self.cells[0] ** 3))  # a ramp grid holds ~4.64 cells per hexahedron
         return int(np.prod(self.cells))
 
     @property
@@ -60,11 +72,17 @@ class Request:
 
 
 def memory_estimate(req):
-    """Device bytes a request holds while resident (FP64 layout; peak of the upload included)."""
-    nx, ny, nz = req.cells
-    cells = nx * ny * nz
-    faces = 3 * cells + nx * ny + ny * nz + nz * nx
+    """Device bytes a request holds while resident (FP64 layout; peak of the upload included; the
+    Krylov workspace of implicit steps)."""
+    cells = req.num_cells
+    if req.mesh == "ramp":
+        faces = int(2.2 * cells)
+    else:
+        nx, ny, nz = req.cells
+        faces = 3 * cells + nx * ny + ny * nz + nz * nx
     per_cell = 700 + (80 if req.physics == _lib.TG_NAVIERSTOKES else 0)
+    if req.method == "implicit euler":
+        per_cell += 40 * (31 + 8)  # Krylov basis (dimension 30) and the Newton vectors
     return int(per_cell * cells + 450 * faces + (8 << 20))
 
 
@@ -185,18 +203,31 @@ class Scheduler:
         return sorted(self.done, key=lambda r: r.id)
 
 
-def solve(req, stream=None, chunk=25):
-    """Solve one request on the current GPU (its own context; used alone or by the server)."""
+def build_problem(req):
+    """Host mesh and equations of a request (teal_b200 Equations with its initial state)."""
     from .api import Equations, Mesh
 
-    nx, ny, nz = req.cells
-    mesh = Mesh.create((0, 0, 0), (nx / ny, 1.0, nz / ny), (nx, ny, nz), (0, 0, 1))
+    if req.mesh == "ramp":
+        from . import meshes
+
+        n = int(req.cells[0])
+        mesh = Mesh.from_cells(meshes.ramp_mesh(n=(n, n, n), seed=req.seed))
+    else:
+        nx, ny, nz = req.cells
+        mesh = Mesh.create((0, 0, 0), (nx / ny, 1.0, nz / ny), (nx, ny, nz), (0, 0, 1))
     eqns = Equations.navierstokes(mesh) if req.physics == _lib.TG_NAVIERSTOKES else Equations.euler(mesh)
     eqns.set_convective_flux(req.flux)
     eqns.set_limiter(req.limiter, 1.0)
     if req.physics == _lib.TG_NAVIERSTOKES:
         eqns.set_property("dynamic viscosity", req.viscosity)
     free = free_stream(req.mach, req.angle)
+    if req.mesh == "ramp":  # the batch workload's boundaries: far field around, slip walls
+        for side in ("left", "right", "top"):
+            eqns.set_boundary_condition(side, "farfield", free)
+        for side in ("bottom", "back", "front"):
+            eqns.set_boundary_condition(side, "slipwall")
+        eqns.primitive[:] = np.tile(free, (mesh.num_cells, 1))
+        return eqns
     for side in ("left", "right", "top"):
         eqns.set_boundary_condition(side, "farfield", free)
     eqns.set_boundary_condition("bottom", "slipwall")
@@ -206,18 +237,44 @@ def solve(req, stream=None, chunk=25):
     r2 = ((c[:, 0] - 0.5 * nx / ny) ** 2 + (c[:, 1] - 0.5) ** 2) / 0.02
     prim[:, 0] *= 1 + 0.2 * np.exp(-r2)
     eqns.set_initial_condition("domain", initial=None, compute=lambda x: prim[: x.shape[0]])
+    return eqns
+
+
+def method_of(req):
+    """(TG_ADVANCE_*, context) of a request's integrator: lserk{3,3}, or implicit Euler with teal's
+    Newton-Krylov settings of its steady airfoil run (run/airfoil/run.c: {0.1, 0.3, 30})."""
+    if req.method == "implicit euler":
+        return _lib.TG_ADVANCE_IMPLICIT_EULER, (0.1, 0.3, 30)
+    if req.method != "lserk":
+        raise ValueError(f"invalid advance method ({req.method})")
+    return _lib.TG_ADVANCE_LSERK, (3, 3)
+
+
+def lane_key(req):
+    """Requests with equal keys can share one arena (the arena shares equations, schemes, properties,
+    precision, integrator and CFL number)."""
+    ns = req.physics == _lib.TG_NAVIERSTOKES
+    return (req.physics, req.flux, req.limiter, req.precision, req.method, req.courant,
+            req.viscosity if ns else None)
+
+
+def solve(req, stream=None, chunk=25):
+    """Solve one request alone on the current GPU (its own context): one step, whose residual sets the
+    tolerance's threshold, then the remaining steps with the residual test on the device."""
+    eqns = build_problem(req)
+    mesh = eqns.mesh
     ctx = eqns.context(req.precision)
     if stream is not None:
         ctx.set_stream(stream)
-    method = _lib.TG_ADVANCE_LSERK
-    t, it, res = ctx.run(method, req.courant, 1, context=(3, 3))
+    method, mctx = method_of(req)
+    t, it, res = ctx.run(method, req.courant, 1, context=mctx)
     total = it
     threshold = req.tolerance * float(np.max(res)) if req.tolerance > 0 else 0.0
     # the remaining steps in chunks (the same steps, replayed from the same graph), so a cancelled
     # request stops at the next chunk boundary
     while total < req.steps and not req.cancelled:
         n = min(chunk, req.steps - total)
-        t, it, res = ctx.run(method, req.courant, n, threshold=threshold, context=(3, 3), time=t)
+        t, it, res = ctx.run(method, req.courant, n, threshold=threshold, context=mctx, time=t)
         total += it
         if it < n:  # the residual fell below the threshold
             break
@@ -228,8 +285,279 @@ def solve(req, stream=None, chunk=25):
     return req
 
 
+class _Entry:
+    """A running request inside a lane."""
+
+    def __init__(self, req, eqns):
+        self.req = req
+        self.eqns = eqns
+        self.time = 0.0
+        self.iterations = 0
+        self.threshold = None  # set from the first step's residual
+        self.residual = None
+
+
+class Lane:
+    """Requests of one scheme advancing together in one resident arena (continuous batching).
+
+    `round()` advances every running request by up to `chunk` steps in one batched run (a request's
+    first step alone, as `solve` takes it, since its residual sets the request's threshold), then
+    removes the requests that finished (step budget, tolerance, a non-finite state, cancellation).
+    When the set of requests changed, the arena is re-packed before the run: the running requests'
+    states (all rows, exact FP64) are read out, the old arena is released, and a new arena is built
+    for the current set with those states, so a request's steps are the ones it takes alone."""
+
+    def __init__(self, key, chunk, stream=None):
+        self.key = key
+        self.chunk = int(chunk)
+        self.stream = stream
+        self.entries = []
+        self.arena = None
+        self.arena_entries = []
+        self.repacks = 0
+
+    def join(self, req, eqns):
+        self.entries.append(_Entry(req, eqns))
+
+    def _repack(self):
+        from .api import Batch
+
+        if self.arena is not None:
+            keep = {id(e) for e in self.entries}
+            for i, e in enumerate(self.arena_entries):
+                if id(e) in keep:
+                    e.eqns.primitive[:] = self.arena.get_primitive(i)
+            self.arena.close()
+            self.arena = None
+        self.arena = Batch([e.eqns for e in self.entries], precision=self.entries[0].req.precision)
+        if self.stream is not None:
+            self.arena.set_stream(self.stream)
+        self.arena_entries = list(self.entries)
+        self.repacks += 1
+
+    def round(self):
+        """One round; returns the requests that finished in it."""
+        finished = [e for e in self.entries if e.req.cancelled]
+        self.entries = [e for e in self.entries if not e.req.cancelled]
+        for e in finished:
+            e.req.error = "cancelled"
+            e.req.iterations = e.iterations
+        if not self.entries:
+            self.close()
+            return [e.req for e in finished]
+        if self.arena_entries != self.entries:
+            self._repack()
+        req0 = self.entries[0].req
+        method, mctx = method_of(req0)
+        max_iter = [1 if e.threshold is None else max(0, min(self.chunk, e.req.steps - e.iterations))
+                    for e in self.entries]
+        thr = [0.0 if e.threshold is None else e.threshold for e in self.entries]
+        t, it, res = self.arena.run(method, req0.courant, max_iter, variable=-1, threshold=thr, context=mctx,
+                                    time=[e.time for e in self.entries])
+        status = self.arena.status()
+        going = []
+        for i, e in enumerate(self.entries):
+            e.time = float(t[i])
+            e.iterations += int(it[i])
+            e.residual = res[i].copy()
+            first = e.threshold is None
+            if first:
+                e.threshold = e.req.tolerance * float(np.max(res[i])) if e.req.tolerance > 0 else 0.0
+            stopped_early = not first and it[i] < max_iter[i]  # below the threshold (or failed)
+            if status[i] != 0 or stopped_early or e.iterations >= e.req.steps:
+                r = e.req
+                r.iterations = e.iterations
+                r.residual = e.residual
+                if status[i] != 0:
+                    r.error = "non-finite time step or residual"
+                else:
+                    r.state = self.arena.get_primitive(i)[: e.eqns.mesh.num_inner_cells].copy()
+                finished.append(e)
+            else:
+                going.append(e)
+        self.entries = going
+        return [e.req for e in finished]
+
+    def close(self):
+        if self.arena is not None:
+            self.arena.close()
+            self.arena = None
+        self.arena_entries = []
+
+
 class Server:
-    """GPU solve server: `Scheduler` with `solve` as the executor, one CUDA stream per request."""
+    """Continuous-batching GPU solve server: admission by HBM budget in arrival order (no overtaking),
+    host meshes built on a thread pool as requests arrive, one `Lane` per scheme on its own thread
+    and CUDA stream, requests joining and leaving their lane's arena between rounds of `chunk`
+    steps."""
+
+    def __init__(self, budget_bytes=None, max_active=64, chunk=10, device=0, builders=4):
+        import torch
+
+        torch.cuda.set_device(device)
+        if budget_bytes is None:
+            free, _ = torch.cuda.mem_get_info()
+            budget_bytes = int(0.8 * free)
+        self.torch = torch
+        self.device = device
+        self.budget = int(budget_bytes)
+        self.max_active = int(max_active)
+        self.chunk = int(chunk)
+        self.builders = int(builders)
+        self.used = 0
+        self.peak_used = 0
+        self.peak_active = 0
+        self.lanes = {}
+        self.repacks = 0
+        self._requests = {}
+        self._cancel_pending = set()
+        self._cancel_lock = threading.Lock()
+
+    def cancel(self, rid):
+        """Cancel request `rid`: one not yet admitted never runs; a running one leaves its lane at the
+        next round (its memory is released then)."""
+        with self._cancel_lock:
+            r = self._requests.get(rid)
+            if r is None:
+                self._cancel_pending.add(rid)
+                return False
+            r.cancelled = True
+            return True
+
+    def serve(self, requests, timeout=None):
+        """Serve `requests` (arrival times relative to now) to completion; returns them by id."""
+        import concurrent.futures
+        import queue
+
+        torch = self.torch
+        clock = time.perf_counter
+        t0 = clock()
+        pending = sorted(requests, key=lambda r: (r.arrival, r.id))
+        with self._cancel_lock:
+            self._requests = {r.id: r for r in pending}
+            for rid in self._cancel_pending:
+                if rid in self._requests:
+                    self._requests[rid].cancelled = True
+        total = len(pending)
+        done = []
+        building = {}  # id -> (request, future)
+        waiting = []   # arrival order, host problem built or being built
+        active = {}    # id -> bytes
+        finished_q = queue.Queue()
+        lane_inbox = {}
+        threads = {}
+        stop = threading.Event()
+        lock = threading.Lock()
+
+        def lane_loop(key, inbox):
+            torch.cuda.set_device(self.device)
+            stream = torch.cuda.Stream()
+            lane = Lane(key, self.chunk, stream.cuda_stream)
+            try:
+                while not stop.is_set():
+                    try:
+                        while True:
+                            req, eqns = inbox.get_nowait()
+                            lane.join(req, eqns)
+                    except queue.Empty:
+                        pass
+                    if not lane.entries:
+                        lane.close()
+                        try:
+                            req, eqns = inbox.get(timeout=0.02)
+                            lane.join(req, eqns)
+                        except queue.Empty:
+                            continue
+                    try:
+                        for r in lane.round():
+                            finished_q.put(r)
+                    except Exception as exc:  # the lane's requests fail, the server goes on
+                        for e in lane.entries:
+                            e.req.error = f"{type(exc).__name__}: {exc}"
+                            finished_q.put(e.req)
+                        lane.entries = []
+                        lane.close()
+            finally:
+                lane.close()
+                with lock:
+                    self.repacks += lane.repacks
+
+        pool = concurrent.futures.ThreadPoolExecutor(max_workers=self.builders)
+        deadline = None if timeout is None else t0 + timeout
+        try:
+            while len(done) < total:
+                now = clock() - t0
+                while pending and pending[0].arrival <= now:
+                    r = pending.pop(0)
+                    if memory_estimate(r) > self.budget:
+                        r.error = "request exceeds the device memory budget"
+                        r.finished = now
+                        done.append(r)
+                        continue
+                    building[r.id] = (r, pool.submit(build_problem, r))
+                    waiting.append(r)
+                # admit in arrival order while memory and slots allow (no overtaking)
+                while waiting and len(active) < self.max_active:
+                    r = waiting[0]
+                    if r.cancelled:  # never admitted
+                        waiting.pop(0)
+                        building.pop(r.id)[1].cancel()
+                        r.error = "cancelled"
+                        r.finished = clock() - t0
+                        done.append(r)
+                        continue
+                    nbytes = memory_estimate(r)
+                    if self.used + nbytes > self.budget:
+                        break
+                    fut = building[r.id][1]
+                    if not fut.done():
+                        break
+                    waiting.pop(0)
+                    del building[r.id]
+                    try:
+                        eqns = fut.result()
+                    except Exception as exc:
+                        r.error = f"{type(exc).__name__}: {exc}"
+                        r.finished = clock() - t0
+                        done.append(r)
+                        continue
+                    self.used += nbytes
+                    self.peak_used = max(self.peak_used, self.used)
+                    active[r.id] = nbytes
+                    self.peak_active = max(self.peak_active, len(active))
+                    r.admitted = clock() - t0
+                    key = lane_key(r)
+                    if key not in lane_inbox:
+                        lane_inbox[key] = queue.Queue()
+                        threads[key] = threading.Thread(target=lane_loop, args=(key, lane_inbox[key]), daemon=True)
+                        threads[key].start()
+                    lane_inbox[key].put((r, eqns))
+                try:
+                    wait = 0.01
+                    if pending:
+                        wait = max(0.0, min(wait, pending[0].arrival - (clock() - t0)))
+                    r = finished_q.get(timeout=wait)
+                    while True:
+                        r.finished = clock() - t0
+                        self.used -= active.pop(r.id)
+                        done.append(r)
+                        r = finished_q.get_nowait()
+                except queue.Empty:
+                    pass
+                if deadline is not None and clock() > deadline:
+                    raise TimeoutError("serving did not finish in time")
+        finally:
+            stop.set()
+            for th in threads.values():
+                th.join(timeout=60)
+            pool.shutdown(wait=False, cancel_futures=True)
+        self.lanes = list(threads)
+        return sorted(done, key=lambda r: r.id)
+
+
+class StreamServer:
+    """GPU solve server without shared launches: `Scheduler` with `solve` as the executor, one
+    context, CUDA stream and host thread per request (their kernels overlap on the device)."""
 
     def __init__(self, budget_bytes=None, max_active=8, device=0):
         import torch
@@ -249,22 +577,32 @@ class Server:
         return self.scheduler.run(requests, timeout=timeout)
 
 
-def poisson_requests(num, rate, seed, min_cells=20_000, max_cells=2_000_000, steps=(50, 200)):
-    """Seeded Poisson arrivals; mesh sizes log-uniform in [min_cells, max_cells]; Mach 0.2-3.0;
-    flux scheme per request; tolerance 1e-6..1e-10."""
+def poisson_requests(num, rate, seed, min_cells=20_000, max_cells=2_000_000, steps=(50, 200), mesh="channel",
+                     physics=(_lib.TG_EULER,), method="lserk", courant=None):
+    """Seeded Poisson arrivals; mesh sizes log-uniform in [min_cells, max_cells]; Mach 0.2-3.0; flux
+    scheme (roe / hllc / ausmd), equations (from `physics`) and tolerance 1e-6..1e-10 per request;
+    channel boxes, or the batch workload's ramp meshes (`mesh="ramp"`)."""
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
     for i in range(num):
         t += rng.exponential(1.0 / rate)
         cells = math.exp(rng.uniform(math.log(min_cells), math.log(max_cells)))
-        nz = 2
-        ny = max(4, int(round(math.sqrt(cells / (3 * nz)))))
-        nx = max(4, int(round(cells / (ny * nz))))
+        if mesh == "ramp":
+            n = max(8, int(round((cells / 4.64) ** (1.0 / 3.0))))
+            dims = (n, n, n)
+        else:
+            nz = 2
+            ny = max(4, int(round(math.sqrt(cells / (3 * nz)))))
+            nx = max(4, int(round(cells / (ny * nz))))
+            dims = (nx, ny, nz)
+        phys = int(rng.choice(list(physics)))
         out.append(Request(
-            id=i, cells=(nx, ny, nz), mach=float(rng.uniform(0.2, 3.0)), angle=float(rng.uniform(0, 10)),
+            id=i, cells=dims, mach=float(rng.uniform(0.2, 3.0)), angle=float(rng.uniform(0, 10)),
             flux=str(rng.choice(["roe", "hllc", "ausmd"])), steps=int(rng.integers(steps[0], steps[1] + 1)),
-            tolerance=float(10 ** rng.uniform(-10, -6)), arrival=t))
+            tolerance=float(10 ** rng.uniform(-10, -6)), arrival=t, physics=phys, mesh=mesh, seed=1000 + i,
+            method=method, courant=courant if courant else (0.5 if method == "lserk" else 30.0),
+            limiter="venkatakrishnan" if method == "implicit euler" else "minmod"))
     return out
 
 
