@@ -325,42 +325,51 @@ def mpi_sample(steps, warmup, ranks, n=128):
 
 
 def run_serving(args, world, rank):
-    """Serving benchmark: seeded Poisson arrivals of steady solve requests (meshes of 20k-2M cells,
-    Mach 0.2-3.0, flux scheme and tolerance per request), served with continuous admission by HBM
-    budget and overlapping solves, against the same requests solved one at a time in arrival order
-    (first in, first out). Each latency runs from arrival to result on the host (mesh generation,
-    upload, solve, read-back)."""
+    """Serving benchmark: seeded Poisson arrivals of steady solve requests on
+    the batch workload's ramp meshes (20k-2M cells, log-uniform), Mach 0.2-3.0, Euler or
+    Navier-Stokes, flux scheme (roe / hllc / ausmd) and tolerance 1e-6..1e-10 per request, implicit
+    Euler with teal's steady Newton-Krylov settings; served with continuous batching (lanes of one
+    scheme sharing an arena, requests joining and leaving between rounds, admission by HBM budget),
+    against the same requests solved one at a time in arrival order (first in, first out). Each
+    latency runs from arrival to result on the host (mesh generation, upload, solve, read-back)."""
     import dataclasses
 
     import torch
 
+    import teal_b200 as tb
     from teal_b200 import serving
 
     if rank != 0:
         return
     torch.cuda.set_device(0)
-    reqs = serving.poisson_requests(args.requests, rate=args.rate, seed=7, steps=(50, 200))
+    reqs = serving.poisson_requests(args.requests, rate=args.rate, seed=7, steps=(10, 40), mesh="ramp",
+                                    physics=(tb.TG_EULER, tb.TG_NAVIERSTOKES), method="implicit euler",
+                                    courant=10.0)
     # warm-up: one small solve (library load, graph capture paths)
     serving.solve(serving.Request(id=-1, cells=(64, 32, 2), steps=5))
     torch.cuda.synchronize()
 
-    server = serving.Server(max_active=args.max_active)
+    server = serving.Server(max_active=args.max_active, chunk=5)
     sampler = ClockSampler(0)
     sampler.start()
     t0 = time.perf_counter()
     done = server.serve([dataclasses.replace(r) for r in reqs], timeout=1800)
     served_s = time.perf_counter() - t0
     clocks = sampler.stop()
-    errors = [r.error for r in done if r.error]
+    errors = {r.id: r.error for r in done if r.error}
     lat = [r.latency for r in done if not r.error]
     work = sum(r.num_cells * r.iterations for r in done if not r.error)
+    stopped_by_tolerance = sum(1 for r in done if not r.error and r.iterations < r.steps)
 
     # one at a time: solve durations measured alone, queued first in, first out at the same arrivals
     durations = []
     for r in reqs:
         solo = dataclasses.replace(r)
         a = time.perf_counter()
-        serving.solve(solo)
+        try:
+            serving.solve(solo)
+        except Exception:  # a request that fails alone fails in the server too
+            pass
         durations.append(time.perf_counter() - a)
     finish, fifo_lat = 0.0, []
     for r, d in zip(reqs, durations):
@@ -368,17 +377,23 @@ def run_serving(args, world, rank):
         finish = start + d
         fifo_lat.append(finish - r.arrival)
     seq_s = finish - reqs[0].arrival
+    ok = [i for i, r in enumerate(done) if not r.error]
     line = {
         "metric": "serving: p50/p99 solve latency and aggregate cell-updates/s", "value": work / served_s,
         "unit": "cell-updates/s", "n_gpus": 1, "steps": len(reqs), "warmup": 1,
         "ms_per_step": 1000 * served_s / len(reqs), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{len(reqs)} poisson requests at {args.rate}/s, meshes 20k-2M cells, mach 0.2-3.0, "
-                               "roe/hllc/ausmd, tolerance 1e-6..1e-10, 50-200 lserk steps",
-                   "max_active": args.max_active, "budget_bytes": server.scheduler.budget},
+        "config": {"workload": f"{len(reqs)} poisson requests at {args.rate}/s, ramp meshes 20k-2M cells, "
+                               "mach 0.2-3.0, euler or navier-stokes, roe/hllc/ausmd + venkatakrishnan(1), "
+                               "tolerance 1e-6..1e-10, 10-40 implicit euler steps cfl 10, newton-krylov "
+                               "{0.1, 0.3, 30}, continuous batching in lanes of one scheme",
+                   "max_active": args.max_active, "budget_bytes": server.budget, "round_steps": server.chunk},
         "latency_p50_s": serving.percentile(lat, 50), "latency_p99_s": serving.percentile(lat, 99),
-        "makespan_s": served_s, "peak_active": server.scheduler.peak_active, "errors": errors,
-        "one_at_a_time": {"value": work / sum(durations), "latency_p50_s": serving.percentile(fifo_lat, 50),
+        "makespan_s": served_s, "peak_active": server.peak_active, "lanes": len(server.lanes),
+        "arena_repacks": server.repacks, "arena_repack_s": server.repack_s,
+        "stopped_by_tolerance": stopped_by_tolerance, "errors": errors,
+        "one_at_a_time": {"value": work / sum(durations[i] for i in ok) if ok else None,
+                          "latency_p50_s": serving.percentile(fifo_lat, 50),
                           "latency_p99_s": serving.percentile(fifo_lat, 99), "makespan_s": seq_s},
         "clocks": clocks,
     }
@@ -635,9 +650,9 @@ def main():
                     help="batch implicit: run each instance to this relative residual drop (0: fixed --steps)")
     ap.add_argument("--courant", type=float, default=None, help="batch implicit: CFL number (default 30)")
     ap.add_argument("--solo-sample", type=int, default=16, help="batch: meshes timed one at a time")
-    ap.add_argument("--requests", type=int, default=16, help="serve: number of requests")
+    ap.add_argument("--requests", type=int, default=32, help="serve: number of requests")
     ap.add_argument("--rate", type=float, default=8.0, help="serve: arrivals per second")
-    ap.add_argument("--max-active", type=int, default=8, help="serve: concurrent solves")
+    ap.add_argument("--max-active", type=int, default=64, help="serve: requests resident at once")
     ap.add_argument("--n", type=int, default=None, help="mesh cells per axis (tgv 128, ramp 80)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "exact"],
                     help="fp64: plain FP64; fp32: FP32-flux form; exact: FP64 with teal's exact arithmetic")

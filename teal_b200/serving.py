@@ -276,7 +276,7 @@ def solve(req, stream=None, chunk=25):
         n = min(chunk, req.steps - total)
         t, it, res = ctx.run(method, req.courant, n, threshold=threshold, context=mctx, time=t)
         total += it
-        if it < n:  # the residual fell below the threshold
+        if threshold > 0 and float(np.max(res)) < threshold:  # the device's stop test (run.c:80-82)
             break
     req.iterations = total
     req.residual = res
@@ -303,37 +303,85 @@ class Lane:
     `round()` advances every running request by up to `chunk` steps in one batched run (a request's
     first step alone, as `solve` takes it, since its residual sets the request's threshold), then
     removes the requests that finished (step budget, tolerance, a non-finite state, cancellation).
-    When the set of requests changed, the arena is re-packed before the run: the running requests'
-    states (all rows, exact FP64) are read out, the old arena is released, and a new arena is built
-    for the current set with those states, so a request's steps are the ones it takes alone."""
+    Joining requests get a new arena: it is built (host merge and upload of every mesh) on a
+    background thread while the current arena keeps stepping; at the next round boundary the running
+    requests' states (all rows, exact FP64) move over and the lane switches, so a request's steps are
+    the ones it takes alone. Finished requests stay in the arena without steps until a re-pack, which
+    also starts when they hold more than half of its cells."""
 
-    def __init__(self, key, chunk, stream=None):
+    def __init__(self, key, chunk, stream=None, device=0):
         self.key = key
         self.chunk = int(chunk)
         self.stream = stream
+        self.device = device
         self.entries = []
         self.arena = None
         self.arena_entries = []
+        self.next = None  # (thread, result holder, entries) of an arena being built
         self.repacks = 0
+        self.repack_s = 0.0
 
     def join(self, req, eqns):
         self.entries.append(_Entry(req, eqns))
 
-    def _repack(self):
+    def _build(self, entries):
         from .api import Batch
 
-        if self.arena is not None:
-            keep = {id(e) for e in self.entries}
-            for i, e in enumerate(self.arena_entries):
-                if id(e) in keep:
-                    e.eqns.primitive[:] = self.arena.get_primitive(i)
-            self.arena.close()
-            self.arena = None
-        self.arena = Batch([e.eqns for e in self.entries], precision=self.entries[0].req.precision)
+        t0 = time.perf_counter()
+        arena = Batch([e.eqns for e in entries], precision=entries[0].req.precision)
         if self.stream is not None:
-            self.arena.set_stream(self.stream)
-        self.arena_entries = list(self.entries)
+            arena.set_stream(self.stream)
+        return arena, time.perf_counter() - t0
+
+    def _start_build(self):
+        import torch
+
+        entries = list(self.entries)
+        holder = {}
+
+        def work():
+            try:
+                torch.cuda.set_device(self.device)
+                holder["arena"], holder["secs"] = self._build(entries)
+            except Exception as exc:  # reported at the switch
+                holder["error"] = exc
+
+        th = threading.Thread(target=work, daemon=True)
+        th.start()
+        self.next = (th, holder, entries)
+
+    def _switch(self):
+        """Move the running requests' states from the current arena into the built one."""
+        th, holder, entries = self.next
+        th.join()
+        self.next = None
+        if "error" in holder:
+            raise holder["error"]
+        arena = holder["arena"]
+        t0 = time.perf_counter()
+        if self.arena is not None:
+            where = {id(e): i for i, e in enumerate(self.arena_entries)}
+            for j, e in enumerate(entries):
+                if id(e) in where:
+                    arena.set_primitive(j, self.arena.get_primitive(where[id(e)]))
+            self.arena.close()
+        self.arena = arena
+        self.arena_entries = entries
         self.repacks += 1
+        self.repack_s += holder["secs"] + (time.perf_counter() - t0)
+
+    def _needs_repack(self):
+        """A request joined (it has no row in the arena), or finished requests, which sit in the arena
+        without steps, hold more than half of its cells."""
+        if self.arena is None:
+            return True
+        inside = {id(e) for e in self.arena_entries}
+        if any(id(e) not in inside for e in self.entries):
+            return True
+        live = {id(e) for e in self.entries}
+        idle = sum(e.eqns.mesh.num_inner_cells for e in self.arena_entries if id(e) not in live)
+        total = sum(e.eqns.mesh.num_inner_cells for e in self.arena_entries)
+        return 2 * idle > total
 
     def round(self):
         """One round; returns the requests that finished in it."""
@@ -345,26 +393,38 @@ class Lane:
         if not self.entries:
             self.close()
             return [e.req for e in finished]
-        if self.arena_entries != self.entries:
-            self._repack()
+        if self.next is not None and not self.next[0].is_alive():
+            self._switch()
+        if self.next is None and self._needs_repack():
+            self._start_build()
+        live = {id(e) for e in self.entries}
+        if self.arena is None or not any(id(e) in live for e in self.arena_entries):
+            if self.next is None:
+                self._start_build()
+            self._switch()  # nothing to step meanwhile: wait for the new arena
         req0 = self.entries[0].req
         method, mctx = method_of(req0)
-        max_iter = [1 if e.threshold is None else max(0, min(self.chunk, e.req.steps - e.iterations))
-                    for e in self.entries]
-        thr = [0.0 if e.threshold is None else e.threshold for e in self.entries]
+        # requests that finished, or joined after this arena was built, take no steps in it
+        max_iter = [0 if id(e) not in live else
+                    1 if e.threshold is None else max(0, min(self.chunk, e.req.steps - e.iterations))
+                    for e in self.arena_entries]
+        thr = [0.0 if e.threshold is None else e.threshold for e in self.arena_entries]
         t, it, res = self.arena.run(method, req0.courant, max_iter, variable=-1, threshold=thr, context=mctx,
-                                    time=[e.time for e in self.entries])
+                                    time=[e.time for e in self.arena_entries])
         status = self.arena.status()
-        going = []
-        for i, e in enumerate(self.entries):
+        done_ids = set()
+        for i, e in enumerate(self.arena_entries):
+            if id(e) not in live:
+                continue
             e.time = float(t[i])
             e.iterations += int(it[i])
             e.residual = res[i].copy()
             first = e.threshold is None
             if first:
                 e.threshold = e.req.tolerance * float(np.max(res[i])) if e.req.tolerance > 0 else 0.0
-            stopped_early = not first and it[i] < max_iter[i]  # below the threshold (or failed)
-            if status[i] != 0 or stopped_early or e.iterations >= e.req.steps:
+            # the device's stop test (run.c:80-82), also when it fired on the round's last step
+            converged = not first and e.threshold > 0 and float(np.max(res[i])) < e.threshold
+            if status[i] != 0 or converged or e.iterations >= e.req.steps:
                 r = e.req
                 r.iterations = e.iterations
                 r.residual = e.residual
@@ -373,12 +433,17 @@ class Lane:
                 else:
                     r.state = self.arena.get_primitive(i)[: e.eqns.mesh.num_inner_cells].copy()
                 finished.append(e)
-            else:
-                going.append(e)
-        self.entries = going
+                done_ids.add(id(e))
+        self.entries = [e for e in self.entries if id(e) not in done_ids]
         return [e.req for e in finished]
 
     def close(self):
+        if self.next is not None:
+            th, holder, _ = self.next
+            th.join()
+            self.next = None
+            if "arena" in holder:
+                holder["arena"].close()
         if self.arena is not None:
             self.arena.close()
             self.arena = None
@@ -409,6 +474,7 @@ class Server:
         self.peak_active = 0
         self.lanes = {}
         self.repacks = 0
+        self.repack_s = 0.0
         self._requests = {}
         self._cancel_pending = set()
         self._cancel_lock = threading.Lock()
@@ -452,7 +518,7 @@ class Server:
         def lane_loop(key, inbox):
             torch.cuda.set_device(self.device)
             stream = torch.cuda.Stream()
-            lane = Lane(key, self.chunk, stream.cuda_stream)
+            lane = Lane(key, self.chunk, stream.cuda_stream, self.device)
             try:
                 while not stop.is_set():
                     try:
@@ -481,6 +547,7 @@ class Server:
                 lane.close()
                 with lock:
                     self.repacks += lane.repacks
+                    self.repack_s += lane.repack_s
 
         pool = concurrent.futures.ThreadPoolExecutor(max_workers=self.builders)
         deadline = None if timeout is None else t0 + timeout
