@@ -268,6 +268,40 @@ int tg_batch_run(tg_ctx *ctx, int method, const void *context, double courant, c
  * counterpart in teal (one mesh per process there). */
 int tg_batch_status(tg_ctx *ctx, int *status);
 
+/* ---- partitions: one rank's share of a mesh (several GPUs) ---------------------------------------
+ * teal decomposes a mesh over MPI ranks and exchanges one layer of ghost cells (src/equations/
+ * exchange.c:8-51, src/mesh/create.c:351-440). A partition here is the same idea for one GPU per
+ * rank: `mesh` holds the rank's inner cells [0, C), the boundary ghosts of its boundary faces
+ * [C, off_boundary) and the periodic ghosts of its periodic faces [off_boundary, num_cells), and
+ * the global mesh's faces that touch its inner cells, in global order and orientation. An inner
+ * face may reference a halo row, off_boundary + h for h < num_halo: an inner cell of another rank.
+ * owner[p] is the state row (an inner cell or a halo row) whose state periodic ghost off_boundary + p
+ * takes; send_rows are the inner cells whose states and gradient records other ranks' halos receive.
+ * mesh->sum_volume is the whole mesh's. Explicit methods only; no source terms or custom boundaries.
+ * Every rank's own cells then sum their faces in the global order, and a face shared by two ranks
+ * is computed on both from the same inputs: the state after a step equals the single-mesh run's. */
+int tg_create_partition(const tg_mesh *mesh, const tg_equations *eqns, int precision, const int *owner,
+                        int num_halo, const int *send_rows, int num_send, tg_ctx **ctx);
+/* Device pointers of the exchange buffers: states send_q[num_send][5] and recv_q[num_halo][5]
+ * (FP64), gradient records send_rec[num_send] and recv_rec[num_halo] of *record_bytes each. The
+ * caller moves send data into the receiving ranks' recv buffers in their halo order. */
+int tg_part_buffers(tg_ctx *ctx, void **send_q, void **recv_q, void **send_rec, void **recv_rec,
+                    long *record_bytes);
+/* A step: tg_part_step_begin gives the minimum stable step of this rank's cells (equations_timestep
+ * over its share); the caller takes the minimum over ranks, times the CFL number and clipped, and
+ * sets it with tg_part_set_step; each RK stage runs tg_part_phase 0, 1, 2 with alpha_{i+1} (and
+ * last on the final stage), exchanging states after phase 0 and records after phase 1 (phase 0
+ * packs, phase 1 and 2 unpack first); tg_part_residual_sums gives this rank's sums of V R^2 of the
+ * last stage (the norm is sqrt of their sum over ranks divided by the total volume). The context's
+ * stream (tg_stream_of) orders everything; the host functions that return values synchronise it. */
+int tg_part_step_begin(tg_ctx *ctx, double *local_min);
+int tg_part_set_step(tg_ctx *ctx, double step, double time);
+int tg_part_phase(tg_ctx *ctx, int phase, double alpha, int last);
+int tg_part_residual_sums(tg_ctx *ctx, double *sums);
+int tg_stream_of(tg_ctx *ctx, void **stream);
+/* teal's low-storage RK coefficients alpha[0..stages] (src/simulation/advance.c:50-75) */
+int tg_lserk_alpha(int order, int stages, double *alpha);
+
 /* ---- drop-in Advance methods with teal's signature (src/simulation.h:6-7) ----------------------- */
 
 /* Bind a teal `Equations *` (used only as a lookup key) to a context and to the host primitive

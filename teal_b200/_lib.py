@@ -138,6 +138,16 @@ SIGNATURES = [
     ("tg_batch_run", ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_double, _vp, _vp, _vp, _vp, _vp, _vp,
                                     _vp]),
     ("tg_batch_status", ctypes.c_int, [_vp, _vp]),
+    ("tg_create_partition", ctypes.c_int, [ctypes.POINTER(TgMesh), ctypes.POINTER(TgEquations), ctypes.c_int, _vp,
+                                           ctypes.c_int, _vp, ctypes.c_int, ctypes.POINTER(_vp)]),
+    ("tg_part_buffers", ctypes.c_int, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.POINTER(_vp),
+                                       ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_long)]),
+    ("tg_part_step_begin", ctypes.c_int, [_vp, _dbl_p]),
+    ("tg_part_set_step", ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double]),
+    ("tg_part_phase", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_int]),
+    ("tg_part_residual_sums", ctypes.c_int, [_vp, _vp]),
+    ("tg_stream_of", ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
+    ("tg_lserk_alpha", ctypes.c_int, [ctypes.c_int, ctypes.c_int, _dbl_p]),
     ("tg_bind", ctypes.c_int, [_vp, _vp, _vp]),
     ("tg_unbind", ctypes.c_int, [_vp]),
     ("tg_teal_euler", ctypes.c_double, [_vp, _dbl_p, _vp, ctypes.c_double, ctypes.c_double, _vp]),

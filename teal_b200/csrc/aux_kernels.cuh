@@ -197,22 +197,24 @@ __global__ void k_count_active(int ninst, Steps st)
 
 // ---- device mesh upload: per-cell slot lists (integer work, checked against a host recompute) --
 
-// count faces per inner cell
-__global__ void k_slot_count(int F, int F_in, const int2 *__restrict__ lr, int *__restrict__ cnt)
+// count faces per inner cell; a partition's halo rows (>= C) sit on faces but own no slots
+__global__ void k_slot_count(int F, int F_in, int C, const int2 *__restrict__ lr, int *__restrict__ cnt)
 {
     int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= F) {
         return;
     }
     int2 c = lr[f];
-    atomicAdd(cnt + c.x, 1);
-    if (f < F_in) {
+    if (c.x < C) {
+        atomicAdd(cnt + c.x, 1);
+    }
+    if (f < F_in && c.y < C) {
         atomicAdd(cnt + c.y, 1);
     }
 }
 
 // scatter face references into the ELL slots (arbitrary order; sorted afterwards)
-__global__ void k_slot_fill(int F, int F_in, int SL, const int2 *__restrict__ lr, int *__restrict__ cursor,
+__global__ void k_slot_fill(int F, int F_in, int C, int SL, const int2 *__restrict__ lr, int *__restrict__ cursor,
                             int *__restrict__ slot_face)
 {
     int f = blockIdx.x * blockDim.x + threadIdx.x;
@@ -220,11 +222,13 @@ __global__ void k_slot_fill(int F, int F_in, int SL, const int2 *__restrict__ lr
         return;
     }
     int2 c = lr[f];
-    int j = atomicAdd(cursor + c.x, 1);
-    if (j < MAX_SLOTS) {
-        slot_face[j * SL + c.x] = f;
+    if (c.x < C) {
+        int j = atomicAdd(cursor + c.x, 1);
+        if (j < MAX_SLOTS) {
+            slot_face[j * SL + c.x] = f;
+        }
     }
-    if (f < F_in) {
+    if (f < F_in && c.y < C) {
         int k = atomicAdd(cursor + c.y, 1);
         if (k < MAX_SLOTS) {
             slot_face[k * SL + c.y] = ~f;
@@ -397,6 +401,70 @@ __global__ void k_grad_to_aos(int C, const R *__restrict__ rec, int limit, doubl
         aos[(size_t)i * 15 + 3 * v] = double(gx);
         aos[(size_t)i * 15 + 3 * v + 1] = double(gy);
         aos[(size_t)i * 15 + 3 * v + 2] = double(gz);
+    }
+}
+
+// ---- halo of a partition (one rank's share of a mesh) ---------------------------------------------
+//
+// A partition's state has, after its inner cells and boundary ghosts, one row per halo cell (an
+// inner cell of another rank on a face of this rank's cells). Before the gradient the halo rows
+// receive their owners' states, before the face fluxes their gradient records: packed by the owner
+// from its `send` rows, moved by the caller, unpacked here in halo order.
+
+// buf[i][v] = q[v][rows[i]]
+__global__ void k_halo_pack_q(int n, const int *__restrict__ rows, int N, const double *__restrict__ q,
+                              double *__restrict__ buf)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+    const int r = rows[i];
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        buf[(size_t)i * 5 + v] = q[(size_t)v * N + r];
+    }
+}
+
+// q[v][row0 + i] = buf[i][v]
+__global__ void k_halo_unpack_q(int n, int row0, int N, const double *__restrict__ buf, double *__restrict__ q)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        q[(size_t)v * N + row0 + i] = buf[(size_t)i * 5 + v];
+    }
+}
+
+// gradient records (20 values of type R per row): buf[i] = rec[rows[i]], and back into rows row0 + i
+template <typename R>
+__global__ void k_halo_pack_rec(int n, const int *__restrict__ rows, const R *__restrict__ rec, R *__restrict__ buf)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+    const R *src = rec + (size_t)rows[i] * 20;
+#pragma unroll
+    for (int k = 0; k < 20; k++) {
+        buf[(size_t)i * 20 + k] = src[k];
+    }
+}
+
+template <typename R>
+__global__ void k_halo_unpack_rec(int n, int row0, const R *__restrict__ buf, R *__restrict__ rec)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+    R *dst = rec + (size_t)(row0 + i) * 20;
+#pragma unroll
+    for (int k = 0; k < 20; k++) {
+        dst[k] = buf[(size_t)i * 20 + k];
     }
 }
 

@@ -278,6 +278,13 @@ struct tg_ctx {
     // created by tg_batch_create: an instance that goes non-finite stops alone (tg_batch_status)
     bool batch = false;
 
+    // a partition (tg_create_partition): halo rows [N - halo, N), rows sent to other ranks, and the
+    // packed exchange buffers
+    int halo = 0, nsend = 0;
+    int *send_rows = nullptr;
+    double *send_q = nullptr, *recv_q = nullptr;  // [nsend][5], [halo][5]
+    void *send_rec = nullptr, *recv_rec = nullptr;  // [nsend][20], [halo][20] records (R)
+
     // implicit step graph (device-driven Newton / Arnoldi / Gram-Schmidt loops) and its key
     cudaGraphExec_t igraph = nullptr;
     long igraph_kernels = 0;
@@ -338,7 +345,8 @@ static void free_ctx(tg_ctx *c)
                     c->gb.slot_w, c->gb.slot_off, c->gb.area32, c->gb.basis32, c->gb.offl32, c->gb.offr32,
                     c->gb.corr32, c->gb.slot_w32, c->gb.slot_off32, c->q, c->U0, c->R, c->qs, c->grad, c->G,
                     c->dtc, c->part_min, c->part_sum, c->sd, c->si, c->aos, c->rowmap, c->cell_inst,
-                    c->inst_cell_off, c->piece_beg, c->inst_piece_off, c->sum_volume, c->src_avg};
+                    c->inst_cell_off, c->piece_beg, c->inst_piece_off, c->sum_volume, c->src_avg,
+                    c->send_rows, c->send_q, c->recv_q, c->send_rec, c->recv_rec};
     for (void *p : ptrs) {
         if (p) cudaFree(p);
     }
@@ -410,6 +418,8 @@ struct MeshInput {
     std::vector<double> sum_volume; // per instance
     std::vector<int> inst_row_off;  // teal rows per instance
     std::vector<int> rowmap;        // teal row -> arena row (periodic ghosts: the owner's row)
+    int halo = 0;                   // partitions: halo rows after the boundary ghosts
+    std::vector<int> send_rows;     // partitions: rows whose state / records other ranks receive
 };
 
 // periodic ghost -> owner cell, by matching each receive tag with the send posted under it
@@ -756,7 +766,7 @@ static int create_ctx(MeshInput &in, const tg_equations *e, int precision, tg_ct
 
         Sizes &s = c->s;
         s.C = m->num_inner_cells;
-        s.N = m->off_boundary_cells;
+        s.N = m->off_boundary_cells + in.halo;  // state rows: inner, boundary ghosts, halo (partitions)
         s.F = m->num_faces;
         s.F_in = m->num_inner_faces;
         s.F_bd = m->off_boundary_faces;
@@ -827,8 +837,8 @@ static int create_ctx(MeshInput &in, const tg_equations *e, int precision, tg_ct
             CU(cudaMemsetAsync(c->slot_nbr, 0, MAX_SLOTS * sizeof(int) * (size_t)s.SL, st));
             CU(cudaMemsetAsync(c->gb.slot_w, 0, 3 * MAX_SLOTS * sizeof(double) * (size_t)s.SL, st));
             CU(cudaMemsetAsync(c->gb.slot_off, 0, 3 * MAX_SLOTS * sizeof(double) * (size_t)s.SL, st));
-            k_slot_count<<<grid_of(s.F), BLOCK, 0, st>>>(s.F, s.F_in, c->lr, d_cnt);
-            k_slot_fill<<<grid_of(s.F), BLOCK, 0, st>>>(s.F, s.F_in, s.SL, c->lr, d_cnt + s.C, c->slot_face);
+            k_slot_count<<<grid_of(s.F), BLOCK, 0, st>>>(s.F, s.F_in, s.C, c->lr, d_cnt);
+            k_slot_fill<<<grid_of(s.F), BLOCK, 0, st>>>(s.F, s.F_in, s.C, s.SL, c->lr, d_cnt + s.C, c->slot_face);
             TRY(upload(&d_weight, m->face_weight, 6 * (size_t)s.F, st));
             TRY(upload(&d_offset, m->face_offset, 6 * (size_t)s.F, st));
             k_slot_finish<double><<<grid_of(s.C), BLOCK, 0, st>>>(s.C, s.SL, c->lr, d_cnt, d_weight, d_offset,
@@ -910,7 +920,17 @@ static int create_ctx(MeshInput &in, const tg_equations *e, int precision, tg_ct
         TRY(dalloc(&c->R, 5 * (size_t)s.C));
         CU(cudaMemsetAsync(c->R, 0, 5 * sizeof(double) * s.C, st));
         if (c->order == 2) {
-            CU(cudaMalloc(&c->grad, 20 * rsz * s.C));
+            // records for every state row: a partition's halo rows receive their owners' records
+            CU(cudaMalloc(&c->grad, 20 * rsz * s.N));
+        }
+        if (in.halo > 0 || !in.send_rows.empty()) {
+            c->halo = in.halo;
+            c->nsend = (int)in.send_rows.size();
+            TRY(upload(&c->send_rows, in.send_rows.data(), in.send_rows.size(), st));
+            TRY(dalloc(&c->send_q, 5 * (size_t)c->nsend));
+            TRY(dalloc(&c->recv_q, 5 * (size_t)c->halo));
+            CU(cudaMalloc(&c->send_rec, 20 * rsz * (size_t)(c->nsend > 0 ? c->nsend : 1)));
+            CU(cudaMalloc(&c->recv_rec, 20 * rsz * (size_t)(c->halo > 0 ? c->halo : 1)));
         }
         // the exact form with a viscous flux keeps the viscous records apart (face.cuh)
         const bool two = precision == TG_PRECISION_FP64_EXACT && c->viscous == TG_VISCOUS_CENTRAL;
@@ -1084,6 +1104,64 @@ extern "C" int tg_create(const tg_mesh *m, const tg_equations *e, int precision,
         return fail(rc, "%s", msg.c_str());
     }
     return TG_OK;
+}
+
+// ---- partitions: one rank's share of a mesh (multi-GPU) ------------------------------------------
+//
+// A partition is uploaded like a one-process mesh whose faces may reference halo rows: state rows
+// after the boundary ghosts that hold inner cells of other ranks. Its faces are the global mesh's
+// faces that touch its own inner cells, in global order and orientation, so every own cell sums
+// its faces in the global order; faces between an own cell and a halo cell are computed on both
+// ranks from the same exchanged inputs. The periodic ghosts of its periodic faces map through
+// `owner` to state rows (own inner cells or halo rows).
+
+extern "C" int tg_create_partition(const tg_mesh *m, const tg_equations *e, int precision, const int *owner,
+                                   int num_halo, const int *send_rows, int num_send, tg_ctx **out)
+{
+    if (!out) return fail(TG_ERR_INVALID, "null output pointer");
+    *out = nullptr;
+    TRY(validate(m, e));
+    if (num_halo < 0 || num_send < 0 || (num_send > 0 && !send_rows))
+        return fail(TG_ERR_INVALID, "invalid halo sizes");
+    if (e->source != TG_SOURCE_NONE)
+        return fail(TG_ERR_INVALID, "source terms are not supported in a partition (their prepare pass is global)");
+    MeshInput in;
+    in.m = *m;
+    const int C = m->num_inner_cells, OB = m->off_boundary_cells, rows = OB + num_halo;
+    const int np = m->num_cells - OB;
+    if (np > 0 && !owner) return fail(TG_ERR_INVALID, "periodic ghosts need their owner rows");
+    in.owner.assign(owner, owner + np);
+    for (int r : in.owner) {
+        if (r < 0 || r >= rows || (r >= C && r < OB))
+            return fail(TG_ERR_INVALID, "periodic ghost owner row %d is neither an inner cell nor a halo row", r);
+    }
+    in.send_rows.assign(send_rows, send_rows + num_send);
+    for (int r : in.send_rows) {
+        if (r < 0 || r >= C) return fail(TG_ERR_INVALID, "send row %d is not an inner cell", r);
+    }
+    for (int f = 0; f < m->off_boundary_faces; f++) {
+        const int l = m->face_cell[2 * f], r = m->face_cell[2 * f + 1];
+        const bool inner = f < m->num_inner_faces;
+        const bool l_ok = (l >= 0 && l < C) || (inner && l >= OB && l < rows);
+        const bool r_ok = inner ? ((r >= 0 && r < C) || (r >= OB && r < rows)) : (r >= C && r < OB);
+        if (!l_ok || !r_ok || (inner && l >= C && r >= C))
+            return fail(TG_ERR_INVALID, "face %d references rows (%d, %d) outside the partition", f, l, r);
+    }
+    TRY(boundary_tables(m, e, in.bent, in.bkind, in.bctx));
+    for (int k : in.bkind) {
+        if (k == TG_BC_CUSTOM) return fail(TG_ERR_INVALID, "custom boundaries are not supported in a partition");
+    }
+    if (e->limiter == TG_LIMITER_VENKATAKRISHNAN) {
+        in.eps2.resize(C);
+        limiter_parameter(m, e, in.eps2.data());
+    }
+    in.inst_cell_off = {0, C};
+    in.sum_volume = {m->sum_volume};
+    in.inst_row_off = {0, m->num_cells};
+    in.rowmap.resize(m->num_cells);
+    for (int r = 0; r < m->num_cells; r++) in.rowmap[r] = r < OB ? r : in.owner[r - OB];
+    in.halo = num_halo;
+    return create_ctx(in, e, precision, out);
 }
 
 extern "C" int tg_batch_create(const tg_mesh *meshes, const tg_equations *eqns, int num, int precision,
@@ -2420,4 +2498,130 @@ extern "C" double tg_teal_implicit_euler(const void *eqns, double *time, void *r
                                          double courant, const void *context)
 {
     return dropin(TG_ADVANCE_IMPLICIT_EULER, eqns, time, residual, max_step, courant, context);
+}
+
+// ---- partitions: the phases of an RK stage around the caller's halo exchange --------------------
+
+// device pointers of the exchange buffers: states [send][5] / [halo][5] (FP64) and gradient records
+// [send][20] / [halo][20] of `record_bytes` / 20 bytes each
+extern "C" int tg_part_buffers(tg_ctx *c, void **send_q, void **recv_q, void **send_rec, void **recv_rec,
+                               long *record_bytes)
+{
+    if (!c) return fail(TG_ERR_INVALID, "null context");
+    if (send_q) *send_q = c->send_q;
+    if (recv_q) *recv_q = c->recv_q;
+    if (send_rec) *send_rec = c->send_rec;
+    if (recv_rec) *recv_rec = c->recv_rec;
+    if (record_bytes) *record_bytes = 20 * (long)(is_fp64(c) ? sizeof(double) : sizeof(float));
+    return TG_OK;
+}
+
+// the cells' stable steps of the current state (U0 refreshed first when the state changed) and
+// their minimum over this partition's cells, in piece order
+extern "C" int tg_part_step_begin(tg_ctx *c, double *local_min)
+{
+    if (!c || !local_min) return fail(TG_ERR_INVALID, "null argument");
+    if (!c->prepared) TRY(run_prepare(c));
+    else TRY(run_pieces(c, 0));
+    std::vector<double> part(c->npieces);
+    CU(cudaMemcpyAsync(part.data(), c->part_min, sizeof(double) * c->npieces, cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    double m = DBL_MAX;
+    for (double v : part) m = fmin(m, v);
+    *local_min = m;
+    return TG_OK;
+}
+
+// the step every rank takes (courant times the minimum over all ranks, clipped) and the time
+extern "C" int tg_part_set_step(tg_ctx *c, double step, double time)
+{
+    if (!c) return fail(TG_ERR_INVALID, "null context");
+    if (!(step > 0) || !std::isfinite(step)) return fail(TG_ERR_NONFINITE, "non-finite time step");
+    hd_at(c, SD_STEP, 0) = step;
+    hd_at(c, SD_STEP0, 0) = step;
+    hd_at(c, SD_TIME, 0) = time;
+    hi_at(c, SI_ACTIVE, 0) = 1;
+    TRY(write_steps(c));
+    return TG_OK;
+}
+
+// One RK stage in three phases, with the halo exchange between them done by the caller:
+//   0  boundary states, then pack the sent rows' states into send_q
+//   1  unpack recv_q into the halo rows, gradients and limiter, pack the sent rows' records
+//   2  unpack recv_rec into the halo records, face fluxes, cell gather and the stage update
+//      U = U0 + alpha step R (the last stage also refreshes U0 and the cells' stable steps)
+extern "C" int tg_part_phase(tg_ctx *c, int phase, double alpha, int last)
+{
+    if (!c) return fail(TG_ERR_INVALID, "null context");
+    const int N = c->s.N, h0 = N - c->halo;
+    const bool f64 = is_fp64(c);
+    if (phase == 0) {
+        TRY(run_boundary(c, c->q));
+        if (c->nsend) k_halo_pack_q<<<grid_of(c->nsend), BLOCK, 0, c->stream>>>(c->nsend, c->send_rows, N, c->q, c->send_q);
+    }
+    else if (phase == 1) {
+        if (c->halo) k_halo_unpack_q<<<grid_of(c->halo), BLOCK, 0, c->stream>>>(c->halo, h0, N, c->recv_q, c->q);
+        CU(cudaGetLastError());
+        if (c->order == 2) {
+            TRY(run_gradient(c, c->q));
+            if (c->nsend && f64)
+                k_halo_pack_rec<double><<<grid_of(c->nsend), BLOCK, 0, c->stream>>>(
+                    c->nsend, c->send_rows, (const double *)c->grad, (double *)c->send_rec);
+            else if (c->nsend)
+                k_halo_pack_rec<float><<<grid_of(c->nsend), BLOCK, 0, c->stream>>>(
+                    c->nsend, c->send_rows, (const float *)c->grad, (float *)c->send_rec);
+        }
+    }
+    else if (phase == 2) {
+        if (c->order == 2 && c->halo) {
+            if (f64)
+                k_halo_unpack_rec<double><<<grid_of(c->halo), BLOCK, 0, c->stream>>>(
+                    c->halo, h0, (const double *)c->recv_rec, (double *)c->grad);
+            else
+                k_halo_unpack_rec<float><<<grid_of(c->halo), BLOCK, 0, c->stream>>>(
+                    c->halo, h0, (const float *)c->recv_rec, (float *)c->grad);
+        }
+        CU(cudaGetLastError());
+        TRY(run_face(c, c->q));
+        TRY(launch_cell<1>(c, alpha, last, c->q, c->R));
+        c->prepared = last != 0;  // the last stage leaves U0 and the cells' steps current
+    }
+    else {
+        return fail(TG_ERR_INVALID, "invalid phase %d", phase);
+    }
+    CU(cudaGetLastError());
+    return TG_OK;
+}
+
+// sums of volume * R^2 per variable over this partition's cells (the last stage's derivative), in
+// piece order; the norm is sqrt(sum over all ranks / total volume)
+extern "C" int tg_part_residual_sums(tg_ctx *c, double *sums)
+{
+    if (!c || !sums) return fail(TG_ERR_INVALID, "null argument");
+    TRY(run_pieces(c, 1));
+    std::vector<double> part(5 * (size_t)c->npieces);
+    CU(cudaMemcpyAsync(part.data(), c->part_sum, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    for (int k = 0; k < 5; k++) {
+        double t = 0;
+        for (int p = 0; p < c->npieces; p++) t += part[5 * (size_t)p + k];
+        sums[k] = t;
+    }
+    return TG_OK;
+}
+
+// teal's low-storage RK coefficients alpha[0..stages] of (order, stages) (advance.c:50-75)
+extern "C" int tg_lserk_alpha(int order, int stages, double *alpha)
+{
+    if (!alpha || order < 1 || order > 3 || stages < 1 || stages > 6)
+        return fail(TG_ERR_INVALID, "invalid lserk order %d / stages %d", order, stages);
+    for (int i = 0; i <= stages; i++) alpha[i] = LSERK_ALPHA[order - 1][stages - 1][i];
+    return TG_OK;
+}
+
+extern "C" int tg_stream_of(tg_ctx *c, void **stream)
+{
+    if (!c || !stream) return fail(TG_ERR_INVALID, "null argument");
+    *stream = (void *)c->stream;
+    return TG_OK;
 }
