@@ -324,6 +324,61 @@ def mpi_sample(steps, warmup, ranks, n=128):
             f"shared-memory MPI subset: {steps} lserk steps after {warmup} warm-up steps, slowest rank")
 
 
+def run_split(args, world, rank, pg):
+    """The Taylor-Green 128^3 workload as ONE mesh over all ranks (strong scaling): teal's grid of
+    ranks and block split (src/mesh/create.c:10-97), each GPU a partition with a one-cell halo;
+    per RK stage the states and then the gradient records of the halo cross between GPUs (NCCL
+    grouped send / receive on the ranks' streams), the step minimum and the residual sums by
+    all-reduce. The state after each step equals the single-mesh run's (tests/test_partition_gpu.py).
+    value = cells of the whole mesh x steps / device time of the slowest rank."""
+    import torch
+
+    import teal_b200 as tb
+    from teal_b200 import partition as pt
+
+    n = args.n
+    lo, hi, nc = (0, 0, 0), (2 * math.pi,) * 3, (n, n, n)
+    t0 = time.perf_counter()
+    mesh = tb.Mesh.create(lo, hi, nc, (1, 1, 1))
+    eqns = tb.Equations.navierstokes(mesh)
+    configure(eqns, "tgv")
+    ranks, dims = pt.cell_ranks(mesh, lo, hi, nc, world)
+    part = pt.partition(mesh, ranks)[rank]
+    prim = tgv_state(mesh.cell_center[: mesh.num_inner_cells])
+    run = pt.DistributedRun(part, eqns, world)
+    run.rank.set_state(prim)
+    t_setup = time.perf_counter() - t0
+    t = 0.0
+    for _ in range(args.warmup):
+        t, s0, res = run.step(t, 0.99)
+    stream = run.rank.stream
+    torch.cuda.synchronize()
+    pg.barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        t, s0, res = run.step(t, 0.99)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    pg.barrier()
+    ms = max_over_ranks(ev0.elapsed_time(ev1), pg)
+    C = mesh.num_inner_cells
+    line = {
+        "metric": METRIC, "value": C * args.steps / (ms / 1000.0), "unit": "cell-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": workload_name("tgv", n), "cells": C, "mesh": f"{n}^3", "global_batch": 1,
+                   "parallelism": f"one mesh split over {world} gpus (rank grid {dims}, one-cell halo)",
+                   "halo_cells_rank0": int(len(part.halo))},
+        "residual": [float(x) for x in res], "setup_s": t_setup,
+    }
+    run.close()
+    if rank == 0:
+        print(json.dumps(line))
+    pg.barrier()
+    pg.destroy_process_group()
+
+
 def run_serving(args, world, rank):
     """Serving benchmark: seeded Poisson arrivals of steady solve requests on
     the batch workload's ramp meshes (20k-2M cells, log-uniform), Mach 0.2-3.0, Euler or
@@ -660,6 +715,9 @@ def main():
     ap.add_argument("--ref-steps", type=int, default=None,
                     help="steps of the CPU baseline sample (tgv: the all-core MPI run, 10; ramp: 20)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--split", action="store_true",
+                    help="tgv with --gpus N: one mesh split over the N GPUs (teal's rank grid, one-cell halo, "
+                         "strong scaling) instead of N independent replicas")
     args = ap.parse_args()
     if args.n is None:
         args.n = 128 if args.workload == "tgv" else 80
@@ -684,13 +742,19 @@ def main():
 
     torch.cuda.set_device(local)
     pg = None
-    if world > 1:
+    if world > 1 or args.split:
         import datetime
 
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        if not dist.is_initialized():
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            os.environ.setdefault("MASTER_PORT", "29511")
+            dist.init_process_group("nccl", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=300))
         pg = dist
+    if args.split:
+        run_split(args, world, rank, pg)
+        return
 
     import teal_b200 as tb
 

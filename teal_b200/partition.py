@@ -292,10 +292,16 @@ class Rank:
         self.record_bytes = rb.value
         ns, nh = len(send), len(part.halo)
         dev = torch.device("cuda", torch.cuda.current_device())
-        self.send_q = torch.as_tensor(_DeviceBytes(p[0].value, 40 * ns), device=dev)
-        self.recv_q = torch.as_tensor(_DeviceBytes(p[1].value, 40 * nh), device=dev)
-        self.send_rec = torch.as_tensor(_DeviceBytes(p[2].value, rb.value * ns), device=dev)
-        self.recv_rec = torch.as_tensor(_DeviceBytes(p[3].value, rb.value * nh), device=dev)
+
+        def view(ptr, n):  # a rank without neighbours has no exchange buffers (NULL, zero bytes)
+            if not ptr or n == 0:
+                return torch.empty(0, dtype=torch.uint8, device=dev)
+            return torch.as_tensor(_DeviceBytes(ptr, n), device=dev)
+
+        self.send_q = view(p[0].value, 40 * ns)
+        self.recv_q = view(p[1].value, 40 * nh)
+        self.send_rec = view(p[2].value, rb.value * ns)
+        self.recv_rec = view(p[3].value, rb.value * nh)
         st = ctypes.c_void_p()
         check(lib.tg_stream_of(self.handle, ctypes.byref(st)))
         self.stream = torch.cuda.ExternalStream(st.value)
