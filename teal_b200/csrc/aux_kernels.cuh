@@ -295,6 +295,29 @@ __global__ void k_slot_finish(int C, int SL, const int2 *__restrict__ lr, const 
     }
 }
 
+// Gradient tiles (grad_tile_bytes) from the pitched slot arrays: block t fills tile t, lane l the
+// column of cell 32 t + l; columns past the last cell hold zeros (their threads never read them)
+template <typename G>
+__global__ void k_grad_tiles(int C, int SL, const long long *__restrict__ toff, const int *__restrict__ slot_nbr,
+                             const double *__restrict__ slot_w, const double *__restrict__ slot_off,
+                             unsigned char *__restrict__ tiles)
+{
+    const int t = blockIdx.x, l = threadIdx.x, c = t * 32 + l;
+    const long long o = toff[t];
+    const int J = int((toff[t + 1] - o) / grad_tile_bytes<G>(1));
+    int *nbr = reinterpret_cast<int *>(tiles + o);
+    G *w = reinterpret_cast<G *>(tiles + o + grad_tile_nbr_bytes<G>(J));
+    G *off = reinterpret_cast<G *>(tiles + o + grad_tile_nbr_bytes<G>(J) + grad_tile_vec_bytes<G>(J));
+    for (int j = 0; j < J; j++) {
+        nbr[j * 32 + l] = c < C ? slot_nbr[(size_t)j * SL + c] : 0;
+        for (int d = 0; d < 3; d++) {
+            const size_t src = (size_t)(d * MAX_SLOTS + j) * SL + c;
+            w[(3 * j + d) * 32 + l] = c < C ? G(slot_w[src]) : G(0);
+            off[(3 * j + d) * 32 + l] = c < C ? G(slot_off[src]) : G(0);
+        }
+    }
+}
+
 // AoS [n][k] -> SoA [k][n] with an element type change
 template <typename T>
 __global__ void k_transpose(int n, int k, const double *__restrict__ aos, T *__restrict__ soa)

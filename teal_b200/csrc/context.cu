@@ -2,6 +2,7 @@
 // equations_derivative and of the Advance methods, CUDA-graph replay of steps, and the C ABI.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -151,9 +152,10 @@ static int dalloc(T **p, size_t n)
 
 struct GeomBuf {
     double *area = nullptr, *basis = nullptr, *offl = nullptr, *offr = nullptr, *corr = nullptr;
-    double *slot_w = nullptr, *slot_off = nullptr;
+    double *slot_w = nullptr, *slot_off = nullptr;  // pitched slot geometry (mesh upload only)
     float *area32 = nullptr, *basis32 = nullptr, *offl32 = nullptr, *offr32 = nullptr, *corr32 = nullptr;
-    float *slot_w32 = nullptr, *slot_off32 = nullptr;
+    unsigned char *tile64 = nullptr, *tile32 = nullptr;  // gradient tiles, FP64 and FP32 geometry
+    long long *toff64 = nullptr, *toff32 = nullptr;       // their byte offsets, [tiles + 1]
 };
 
 // workspace of the Jacobian-free Newton-GMRES implicit step
@@ -343,7 +345,7 @@ static void free_ctx(tg_ctx *c)
                     c->lr, c->slot_nbr, c->slot_face, c->slot_cnt, c->owner, c->bface_ent, c->bkind, c->bctx,
                     c->volume, c->proj, c->eps2, c->gb.area, c->gb.basis, c->gb.offl, c->gb.offr, c->gb.corr,
                     c->gb.slot_w, c->gb.slot_off, c->gb.area32, c->gb.basis32, c->gb.offl32, c->gb.offr32,
-                    c->gb.corr32, c->gb.slot_w32, c->gb.slot_off32, c->q, c->U0, c->R, c->qs, c->grad, c->G,
+                    c->gb.corr32, c->gb.tile64, c->gb.tile32, c->gb.toff64, c->gb.toff32, c->q, c->U0, c->R, c->qs, c->grad, c->G,
                     c->dtc, c->part_min, c->part_sum, c->sd, c->si, c->aos, c->rowmap, c->cell_inst,
                     c->inst_cell_off, c->piece_beg, c->inst_piece_off, c->sum_volume, c->src_avg,
                     c->send_rows, c->send_q, c->recv_q, c->send_rec, c->recv_rec};
@@ -716,8 +718,6 @@ static int alloc_geom32(tg_ctx *c)
     TRY(dalloc(&c->gb.offl32, 3 * (size_t)s.F));
     TRY(dalloc(&c->gb.offr32, 3 * (size_t)s.F));
     if (c->gb.corr) TRY(dalloc(&c->gb.corr32, 4 * (size_t)s.F));
-    TRY(dalloc(&c->gb.slot_w32, 3 * MAX_SLOTS * (size_t)s.SL));
-    TRY(dalloc(&c->gb.slot_off32, 3 * MAX_SLOTS * (size_t)s.SL));
     return TG_OK;
 }
 
@@ -853,6 +853,31 @@ static int create_ctx(MeshInput &in, const tg_equations *e, int precision, tg_ct
                 CU(cudaStreamSynchronize(st));
                 c->full_slots = true;
                 for (uint8_t k : cnt) c->full_slots = c->full_slots && k == MAX_SLOTS;
+
+                // gradient tiles: the slot geometry of every 32 cells in one block, as many slots as
+                // the block's cell with the most faces (FP64 always; FP32 for the FP32-flux form)
+                const int ntiles = (s.C + GRAD_CELLS - 1) / GRAD_CELLS;
+                std::vector<int> tj(ntiles, 0);
+                for (int i = 0; i < s.C; i++) tj[i / GRAD_CELLS] = std::max(tj[i / GRAD_CELLS], int(cnt[i]));
+                auto tiles = [&](auto zero, unsigned char **buf, long long **toff) -> int {
+                    using G = decltype(zero);
+                    std::vector<long long> off(ntiles + 1, 0);
+                    for (int t = 0; t < ntiles; t++) off[t + 1] = off[t] + grad_tile_bytes<G>(tj[t]);
+                    TRY(upload(toff, off.data(), off.size(), st));
+                    TRY(dalloc(buf, (size_t)off[ntiles]));
+                    if (ntiles > 0) {
+                        k_grad_tiles<G><<<ntiles, GRAD_CELLS, 0, st>>>(s.C, s.SL, *toff, c->slot_nbr, c->gb.slot_w,
+                                                                      c->gb.slot_off, *buf);
+                    }
+                    CU(cudaGetLastError());
+                    return TG_OK;
+                };
+                TRY(tiles(double(0), &c->gb.tile64, &c->gb.toff64));
+                if (precision == TG_PRECISION_FP32_FLUX) TRY(tiles(float(0), &c->gb.tile32, &c->gb.toff32));
+                CU(cudaStreamSynchronize(st));
+                cudaFree(c->gb.slot_w);
+                cudaFree(c->gb.slot_off);
+                c->gb.slot_w = c->gb.slot_off = nullptr;
             }
 
             // face geometry, structure of arrays
@@ -901,14 +926,12 @@ static int create_ctx(MeshInput &in, const tg_equations *e, int precision, tg_ct
             TRY(to_float(c->gb.offl, c->gb.offl32, 3 * (size_t)s.F, st));
             TRY(to_float(c->gb.offr, c->gb.offr32, 3 * (size_t)s.F, st));
             TRY(to_float(c->gb.corr, c->gb.corr32, 4 * (size_t)s.F, st));
-            TRY(to_float(c->gb.slot_w, c->gb.slot_w32, 3 * MAX_SLOTS * (size_t)s.SL, st));
-            TRY(to_float(c->gb.slot_off, c->gb.slot_off32, 3 * MAX_SLOTS * (size_t)s.SL, st));
         }
         c->g64 = Geometry<double>{c->lr,       c->gb.area,  c->gb.basis,   c->gb.offl,   c->gb.offr,   c->gb.corr,
-                                  c->slot_nbr, c->slot_face, c->slot_cnt, c->gb.slot_w, c->gb.slot_off};
+                                  c->slot_nbr, c->slot_face, c->slot_cnt, c->gb.tile64, c->gb.toff64};
         c->g32 = Geometry<float>{c->lr,         c->gb.area32, c->gb.basis32, c->gb.offl32,   c->gb.offr32,
-                                 c->gb.corr32, c->slot_nbr,  c->slot_face,  c->slot_cnt, c->gb.slot_w32,
-                                 c->gb.slot_off32};
+                                 c->gb.corr32, c->slot_nbr,  c->slot_face,  c->slot_cnt, c->gb.tile32,
+                                 c->gb.toff32};
 
         // state
         // FP64 record size in every form: the FP32-flux form's implicit step evaluates its Newton
@@ -1387,19 +1410,19 @@ static void launch_gradient_s(tg_ctx *c, const Geometry<R> &g, bool fold, const 
     R *rec = (R *)c->grad;
     switch (c->limiter) {
         case TG_LIMITER_NONE:
-            k_gradient<R, 0, true, MIXED, false><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
+            k_gradient<R, 0, true, MIXED, false><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec, c->st.error, c->wait_polls);
             break;
         case TG_LIMITER_BARTH_JESPERSEN:
             if (fold)
-                k_gradient<R, 1, true, MIXED, false><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
+                k_gradient<R, 1, true, MIXED, false><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec, c->st.error, c->wait_polls);
             else
-                k_gradient<R, 1, false, MIXED, false><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
+                k_gradient<R, 1, false, MIXED, false><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec, c->st.error, c->wait_polls);
             break;
         default:
             if (fold)
-                k_gradient<R, 2, true, MIXED, false><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
+                k_gradient<R, 2, true, MIXED, false><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec, c->st.error, c->wait_polls);
             else
-                k_gradient<R, 2, false, MIXED, false><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec);
+                k_gradient<R, 2, false, MIXED, false><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec, c->st.error, c->wait_polls);
             break;
     }
 }
@@ -1421,7 +1444,8 @@ static int run_gradient(tg_ctx *c, const double *q, int limiter_override = -1)
     bool fold = fold_psi(c);
     Launch l(c, TG_PROF_GRADIENT);
     if (is_exact(c)) {
-        GradientLaunch a{c->s, c->g64, c->eps2, q, (double *)c->grad, c->limiter, fold, !c->full_slots};
+        GradientLaunch a{c->s,  c->g64, c->eps2,         q, (double *)c->grad, c->limiter, fold, !c->full_slots,
+                         c->st.error, c->wait_polls};
         cudaError_t e = launch_gradient_exact(a, c->stream);
         c->limiter = saved;
         CU(e);
@@ -2418,6 +2442,18 @@ extern "C" int tg_layout(tg_ctx *c, const char *name, void *out, long count)
     }
     else if (!strcmp(name, "owner")) {
         src = c->owner, expect = c->num_periodic, bytes = sizeof(int);
+    }
+    else if (!strcmp(name, "tile_slots")) {
+        // slots of each gradient tile (32 cells), from the tiles' byte offsets
+        const long ntiles = (c->s.C + GRAD_CELLS - 1) / GRAD_CELLS;
+        if (count != ntiles) return fail(TG_ERR_INVALID, "layout array %s has %ld elements, not %ld", name, ntiles, count);
+        std::vector<long long> off(ntiles + 1);
+        CU(cudaMemcpyAsync(off.data(), c->gb.toff64, sizeof(long long) * (ntiles + 1), cudaMemcpyDeviceToHost,
+                           c->stream));
+        CU(cudaStreamSynchronize(c->stream));
+        int *o = static_cast<int *>(out);
+        for (long t = 0; t < ntiles; t++) o[t] = int((off[t + 1] - off[t]) / grad_tile_bytes<double>(1));
+        return TG_OK;
     }
     else {
         return fail(TG_ERR_INVALID, "unknown layout array (%s)", name);

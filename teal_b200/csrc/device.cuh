@@ -31,9 +31,30 @@ struct Geometry {
     const int *slot_nbr;  // [6][SL] neighbour state row
     const int *slot_face; // [6][SL] face index f (cell is left) or ~f (cell is right)
     const uint8_t *slot_cnt; // [C]
-    const G *slot_w;      // [3][6][SL] least-squares weight of this cell's side
-    const G *slot_off;    // [3][6][SL] face centre - cell centre (limiter)
+    // gradient tiles: the slot geometry of 32 consecutive cells in one contiguous block (see
+    // grad_tile_bytes), as many slots as the tile's cell with the most faces has
+    const unsigned char *gtile;
+    const long long *gtile_off;  // [tiles + 1] byte offset of each tile
 };
+
+// One gradient tile of J slots for element type G: neighbour rows [J][32] int, least-squares
+// weights [J][3][32] G (slot j, component d at row 3 j + d), face offsets [J][3][32] G; every part
+// a multiple of 16 bytes, so the three parts are bulk copies of their own.
+template <typename G>
+__host__ __device__ constexpr long long grad_tile_nbr_bytes(int J)
+{
+    return (long long)J * 32 * sizeof(int);
+}
+template <typename G>
+__host__ __device__ constexpr long long grad_tile_vec_bytes(int J)
+{
+    return (long long)J * 3 * 32 * sizeof(G);
+}
+template <typename G>
+__host__ __device__ constexpr long long grad_tile_bytes(int J)
+{
+    return grad_tile_nbr_bytes<G>(J) + 2 * grad_tile_vec_bytes<G>(J);
+}
 
 struct CellData {
     const double *volume;     // [C]

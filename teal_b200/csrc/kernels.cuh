@@ -4,6 +4,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "tma.cuh"
 
 namespace tg {
 
@@ -44,10 +45,13 @@ __global__ void k_boundary(Sizes s, const int2 *__restrict__ lr, const double *_
 //
 // One thread per (cell, variable): a block of 5 x 32 threads covers 32 consecutive cells, warp w
 // handling variable w, so each warp reads one contiguous row of the state. The block first stages
-// the slot geometry of its 32 cells (neighbour rows, least-squares weights, face offsets: 312 bytes
-// per cell in FP64) in shared memory with 16-byte loads; the five variable warps then read it
-// from there instead of each fetching it from L1/L2. Each gradient component is summed over the
-// cell's slots in face order, as teal's face loop adds it. Output: one gradient record per cell,
+// its 32 cells' slot geometry (neighbour rows, least-squares weights, face offsets), which the
+// mesh upload packed into one contiguous tile per 32 cells with as many slots as the tile's cell
+// with the most faces (grad_tile_bytes; no padding slots beyond that on mixed meshes), with up to
+// three bulk asynchronous copies issued by one thread and completing on an mbarrier (a bounded
+// wait: a block that gives up sets ERR_TIMEOUT in the error word and ends); the five variable
+// warps then read it from shared memory. Each gradient component is summed over the cell's slots
+// in face order, as teal's face loop adds it. Output: one gradient record per cell,
 // (gx, gy, gz, psi) per variable (grad_rec_store); FOLD multiplies psi in (Euler: only the limited
 // gradient is used), otherwise the record keeps the unlimited gradient for the viscous flux.
 constexpr int GRAD_CELLS = 32;
@@ -57,48 +61,44 @@ template <typename R, int LIM, bool FOLD, bool MIXED, bool X>
 __global__ void __launch_bounds__(GRAD_THREADS, GRAD_MINB) k_gradient(Sizes s, Geometry<R> g,
                                                            const double *__restrict__ eps2,
                                                            const double *__restrict__ q,
-                                                           R *__restrict__ rec)
+                                                           R *__restrict__ rec, int *err, int polls)
 {
     static_assert(X == kExact, "exact kernels live in the exact translation units only");
     __shared__ __align__(16) int s_nbr[MAX_SLOTS][GRAD_CELLS];
-    __shared__ int s_cnt[GRAD_CELLS];
     __shared__ __align__(16) R s_w[3 * MAX_SLOTS][GRAD_CELLS];
     __shared__ __align__(16) R s_off[(LIM != 0) ? 3 * MAX_SLOTS : 1][GRAD_CELLS];
+    __shared__ int s_cnt[GRAD_CELLS];
+    __shared__ uint64_t bar;
+    __shared__ int s_J;
     const int C = s.C;
     const int base = blockIdx.x * GRAD_CELLS;
     const int ncell = min(GRAD_CELLS, C - base);
-    const int SL = s.SL;
-    {
-        // every slot row of the block's 32 cells is 16-byte aligned and contiguous (SL is a multiple
-        // of 4 and base of 32): copy the 6 + 18 + 18 rows with 16-byte vector loads, padding slots
-        // included (zero weights and offsets, never read; on mixed meshes this beats skipping them
-        // with per-element tests: ramp gradient 0.297 vs 0.322 ms)
-        constexpr int NV = GRAD_CELLS * int(sizeof(int)) / 16;  // vectors per neighbour row
-        constexpr int RV = GRAD_CELLS * int(sizeof(R)) / 16;    // vectors per weight / offset row
-        const int live = min(GRAD_CELLS, SL - base);            // cells of the rows inside the arrays
-        for (int i = threadIdx.x; i < MAX_SLOTS * NV; i += GRAD_THREADS) {
-            const int j = i / NV, k = i % NV;
-            if (k * 16 < live * int(sizeof(int))) {
-                reinterpret_cast<uint4 *>(&s_nbr[j][0])[k] =
-                    __ldg(reinterpret_cast<const uint4 *>(g.slot_nbr + (size_t)j * SL + base) + k);
-            }
-        }
-        for (int i = threadIdx.x; i < 3 * MAX_SLOTS * RV; i += GRAD_THREADS) {
-            const int j = i / RV, k = i % RV;
-            if (k * 16 < live * int(sizeof(R))) {
-                reinterpret_cast<uint4 *>(&s_w[j][0])[k] =
-                    __ldg(reinterpret_cast<const uint4 *>(g.slot_w + (size_t)j * SL + base) + k);
-                if (LIM != 0) {
-                    reinterpret_cast<uint4 *>(&s_off[j][0])[k] =
-                        __ldg(reinterpret_cast<const uint4 *>(g.slot_off + (size_t)j * SL + base) + k);
-                }
-            }
+    if (threadIdx.x == 0) {
+        const long long t0 = __ldg(g.gtile_off + blockIdx.x);
+        const int J = int((__ldg(g.gtile_off + blockIdx.x + 1) - t0) / grad_tile_bytes<R>(1));  // slots in the tile
+        s_J = J;
+        const unsigned char *tile = g.gtile + t0;
+        const uint32_t nb = uint32_t(grad_tile_nbr_bytes<R>(J)), vb = uint32_t(grad_tile_vec_bytes<R>(J));
+        mbar_init(&bar, 1);
+        mbar_arrive_expect_tx(&bar, nb + vb + (LIM != 0 ? vb : 0u));
+        bulk_g2s(&s_nbr[0][0], tile, nb, &bar);
+        bulk_g2s(&s_w[0][0], tile + nb, vb, &bar);
+        if (LIM != 0) {
+            bulk_g2s(&s_off[0][0], tile + nb + vb, vb, &bar);
         }
     }
     if (threadIdx.x < GRAD_CELLS) {
         s_cnt[threadIdx.x] = (threadIdx.x < ncell) ? int(g.slot_cnt[base + threadIdx.x]) : 0;
     }
     __syncthreads();
+    const bool ok = mbar_wait_bounded(&bar, 0, polls);
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) {
+            atomicOr(err, ERR_TIMEOUT);
+        }
+        mbar_wait_bounded(&bar, 0, MBAR_POLLS);  // let copies still in flight land before the block exits
+        return;
+    }
 
     const int v = threadIdx.x / GRAD_CELLS;  // variable of this warp
     const int l = threadIdx.x % GRAD_CELLS;
@@ -111,9 +111,9 @@ __global__ void __launch_bounds__(GRAD_THREADS, GRAD_MINB) k_gradient(Sizes s, G
     // on meshes of hexahedra only (not MIXED) every cell has MAX_SLOTS slots: the slot tests below
     // fold away
     const int cnt = MIXED ? s_cnt[l] : MAX_SLOTS;
-    // the warp's largest slot count: slots beyond it are skipped by the whole warp (a warp of
+    // the tile's largest slot count: slots beyond it are skipped by the whole warp (a warp of
     // tetrahedra stops after 4)
-    const int jmax = MIXED ? __reduce_max_sync(__activemask(), cnt) : MAX_SLOTS;
+    const int jmax = MIXED ? s_J : MAX_SLOTS;
     double qn[MAX_SLOTS];
 #pragma unroll
     for (int j = 0; j < MAX_SLOTS; j++) {
@@ -127,9 +127,9 @@ __global__ void __launch_bounds__(GRAD_THREADS, GRAD_MINB) k_gradient(Sizes s, G
         if (j >= jmax) break;
         if (j < cnt) {
             R d = R(qn[j] - qc);
-            gx += d * s_w[0 * MAX_SLOTS + j][l];
-            gy += d * s_w[1 * MAX_SLOTS + j][l];
-            gz += d * s_w[2 * MAX_SLOTS + j][l];
+            gx += d * s_w[3 * j + 0][l];
+            gy += d * s_w[3 * j + 1][l];
+            gz += d * s_w[3 * j + 2][l];
             mn = fmin(mn, qn[j]);
             mx = fmax(mx, qn[j]);
         }
@@ -152,8 +152,7 @@ __global__ void __launch_bounds__(GRAD_THREADS, GRAD_MINB) k_gradient(Sizes s, G
         for (int j = 0; j < MAX_SLOTS; j++) {
             if (j >= jmax) break;
             if (j < cnt) {
-                R d2 = ((gx * s_off[0 * MAX_SLOTS + j][l]) + (gy * s_off[1 * MAX_SLOTS + j][l])) +
-                       (gz * s_off[2 * MAX_SLOTS + j][l]);
+                R d2 = ((gx * s_off[3 * j + 0][l]) + (gy * s_off[3 * j + 1][l])) + (gz * s_off[3 * j + 2][l]);
                 if (!is_close_zero(d2)) {
                     const R d1 = ((d2 > R(0)) ? R(mx) : R(mn)) - R(qc);
                     if (LIM == 1) {
@@ -176,8 +175,7 @@ __global__ void __launch_bounds__(GRAD_THREADS, GRAD_MINB) k_gradient(Sizes s, G
         for (int j = 0; j < MAX_SLOTS; j++) {
             if (j >= jmax) break;
             if (j < cnt) {
-                R d2 = ((gx * s_off[0 * MAX_SLOTS + j][l]) + (gy * s_off[1 * MAX_SLOTS + j][l])) +
-                       (gz * s_off[2 * MAX_SLOTS + j][l]);
+                R d2 = ((gx * s_off[3 * j + 0][l]) + (gy * s_off[3 * j + 1][l])) + (gz * s_off[3 * j + 2][l]);
                 if (!is_close_zero(d2)) {
                     const R d1 = (d2 > R(0)) ? dmx : dmn;
                     R num, den;
@@ -435,6 +433,8 @@ struct GradientLaunch {
     int limiter;  // TG_LIMITER_*
     bool fold;    // multiply psi into the record
     bool mixed;   // cells with fewer than MAX_SLOTS faces exist
+    int *err;     // device error word (a staging wait that gives up sets ERR_TIMEOUT)
+    int polls;    // limit of the staging wait (MBAR_POLLS unless a test lowers it)
 };
 
 struct CellLaunch {

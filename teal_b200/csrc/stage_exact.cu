@@ -15,18 +15,18 @@ static void gradient_m(const GradientLaunch &a, cudaStream_t st)
 {
     dim3 grid((a.s.C + GRAD_CELLS - 1) / GRAD_CELLS);
     switch (a.limiter) {
-        case 0: k_gradient<double, 0, true, MIXED, true><<<grid, GRAD_THREADS, 0, st>>>(a.s, a.g, a.eps2, a.q, a.rec); break;
+        case 0: k_gradient<double, 0, true, MIXED, true><<<grid, GRAD_THREADS, 0, st>>>(a.s, a.g, a.eps2, a.q, a.rec, a.err, a.polls); break;
         case 1:
             if (a.fold)
-                k_gradient<double, 1, true, MIXED, true><<<grid, GRAD_THREADS, 0, st>>>(a.s, a.g, a.eps2, a.q, a.rec);
+                k_gradient<double, 1, true, MIXED, true><<<grid, GRAD_THREADS, 0, st>>>(a.s, a.g, a.eps2, a.q, a.rec, a.err, a.polls);
             else
-                k_gradient<double, 1, false, MIXED, true><<<grid, GRAD_THREADS, 0, st>>>(a.s, a.g, a.eps2, a.q, a.rec);
+                k_gradient<double, 1, false, MIXED, true><<<grid, GRAD_THREADS, 0, st>>>(a.s, a.g, a.eps2, a.q, a.rec, a.err, a.polls);
             break;
         default:
             if (a.fold)
-                k_gradient<double, 2, true, MIXED, true><<<grid, GRAD_THREADS, 0, st>>>(a.s, a.g, a.eps2, a.q, a.rec);
+                k_gradient<double, 2, true, MIXED, true><<<grid, GRAD_THREADS, 0, st>>>(a.s, a.g, a.eps2, a.q, a.rec, a.err, a.polls);
             else
-                k_gradient<double, 2, false, MIXED, true><<<grid, GRAD_THREADS, 0, st>>>(a.s, a.g, a.eps2, a.q, a.rec);
+                k_gradient<double, 2, false, MIXED, true><<<grid, GRAD_THREADS, 0, st>>>(a.s, a.g, a.eps2, a.q, a.rec, a.err, a.polls);
             break;
     }
 }

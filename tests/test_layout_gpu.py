@@ -81,3 +81,25 @@ def test_layout_rejects_wrong_count():
     out = np.zeros(3, dtype=np.int32)
     st = tb.lib.tg_layout(ctx.handle, b"slot_face", ctypes.c_void_p(out.ctypes.data), 3)
     assert st == tb._lib.TG_ERR_INVALID
+
+
+def test_gradient_tiles_carry_each_tiles_largest_slot_count():
+    # the gradient kernel stages the slot geometry of 32 cells as one tile holding as many slots as
+    # the tile's cell with the most faces: no padding slots beyond that on a mixed-element mesh
+    from teal_b200 import meshes
+
+    m = tb.Mesh.from_cells(meshes.ramp_mesh(n=(10, 10, 10), seed=3))
+    e = tb.Equations.euler(m)
+    for i in range(len(e.boundary_name)):
+        e.set_boundary_condition(m.entities[m.struct.num_inner_entities + i][0], "slipwall")
+    ctx = e.context()
+    C = m.num_inner_cells
+    cnt = layout(ctx, "slot_cnt", np.uint8, C).astype(np.int32)
+    nt = (C + 31) // 32
+    tiles = layout(ctx, "tile_slots", np.int32, nt)
+    assert np.array_equal(tiles, [cnt[32 * t: 32 * t + 32].max() for t in range(nt)])
+    assert tiles.min() < 6
+    # hexahedra only: every tile has 6 slots
+    h = tb.Mesh.create((0, 0, 0), (1, 1, 1), (7, 6, 5), (1, 1, 1))
+    hctx = tb.Equations.euler(h).context()
+    assert np.all(layout(hctx, "tile_slots", np.int32, (h.num_inner_cells + 31) // 32) == 6)

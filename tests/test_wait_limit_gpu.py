@@ -1,11 +1,11 @@
 """Bounded device-side waits and loops, made to run out without a fault.
 
-The staged face kernel (the Euler form's face-flux kernel, whose geometry tile arrives by bulk copies
-completing on an mbarrier) polls the barrier a bounded number of times. tg_set_wait_limit lowers that
-bound; at 0 every block gives up at once, sets ERR_TIMEOUT in the context's error word, waits (with
-the full bound) for its own copies to land and returns. The call must report TG_ERR_TIMEOUT, and the
-same context must then evaluate the residual exactly as a fresh one does: no hang, no trap, no lost
-context.
+The staged kernels (the gradient kernel, whose tile of slot geometry arrives by bulk copies completing
+on an mbarrier, and the Euler form's face-flux kernel, whose geometry tile does) poll the barrier a
+bounded number of times. tg_set_wait_limit lowers that bound; at 0 every block gives up at once, sets
+ERR_TIMEOUT in the context's error word, waits (with the full bound) for its own copies to land and
+returns. The call must report TG_ERR_TIMEOUT, and the same context must then evaluate the residual
+exactly as a fresh one does: no hang, no trap, no lost context.
 """
 
 import numpy as np
@@ -19,14 +19,16 @@ from tests.cases import vortex
 pytestmark = pytest.mark.gpu
 
 
-def vortex_context():
+def vortex_context(physics="euler"):
     m = tb.Mesh.create((0, 0, 0), (10, 10, 0.625), (16, 16, 4), (1, 1, 1))
-    e = tb.Equations.euler(m)  # Euler: the face kernel stages its geometry (tuned.h)
+    # Euler: the face kernel stages its geometry too (tuned.h); Navier-Stokes: only the gradient
+    e = tb.Equations.euler(m) if physics == "euler" else tb.Equations.navierstokes(m)
     return m, e, tb.Context(m, e)
 
 
-def test_wait_that_runs_out_reports_timeout_and_leaves_the_context_usable():
-    m, e, ctx = vortex_context()
+@pytest.mark.parametrize("physics", ["euler", "navierstokes"])
+def test_wait_that_runs_out_reports_timeout_and_leaves_the_context_usable(physics):
+    m, e, ctx = vortex_context(physics)
     try:
         prim = vortex(m.cell_center)
         expect = ctx.derivative(prim)
