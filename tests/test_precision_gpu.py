@@ -91,6 +91,57 @@ def test_fp32_taylor_green_histories():
     assert max(ke_err) < 1e-7 and max(en_err) < 1e-7
 
 
+def test_fp32_taylor_green_48_cubed_200_steps_histories():
+    """The Taylor-Green workload at 48^3 for 200 steps (Roe, Venkatakrishnan(1), Re 1600, Ma 0.1,
+    lserk{3,3}, CFL 0.99) in the FP32-flux form against the plain FP64 form on the device (itself
+    within 1e-12 of the reference, tests/test_exact_gpu.py): the state per conserved variable and the
+    kinetic-energy and enstrophy histories, every 20 steps."""
+    n = 48
+    m = tb.Mesh.create((0, 0, 0), (2 * np.pi,) * 3, (n, n, n), (1, 1, 1))
+    e = tb.Equations.navierstokes(m)
+    e.set_convective_flux("roe")
+    e.set_limiter("venkatakrishnan", 1.0)
+    e.set_property("dynamic viscosity", 1 / 1600)
+    C = m.num_inner_cells
+    vol = np.asarray(m.cell_volume[:C])
+    prim = np.zeros((m.num_cells, 5))
+    prim[:C] = taylor_green(m.cell_center)[:C]
+    ctx = {name: tb.Context(m, e, precision=p) for name, p in (("fp64", tb.TG_PRECISION_FP64), ("fp32", FP32))}
+    grad = tb.Context(m, e, precision=tb.TG_PRECISION_FP64)
+
+    def conserved(p, gamma=1.4):
+        rho, u, pr = p[:, 0], p[:, 1:4], p[:, 4]
+        return np.column_stack([rho, rho[:, None] * u, pr / (gamma - 1) + 0.5 * rho * (u ** 2).sum(axis=1)])
+
+    try:
+        for c in ctx.values():
+            c.set_primitive(prim)
+        t = {k: 0.0 for k in ctx}
+        ke_err, en_err, state_err = [], [], []
+        for _ in range(10):
+            hist = {}
+            for k, c in ctx.items():
+                t[k], _, _ = c.run(tb.TG_ADVANCE_LSERK, 0.99, 20, context=(3, 3), time=t[k])
+                q = c.get_primitive()
+                grad.set_primitive(q)
+                hist[k] = (q[:C].copy(), diagnostics.kinetic_energy(q[:C], vol),
+                           diagnostics.enstrophy(q[:C], grad.gradient(), vol))
+            (q64, ke64, en64), (q32, ke32, en32) = hist["fp64"], hist["fp32"]
+            ke_err.append(abs(ke32 - ke64) / ke64)
+            en_err.append(abs(en32 - en64) / en64)
+            state_err.append(rel_l2(conserved(q32), conserved(q64)))
+        report("tgv 48^3 kinetic energy rel error every 20 steps", ke_err)
+        report("tgv 48^3 enstrophy rel error every 20 steps", en_err)
+        report("tgv 48^3 state rel L2 per conserved variable after 200 steps", state_err[-1])
+        # measured: kinetic energy and enstrophy within 1.9e-8 after 200 steps, growing linearly; the
+        # state within 1.1e-7 (rho w) per conserved variable
+        assert max(ke_err) < 1e-7 and max(en_err) < 1e-7
+        assert np.max(state_err[-1]) < 1e-6
+    finally:
+        for c in list(ctx.values()) + [grad]:
+            c.close()
+
+
 def test_fp32_matvec_implicit_step_converges_to_the_fp64_step():
     """The FP32-flux form's implicit Euler step evaluates its Newton residuals with the FP64 kernels
     and only the finite-difference matvec with FP32 fluxes ("FP64 Arnoldi, FP32 matvec flux"): with
