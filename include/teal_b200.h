@@ -197,11 +197,12 @@ const char *tg_last_error(void);
 int tg_set_stream(tg_ctx *ctx, void *stream);
 
 /* Failure-detection control, no counterpart in teal. Every device-side wait of this context (the
- * staged face kernel's wait for its bulk copies of face geometry) polls at most `polls` times before
- * it gives up; the call then returns TG_ERR_TIMEOUT, the blocks that gave up first let their copies
- * land, and the context stays usable. Default and maximum 16777216 polls (about a second);
- * 0 makes every such wait give up at once, which is how the timeout path is tested without a
- * fault. */
+ * gradient kernel's and the staged face kernel's waits for their bulk copies of slot and face
+ * geometry) tries at most `polls` times, each try suspending the thread for up to about a
+ * microsecond, before it gives up; the call then returns TG_ERR_TIMEOUT, the blocks that gave up
+ * first let their copies land, and the context stays usable. Default and maximum 1048576 tries
+ * (about a second); 0 makes every such wait give up at once, which is how the timeout path is
+ * tested without a fault. */
 int tg_set_wait_limit(tg_ctx *ctx, int polls);
 
 /* Resident primitive state: [num_cells][5] in teal's cell order (density, velocity, pressure).

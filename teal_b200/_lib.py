@@ -25,7 +25,7 @@ TG_VISCOUS_NONE, TG_VISCOUS_CENTRAL = 0, 1
 TG_LIMITER_NONE, TG_LIMITER_BARTH_JESPERSEN, TG_LIMITER_VENKATAKRISHNAN = 0, 1, 2
 TG_ADVANCE_EULER, TG_ADVANCE_LSERK, TG_ADVANCE_IMPLICIT_EULER = 0, 1, 2
 TG_PRECISION_FP64, TG_PRECISION_FP32_FLUX, TG_PRECISION_FP64_EXACT = 0, 1, 2
-TG_WAIT_POLLS = 1 << 24  # default (and maximum) polls of a device-side bounded wait
+TG_WAIT_POLLS = 1 << 20  # default (and maximum) tries of a device-side bounded wait
 TG_SOURCE_NONE, TG_SOURCE_BODY_FORCE, TG_SOURCE_BULK_FORCING, TG_SOURCE_DEVICE = 0, 1, 2, 3
 TG_BC_CUSTOM = 9
 TG_FUNCTION_BOUNDARY, TG_FUNCTION_SOURCE = 1, 2

@@ -35,31 +35,31 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
                  : "memory");
 }
 
-__device__ __forceinline__ bool mbar_test_wait(uint64_t *bar, uint32_t phase)
+// One try at the barrier's phase: the thread is suspended in hardware until the phase completes or
+// about `hint_ns` nanoseconds pass (mbarrier.try_wait with a suspend-time hint), so a waiting warp
+// issues one instruction per try instead of spinning on test_wait.
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t phase, uint32_t hint_ns)
 {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(done)
-        : "r"(smem_u32(bar)), "r"(phase)
+        : "r"(smem_u32(bar)), "r"(phase), "r"(hint_ns)
         : "memory");
     return done != 0;
 }
 
-// polls of a bounded wait: about a second
-constexpr int MBAR_POLLS = 1 << 24;
+// tries of a bounded wait (each suspends up to about a microsecond): about a second
+constexpr int MBAR_POLLS = 1 << 20;
 
-// Wait for the barrier's phase with an iteration limit; false when it gave up.
+// Wait for the barrier's phase with an iteration limit; false when it gave up (at once for 0).
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t phase, int polls)
 {
     for (int it = 0; it < polls; it++) {
-        if (mbar_test_wait(bar, phase)) {
+        if (mbar_try_wait(bar, phase, 1000u)) {
             return true;
-        }
-        if (it >= 32) {
-            __nanosleep(64);
         }
     }
     return false;
