@@ -44,16 +44,18 @@ __global__ void k_boundary(Sizes s, const int2 *__restrict__ lr, const double *_
 // ---- least-squares gradient + limiter (src/equations/gradient.c:7-58, limiter.c:23-113) -------
 //
 // One thread per (cell, variable): a block of 5 x 32 threads covers 32 consecutive cells, warp w
-// handling variable w, so each warp reads one contiguous row of the state. The block first stages
-// its 32 cells' slot geometry (neighbour rows, least-squares weights, face offsets), which the
-// mesh upload packed into one contiguous tile per 32 cells with as many slots as the tile's cell
-// with the most faces (grad_tile_bytes; no padding slots beyond that on mixed meshes), with up to
-// three bulk asynchronous copies issued by one thread and completing on an mbarrier (a bounded
-// wait: a block that gives up sets ERR_TIMEOUT in the error word and ends); the five variable
-// warps then read it from shared memory. Each gradient component is summed over the cell's slots
-// in face order, as teal's face loop adds it. Output: one gradient record per cell,
-// (gx, gy, gz, psi) per variable (grad_rec_store); FOLD multiplies psi in (Euler: only the limited
-// gradient is used), otherwise the record keeps the unlimited gradient for the viscous flux.
+// handling variable w, so each warp reads one contiguous row of the state. The mesh upload packed
+// the slot geometry of every 32 cells (neighbour rows, least-squares weights, face offsets) into one
+// contiguous tile with as many slots as the tile's cell with the most faces (grad_tile_bytes; no
+// padding slots beyond that on mixed meshes). One thread stages the block's tile with bulk
+// asynchronous copies completing on an mbarrier (a bounded wait: a block that gives up sets
+// ERR_TIMEOUT in the error word and ends); the five variable warps then read it from shared memory.
+// On meshes of hexahedra the threads read their neighbour rows from the tile in global memory and
+// gather the neighbours' states while the weights and offsets are still on their way. Each
+// gradient component is summed over the cell's slots in face order, as teal's face loop adds it.
+// Output: one gradient record per cell, (gx, gy, gz, psi) per variable (grad_rec_store); FOLD
+// multiplies psi in (Euler: only the limited gradient is used), otherwise the record keeps the
+// unlimited gradient for the viscous flux.
 constexpr int GRAD_CELLS = 32;
 constexpr int GRAD_THREADS = 5 * GRAD_CELLS;
 
@@ -64,32 +66,65 @@ __global__ void __launch_bounds__(GRAD_THREADS, GRAD_MINB) k_gradient(Sizes s, G
                                                            R *__restrict__ rec, int *err, int polls)
 {
     static_assert(X == kExact, "exact kernels live in the exact translation units only");
-    __shared__ __align__(16) int s_nbr[MAX_SLOTS][GRAD_CELLS];
+    __shared__ __align__(16) int s_nbr[MIXED ? MAX_SLOTS : 1][GRAD_CELLS];
     __shared__ __align__(16) R s_w[3 * MAX_SLOTS][GRAD_CELLS];
     __shared__ __align__(16) R s_off[(LIM != 0) ? 3 * MAX_SLOTS : 1][GRAD_CELLS];
-    __shared__ int s_cnt[GRAD_CELLS];
+    __shared__ int s_cnt[MIXED ? GRAD_CELLS : 1];
     __shared__ uint64_t bar;
     __shared__ int s_J;
     const int C = s.C;
     const int base = blockIdx.x * GRAD_CELLS;
     const int ncell = min(GRAD_CELLS, C - base);
-    if (threadIdx.x == 0) {
-        const long long t0 = __ldg(g.gtile_off + blockIdx.x);
-        const int J = int((__ldg(g.gtile_off + blockIdx.x + 1) - t0) / grad_tile_bytes<R>(1));  // slots in the tile
-        s_J = J;
-        const unsigned char *tile = g.gtile + t0;
-        const uint32_t nb = uint32_t(grad_tile_nbr_bytes<R>(J)), vb = uint32_t(grad_tile_vec_bytes<R>(J));
-        mbar_init(&bar, 1);
-        mbar_arrive_expect_tx(&bar, nb + vb + (LIM != 0 ? vb : 0u));
-        bulk_g2s(&s_nbr[0][0], tile, nb, &bar);
-        bulk_g2s(&s_w[0][0], tile + nb, vb, &bar);
-        if (LIM != 0) {
-            bulk_g2s(&s_off[0][0], tile + nb + vb, vb, &bar);
+    const int v = threadIdx.x / GRAD_CELLS;  // variable of this warp
+    const int l = threadIdx.x % GRAD_CELLS;
+    const int c = base + min(l, ncell - 1);
+    const double *qv = q + (size_t)v * s.N;
+    double qn[MAX_SLOTS];
+    if constexpr (MIXED) {
+        // the whole tile by bulk copies; its slot count is the tile's largest, so a warp of
+        // tetrahedra stops after 4
+        if (threadIdx.x == 0) {
+            const long long t0 = __ldg(g.gtile_off + blockIdx.x);
+            const int J = int((__ldg(g.gtile_off + blockIdx.x + 1) - t0) / grad_tile_bytes<R>(1));
+            s_J = J;
+            const unsigned char *tile = g.gtile + t0;
+            const uint32_t nb = uint32_t(grad_tile_nbr_bytes<R>(J)), vb = uint32_t(grad_tile_vec_bytes<R>(J));
+            mbar_init(&bar, 1);
+            mbar_arrive_expect_tx(&bar, nb + vb + (LIM != 0 ? vb : 0u));
+            bulk_g2s(&s_nbr[0][0], tile, nb, &bar);
+            bulk_g2s(&s_w[0][0], tile + nb, vb, &bar);
+            if (LIM != 0) {
+                bulk_g2s(&s_off[0][0], tile + nb + vb, vb, &bar);
+            }
+        }
+        if (threadIdx.x < GRAD_CELLS) {
+            s_cnt[threadIdx.x] = (threadIdx.x < ncell) ? int(g.slot_cnt[base + threadIdx.x]) : 0;
         }
     }
-    if (threadIdx.x < GRAD_CELLS) {
-        s_cnt[threadIdx.x] = (threadIdx.x < ncell) ? int(g.slot_cnt[base + threadIdx.x]) : 0;
+    else {
+        // hexahedra only: every tile has MAX_SLOTS slots (the slot tests below fold away). The weights
+        // and offsets come by bulk copies; meanwhile the threads read their neighbour rows from the
+        // tile's first part themselves and gather the neighbours' states (padding slots name the
+        // cell itself), so the gathers overlap the copies
+        const unsigned char *tile = g.gtile + (size_t)blockIdx.x * (size_t)grad_tile_bytes<R>(MAX_SLOTS);
+        constexpr uint32_t nb = uint32_t(grad_tile_nbr_bytes<R>(MAX_SLOTS));
+        constexpr uint32_t vb = uint32_t(grad_tile_vec_bytes<R>(MAX_SLOTS));
+        if (threadIdx.x == 0) {
+            mbar_init(&bar, 1);
+            mbar_arrive_expect_tx(&bar, vb + (LIM != 0 ? vb : 0u));
+            bulk_g2s(&s_w[0][0], tile + nb, vb, &bar);
+            if (LIM != 0) {
+                bulk_g2s(&s_off[0][0], tile + nb + vb, vb, &bar);
+            }
+        }
+        const int *nbr = reinterpret_cast<const int *>(tile);
+#pragma unroll
+        for (int j = 0; j < MAX_SLOTS; j++) {
+            qn[j] = __ldg(qv + __ldg(nbr + j * GRAD_CELLS + l));
+        }
     }
+    // the cell's own state does not depend on the tile: its load overlaps the copies
+    const double qc = __ldg(qv + c);
     __syncthreads();
     const bool ok = mbar_wait_bounded(&bar, 0, polls);
     if (__syncthreads_or(!ok)) {
@@ -99,26 +134,17 @@ __global__ void __launch_bounds__(GRAD_THREADS, GRAD_MINB) k_gradient(Sizes s, G
         mbar_wait_bounded(&bar, 0, MBAR_POLLS);  // let copies still in flight land before the block exits
         return;
     }
-
-    const int v = threadIdx.x / GRAD_CELLS;  // variable of this warp
-    const int l = threadIdx.x % GRAD_CELLS;
     if (l >= ncell) {
         return;
     }
-    const int c = base + l;
-    const double *qv = q + (size_t)v * s.N;
-    const double qc = __ldg(qv + c);
-    // on meshes of hexahedra only (not MIXED) every cell has MAX_SLOTS slots: the slot tests below
-    // fold away
     const int cnt = MIXED ? s_cnt[l] : MAX_SLOTS;
-    // the tile's largest slot count: slots beyond it are skipped by the whole warp (a warp of
-    // tetrahedra stops after 4)
     const int jmax = MIXED ? s_J : MAX_SLOTS;
-    double qn[MAX_SLOTS];
+    if constexpr (MIXED) {
 #pragma unroll
-    for (int j = 0; j < MAX_SLOTS; j++) {
-        if (j >= jmax) break;
-        qn[j] = __ldg(qv + ((j < cnt) ? s_nbr[j][l] : c));
+        for (int j = 0; j < MAX_SLOTS; j++) {
+            if (j >= jmax) break;
+            qn[j] = __ldg(qv + ((j < cnt) ? s_nbr[j][l] : c));
+        }
     }
     R gx = R(0), gy = R(0), gz = R(0);
     double mn = qc, mx = qc;
