@@ -306,6 +306,15 @@ __global__ void __launch_bounds__(CELL_BLOCK, CELL_MINB) k_cell(Sizes s, const i
     if (c >= C) {
         return;
     }
+    // the stage update's inputs do not depend on the face records: their loads are issued first so
+    // that their latency overlaps the record gathers
+    int inst = 0, act = 1;
+    double step = 0.0;
+    if (MODE != 0) {
+        inst = __ldg(seg.cell_inst + c);
+        act = st.active[inst];
+        step = st.step[inst];
+    }
     double r[5];
     if constexpr (X) {
         double acc[5] = {0, 0, 0, 0, 0};
@@ -396,14 +405,12 @@ __global__ void __launch_bounds__(CELL_BLOCK, CELL_MINB) k_cell(Sizes s, const i
     if (MODE == 0) {
         return;
     }
-    const int inst = __ldg(seg.cell_inst + c);
-    if (!st.active[inst]) {
+    if (!act) {
         if (last) {
             dtc[c] = DBL_MAX;
         }
         return;
     }
-    const double step = st.step[inst];
     Cons<double> u;
     u.rho = __ldg(U0 + c) + ((r[0] * alpha) * step);
     u.m.x = __ldg(U0 + C + c) + ((r[1] * alpha) * step);
