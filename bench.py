@@ -67,27 +67,33 @@ def tgv_state(center, gamma=1.4, mach=0.1):
     return out
 
 
-def stage_bytes(C, F, ns=True):
-    """Algorithmic HBM bytes of one residual stage (unique-footprint count, FP64): Euler
-    408 C + 184 F, Navier-Stokes + 88 C + 32 F."""
-    b = 408 * C + 184 * F
+def stage_bytes(C, F, ns=True, g=8):
+    """Algorithmic HBM bytes of one residual stage (unique-footprint count): Euler 408 C + 184 F,
+    Navier-Stokes + 88 C + 32 F with FP64 elements; with the FP32-flux form's 4-byte gradient and
+    geometry elements (g = 4; the state, U0 and volumes stay FP64) 288 C + 96 F, + 48 C + 16 F."""
+    # per cell: q read (gradient) 40 + gradient write 15 g + q read (face) 40 + gradient read 15 g +
+    # U0 read 40 + q write 40 + V 8; per face: cells 8 + weights 6 g + area g + basis 9 g + offsets 6 g
+    b = (168 + 30 * g) * C + (8 + 22 * g) * F
     if ns:
-        b += 88 * C + 32 * F
+        # unlimited gradient kept via psi (5 g written, 5 g read), eps^2 8; correction 4 g
+        b += (10 * g + 8) * C + 4 * g * F
     return b
 
 
-def kernel_bytes(C, F, S, NB, ns=True, fold=False):
-    """Unique bytes each hot-path kernel of one stage must move (FP64 layout of teal_b200)."""
-    grad_state = 120 + (0 if fold else 40)
+def kernel_bytes(C, F, S, NB, ns=True, fold=False, g=8, basis=3):
+    """Unique bytes each hot-path kernel of one stage must move in teal_b200's layout: g is the
+    gradient / geometry / flux-record element size (8 in FP64, 4 in the FP32-flux form), basis the
+    basis rows a face reads (3: the normal, the plain forms; 9 in the exact form)."""
+    grad_state = (15 + (0 if fold else 5)) * g
     return {
-        # q of cells and boundary ghosts, per slot: neighbour 4 + weight 24 + offset 24; counts,
+        # q of cells and boundary ghosts, per slot: neighbour 4 + weight 3 g + offset 3 g; counts,
         # eps^2; writes gradient (+ limiter factors)
-        "gradient": 40 * (C + NB) + 52 * S + 9 * C + grad_state * C,
-        # per face: cells 8, area 8, basis 72, offsets 48 (+ correction 32), G write 40; per cell:
-        # q, gradient (+ psi); ghost rows
-        "face": (176 + (32 if ns else 0)) * F + (40 + grad_state) * C + 40 * NB,
+        "gradient": 40 * (C + NB) + (4 + 6 * g) * S + 9 * C + grad_state * C,
+        # per face: cells 8, area, basis rows, offsets (+ correction), G write 5 g; per cell: q,
+        # gradient (+ psi); ghost rows
+        "face": (8 + (1 + basis + 6 + 5 + (4 if ns else 0)) * g) * F + (40 + grad_state) * C + 40 * NB,
         # slot face indices, G read once, U0, volume, q write (last stage adds R, U0, projection)
-        "cell": 4 * S + 1 * C + 40 * F + (40 + 8 + 40) * C,
+        "cell": 4 * S + 1 * C + 5 * g * F + (40 + 8 + 40) * C,
     }
 
 
@@ -872,9 +878,10 @@ def main():
     peak, peak_kind = read_peaks()
     stages = ksteps * rk[1]
     stage_ms = sum(prof[k][0] for k in ("boundary", "gradient", "face", "cell")) / stages
-    b_stage = stage_bytes(C, F, ns=ns)
+    g = 4 if args.precision == "fp32" else 8  # gradient / geometry / flux-record element size
+    b_stage = stage_bytes(C, F, ns=ns, g=g)
     achieved = b_stage / (stage_ms / 1000.0) / 1e9
-    kb = kernel_bytes(C, F, S, NB, ns=ns, fold=not ns)
+    kb = kernel_bytes(C, F, S, NB, ns=ns, fold=not ns, g=g, basis=9 if args.precision == "exact" else 3)
     kernels = {}
     for k in ("gradient", "face", "cell"):
         kms, kn = prof[k]
@@ -886,7 +893,7 @@ def main():
 
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "stage_traffic.json")
-    if ns and os.path.exists(tpath):
+    if ns and args.precision == "fp64" and os.path.exists(tpath):  # measured for the plain FP64 form
         with open(tpath) as f:
             tr = json.load(f)
         if tr.get("n") and tr.get("bytes_per_stage"):
