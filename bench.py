@@ -332,7 +332,8 @@ def mpi_sample(steps, warmup, ranks, n=128):
 
 def run_split(args, world, rank, pg):
     """The Taylor-Green 128^3 workload as ONE mesh over all ranks (strong scaling): teal's grid of
-    ranks and block split (src/mesh/create.c:10-97), each GPU a partition with a one-cell halo;
+    ranks and block split (src/mesh/create.c:10-97), or with --workload ramp the unstructured ramp
+    split by recursive coordinate bisection, each GPU a partition with a one-cell halo;
     per RK stage the states and then the gradient records of the halo cross between GPUs (NCCL
     grouped send / receive on the ranks' streams), the step minimum and the residual sums by
     all-reduce. The state after each step equals the single-mesh run's (tests/test_partition_gpu.py).
@@ -342,15 +343,27 @@ def run_split(args, world, rank, pg):
     import teal_b200 as tb
     from teal_b200 import partition as pt
 
-    n = args.n
-    lo, hi, nc = (0, 0, 0), (2 * math.pi,) * 3, (n, n, n)
+    ramp = args.workload == "ramp"
+    n = args.n or (80 if ramp else 128)
     t0 = time.perf_counter()
-    mesh = tb.Mesh.create(lo, hi, nc, (1, 1, 1))
-    eqns = tb.Equations.navierstokes(mesh)
-    configure(eqns, "tgv")
-    ranks, dims = pt.cell_ranks(mesh, lo, hi, nc, world)
+    if ramp:
+        # unstructured: split by recursive coordinate bisection (teal's ParMETIS split is not available)
+        from teal_b200 import meshes
+
+        mesh = tb.Mesh.from_cells(meshes.ramp_mesh(n=(n, n, n)))
+        eqns = tb.Equations.euler(mesh)
+        configure(eqns, "ramp")
+        ranks = pt.bisection_ranks(mesh, world)
+        dims = "recursive coordinate bisection"
+        prim = ramp_state(mesh.cell_center[: mesh.num_inner_cells])
+    else:
+        lo, hi, nc = (0, 0, 0), (2 * math.pi,) * 3, (n, n, n)
+        mesh = tb.Mesh.create(lo, hi, nc, (1, 1, 1))
+        eqns = tb.Equations.navierstokes(mesh)
+        configure(eqns, "tgv")
+        ranks, dims = pt.cell_ranks(mesh, lo, hi, nc, world)
+        prim = tgv_state(mesh.cell_center[: mesh.num_inner_cells])
     part = pt.partition(mesh, ranks)[rank]
-    prim = tgv_state(mesh.cell_center[: mesh.num_inner_cells])
     run = pt.DistributedRun(part, eqns, world)
     run.rank.set_state(prim)
     t_setup = time.perf_counter() - t0
@@ -373,8 +386,10 @@ def run_split(args, world, rank, pg):
         "metric": METRIC, "value": C * args.steps / (ms / 1000.0), "unit": "cell-updates/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": workload_name("tgv", n), "cells": C, "mesh": f"{n}^3", "global_batch": 1,
-                   "parallelism": f"one mesh split over {world} gpus (rank grid {dims}, one-cell halo)",
+        "config": {"workload": workload_name("ramp" if ramp else "tgv", n), "cells": C, "mesh": f"{n}^3",
+                   "global_batch": 1,
+                   "parallelism": f"one mesh split over {world} gpus ({dims if ramp else f'rank grid {dims}'}, "
+                                  "one-cell halo)",
                    "halo_cells_rank0": int(len(part.halo))},
         "residual": [float(x) for x in res], "setup_s": t_setup,
     }

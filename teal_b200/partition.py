@@ -15,7 +15,9 @@ orientation) and halo rows for the inner cells of other ranks on those faces. A 
 so each rank's cells see exactly the inputs they see in the single-mesh run, and the state after
 every step equals it bit for bit (the residual norm, a sum over ranks, agrees to rounding).
 
-`partition` builds the ranks' partitions and halo maps on the host from the single-process mesh;
+`cell_ranks` splits a Cartesian mesh as teal does, `bisection_ranks` any mesh by recursive
+coordinate bisection; `partition` builds the ranks' partitions and halo maps on the host from the
+single-process mesh;
 `LocalRun` drives all ranks in one process on one GPU (the halo moved by device copies; for tests);
 `DistributedRun` drives one rank per process and GPU over torch.distributed (the halo by
 send/receive, the reductions by all-reduce).
@@ -88,6 +90,35 @@ def cell_ranks(mesh, min_coord, max_coord, num_cells, size):
     ijk = np.clip(ijk, 0, np.maximum(n - 1, 0))
     coord = [_block(ijk[:, a], max(int(n[a]), 1), dims[a]) for a in range(3)]
     return ((coord[0] * dims[1] + coord[1]) * dims[2] + coord[2]).astype(np.int64), dims
+
+
+def bisection_ranks(mesh, size):
+    """Rank of every inner cell of any mesh, by recursive coordinate bisection of the cell centres:
+    a group of cells going to n ranks is split across the longest extent of its bounding box, the
+    first n // 2 ranks taking that share of its cells (cells ordered by the coordinate, ties by
+    index). For unstructured meshes, whose split in teal is ParMETIS's (src/mesh/read.c:275-292 over
+    the dual graph of src/mesh/dual.c), a library that is not available here: any split gives the
+    same results (each rank's cells sum their faces in the global order); only the balance and the
+    halo sizes differ."""
+    C = mesh.num_inner_cells
+    if not 1 <= size <= C:
+        raise ValueError(f"cannot split {C} cells over {size} ranks")
+    center = np.asarray(mesh.cell_center[:C])
+    ranks = np.empty(C, dtype=np.int64)
+    stack = [(np.arange(C), 0, size)]
+    while stack:
+        idx, r0, n = stack.pop()
+        if n == 1:
+            ranks[idx] = r0
+            continue
+        pts = center[idx]
+        axis = int(np.argmax(pts.max(axis=0) - pts.min(axis=0)))
+        nl = n // 2
+        k = len(idx) * nl // n
+        order = np.lexsort((idx, pts[:, axis]))
+        stack.append((idx[order[:k]], r0, nl))
+        stack.append((idx[order[k:]], r0 + nl, n - nl))
+    return ranks
 
 
 def periodic_owners(mesh):

@@ -44,10 +44,29 @@ def faces_of_cells(fc, num_inner_faces, C):
 @pytest.mark.parametrize("size", [2, 3, 4])
 def test_partitions_cover_the_mesh_in_global_face_order(case, size):
     mesh = tb.Mesh.create(*case)
-    s = mesh.struct
-    C = s.num_inner_cells
     ranks, dims = pt.cell_ranks(mesh, case[0], case[1], case[2], size)
     assert int(np.prod(dims)) == size and set(ranks.tolist()) == set(range(size))
+    check_partitions(mesh, ranks, size)
+
+
+@pytest.mark.parametrize("size", [2, 3, 5])
+def test_bisection_splits_an_unstructured_mesh(size):
+    # the mixed-element compression ramp (tetrahedra, prisms, pyramids, hexahedra; walls, inflow,
+    # outflow): recursive coordinate bisection, ranks within one cell of each other
+    from teal_b200 import meshes
+
+    mesh = tb.Mesh.from_cells(meshes.ramp_mesh(n=(8, 8, 8), seed=5))
+    ranks = pt.bisection_ranks(mesh, size)
+    count = np.bincount(ranks, minlength=size)
+    assert count.sum() == mesh.num_inner_cells and count.max() - count.min() <= 1
+    check_partitions(mesh, ranks, size)
+    with pytest.raises(ValueError):
+        pt.bisection_ranks(mesh, mesh.num_inner_cells + 1)
+
+
+def check_partitions(mesh, ranks, size):
+    s = mesh.struct
+    C = s.num_inner_cells
     parts = pt.partition(mesh, ranks)
     owned = np.concatenate([p.cells for p in parts])
     assert np.array_equal(np.sort(owned), np.arange(C))

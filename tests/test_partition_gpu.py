@@ -26,9 +26,10 @@ def single_steps(e, prim, steps, courant, precision):
     return out
 
 
-def check(case, e, prim, size, steps=4, courant=0.9, precision=tb.TG_PRECISION_FP64):
+def check(case, e, prim, size, steps=4, courant=0.9, precision=tb.TG_PRECISION_FP64, ranks=None):
     ref = single_steps(e, prim, steps, courant, precision)
-    ranks, _ = pt.cell_ranks(e.mesh, case[0], case[1], case[2], size)
+    if ranks is None:
+        ranks, _ = pt.cell_ranks(e.mesh, case[0], case[1], case[2], size)
     run = pt.LocalRun(pt.partition(e.mesh, ranks), e, precision)
     try:
         run.set_state(prim)
@@ -85,3 +86,22 @@ def test_partitioned_exact_form_equals_the_single_mesh():
     e.set_limiter("venkatakrishnan", 1.0)
     e.set_property("dynamic viscosity", 1 / 1600)
     check(case, e, taylor_green(m.cell_center), 2, courant=0.99, precision=tb.TG_PRECISION_FP64_EXACT)
+
+
+@pytest.mark.parametrize("size", [2, 3, 4])
+def test_bisected_compression_ramp_equals_the_single_mesh(size):
+    # the unstructured ramp (mixed elements, supersonic inflow / outflow, slip walls, AUSMD +
+    # Barth-Jespersen), split by recursive coordinate bisection
+    from teal_b200 import meshes
+
+    m = tb.Mesh.from_cells(meshes.ramp_mesh(n=(12, 12, 12), seed=2))
+    e = tb.Equations.euler(m)
+    e.set_convective_flux("ausmd")
+    e.set_limiter("minmod", 0.0)
+    inflow = (1.0, 2.5, 0.0, 0.0, 1.0 / 1.4)
+    e.set_boundary_condition("left", "supersonic inflow", inflow)
+    e.set_boundary_condition("right", "supersonic outflow")
+    for side in ("bottom", "top", "back", "front"):
+        e.set_boundary_condition(side, "slipwall")
+    check(None, e, random_state(m.num_cells, seed=7, mach=1.5), size, courant=0.9,
+          ranks=pt.bisection_ranks(m, size))
