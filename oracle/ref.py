@@ -33,6 +33,7 @@ def lib():
             "ref_set_quiet": (None, [ctypes.c_int]),
             "ref_mesh_cartesian": (vp, [dp, dp, ip, ip]),
             "ref_mesh_displace": (None, [vp, dp, ctypes.c_int]),
+            "ref_mesh_read": (vp, [ctypes.c_char_p]),
             "ref_mesh_cells": (vp, [ctypes.c_int, dp, ctypes.c_int, ctypes.c_int, ip, ip, ctypes.c_int,
                                     ctypes.POINTER(ctypes.c_char_p), ip]),
             "ref_mesh_split": (None, [vp, ctypes.c_char_p, dp, dp]),
@@ -122,6 +123,16 @@ class RefMesh:
         self.ptr = ctypes.c_void_p(L.ref_mesh_cells(coord.shape[0], _d(coord), off.size - 1, mesh["num_inner"],
                                                     off.ctypes.data_as(ip), idx.ctypes.data_as(ip), len(ents),
                                                     names, eoff.ctypes.data_as(ip)))
+        if generate:
+            L.ref_mesh_generate(self.ptr)
+        return self
+
+    @classmethod
+    def read(cls, path, generate=True):
+        """teal's mesh_read of a Gmsh 4.1 file (one rank), then mesh_generate."""
+        L = lib()
+        self = cls.__new__(cls)
+        self.ptr = ctypes.c_void_p(L.ref_mesh_read(str(path).encode()))
         if generate:
             L.ref_mesh_generate(self.ptr)
         return self

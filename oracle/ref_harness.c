@@ -98,6 +98,12 @@ void *ref_mesh_cells(int num_nodes, const double *coord, int num_cells, int num_
     return mesh;
 }
 
+/* teal's mesh_read of a Gmsh 4.1 file (mesh/read.c:901-917, one rank), before mesh_generate */
+void *ref_mesh_read(const char *fname)
+{
+    return mesh_read(fname);
+}
+
 /* apply a node displacement table (in node order at the time of the call) before generation */
 static const double *displacement = 0;
 static int displacement_num = 0;

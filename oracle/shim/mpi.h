@@ -8,7 +8,8 @@
  * messages are self-sends matched by tag in posting order, which is what the reference's periodic
  * halo exchange needs on one rank (equations/exchange.c:8-51, mesh/create.c:351-440: a periodic
  * Cartesian axis makes the rank its own neighbour). Cartesian topology: every coordinate is 0; a
- * periodic axis shifts to rank 0, a non-periodic axis to MPI_PROC_NULL.
+ * periodic axis shifts to rank 0, a non-periodic axis to MPI_PROC_NULL. Files (the reference's .msh
+ * reader): stdio reads at explicit offsets.
  *
  * shim_mpi_fork.c (linked into _ref/teal_ref_mpi): TEAL_SHIM_RANKS processes forked by MPI_Init,
  * messages through shared-memory inboxes; see that file.
@@ -47,6 +48,26 @@ typedef struct {
 #define MPI_LONG ((4 << 20) | 8)
 #define MPI_FLOAT ((5 << 20) | 4)
 #define MPI_DOUBLE ((6 << 20) | 8)
+/* fixed-width types and file offsets of the reference's .msh reader (core/parse.c, mesh/gmsh.c);
+   kinds 7 and 8 are the derived types of MPI_Type_contiguous / MPI_Type_create_resized */
+#define MPI_INT8_T ((9 << 20) | 1)
+#define MPI_INT16_T ((10 << 20) | 2)
+#define MPI_INT32_T ((11 << 20) | 4)
+#define MPI_INT64_T ((12 << 20) | 8)
+#define MPI_UINT8_T ((13 << 20) | 1)
+#define MPI_UINT16_T ((14 << 20) | 2)
+#define MPI_UINT32_T ((15 << 20) | 4)
+#define MPI_UINT64_T ((16 << 20) | 8)
+#define MPI_OFFSET ((17 << 20) | 8)
+
+/* files: one process reading with stdio (shim_mpi.c only) */
+typedef struct shim_file *MPI_File;
+typedef int MPI_Errhandler;
+#define MPI_ERRORS_ARE_FATAL 1
+#define MPI_MODE_RDONLY 2
+#define MPI_SEEK_SET 600
+#define MPI_SEEK_CUR 602
+#define MPI_SEEK_END 604
 
 #define MPI_SUM 1
 #define MPI_MIN 2
@@ -66,6 +87,22 @@ int MPI_Type_contiguous(int count, MPI_Datatype old, MPI_Datatype *type);
 int MPI_Type_create_resized(MPI_Datatype old, MPI_Aint lb, MPI_Aint extent, MPI_Datatype *type);
 int MPI_Type_commit(MPI_Datatype *type);
 int MPI_Type_free(MPI_Datatype *type);
+int MPI_Type_create_struct(int count, const int *lens, const MPI_Aint *offs, const MPI_Datatype *types,
+                           MPI_Datatype *type);
+int MPI_Type_get_name(MPI_Datatype type, char *name, int *len);
+int MPI_Get_count(const MPI_Status *status, MPI_Datatype type, int *count);
+
+int MPI_Dist_graph_create_adjacent(MPI_Comm old, int indegree, const int *sources, const int *sourceweights,
+                                   int outdegree, const int *dests, const int *destweights, MPI_Info info,
+                                   int reorder, MPI_Comm *comm);
+
+int MPI_File_open(MPI_Comm comm, const char *name, int amode, MPI_Info info, MPI_File *fh);
+int MPI_File_close(MPI_File *fh);
+int MPI_File_set_errhandler(MPI_File fh, MPI_Errhandler handler);
+int MPI_File_read_at(MPI_File fh, MPI_Offset offset, void *buf, int count, MPI_Datatype type,
+                     MPI_Status *status);
+int MPI_File_seek(MPI_File fh, MPI_Offset offset, int whence);
+int MPI_File_get_position(MPI_File fh, MPI_Offset *offset);
 
 int MPI_Allreduce(const void *send, void *recv, int count, MPI_Datatype type, MPI_Op op,
                   MPI_Comm comm);

@@ -104,3 +104,48 @@ int METIS_Free(void *ptr)
     free(ptr);
     return METIS_OK;
 }
+
+/* ---- ParMETIS on one rank (parmetis.h) ------------------------------------------------------ */
+
+#include "parmetis.h"
+
+int ParMETIS_V3_Mesh2Dual(idx_t *elmdist, idx_t *eptr, idx_t *eind, idx_t *numflag, idx_t *ncommonnodes,
+                          idx_t **xadj, idx_t **adjncy, MPI_Comm *comm)
+{
+    int size = 1;
+    MPI_Comm_size(*comm, &size);
+    if (size != 1 || elmdist[0] != 0) {
+        return METIS_ERROR;
+    }
+    idx_t ne = elmdist[1], nn = 0;
+    for (idx_t k = 0; k < eptr[ne]; k++) {
+        if (eind[k] + 1 > nn) nn = eind[k] + 1;
+    }
+    return METIS_MeshToDual(&ne, &nn, eptr, eind, ncommonnodes, numflag, xadj, adjncy);
+}
+
+int ParMETIS_V3_PartKway(idx_t *vtxdist, idx_t *xadj, idx_t *adjncy, idx_t *vwgt, idx_t *adjwgt, idx_t *wgtflag,
+                         idx_t *numflag, idx_t *ncon, idx_t *nparts, real_t *tpwgts, real_t *ubvec, idx_t *options,
+                         idx_t *edgecut, idx_t *part, MPI_Comm *comm)
+{
+    (void)xadj;
+    (void)adjncy;
+    (void)vwgt;
+    (void)adjwgt;
+    (void)wgtflag;
+    (void)numflag;
+    (void)ncon;
+    (void)tpwgts;
+    (void)ubvec;
+    (void)options;
+    int size = 1;
+    MPI_Comm_size(*comm, &size);
+    if (size != 1 || *nparts != 1) {
+        return METIS_ERROR;
+    }
+    for (idx_t i = 0; i < vtxdist[1] - vtxdist[0]; i++) {
+        part[i] = 0;
+    }
+    *edgecut = 0;
+    return METIS_OK;
+}

@@ -1,7 +1,7 @@
 /*
  * Single-rank MPI stand-in (see mpi.h). Test infrastructure only.
  */
-#define _POSIX_C_SOURCE 199309L
+#define _POSIX_C_SOURCE 200809L
 #include "mpi.h"
 
 #include <stdio.h>
@@ -404,5 +404,128 @@ int MPI_Cart_shift(MPI_Comm comm, int direction, int disp, int *source, int *des
     int nbr = cart_periods[direction] ? 0 : MPI_PROC_NULL;
     *source = nbr;
     *dest = nbr;
+    return MPI_SUCCESS;
+}
+
+/* ---- derived types, names and counts ---------------------------------------------------------- */
+
+int MPI_Type_create_struct(int count, const int *lens, const MPI_Aint *offs, const MPI_Datatype *types,
+                           MPI_Datatype *type)
+{
+    long end = 0;
+    for (int i = 0; i < count; i++) {
+        long e = offs[i] + (long)lens[i] * type_bytes(types[i]);
+        if (e > end) end = e;
+    }
+    *type = (18 << 20) | (int)end;
+    return MPI_SUCCESS;
+}
+
+int MPI_Type_get_name(MPI_Datatype type, char *name, int *len)
+{
+    static const char *names[] = {"?",         "MPI_CHAR",     "MPI_INT",      "MPI_UINT",     "MPI_LONG",
+                                  "MPI_FLOAT", "MPI_DOUBLE",   "contiguous",   "resized",      "MPI_INT8_T",
+                                  "MPI_INT16_T", "MPI_INT32_T", "MPI_INT64_T", "MPI_UINT8_T", "MPI_UINT16_T",
+                                  "MPI_UINT32_T", "MPI_UINT64_T", "MPI_OFFSET", "struct"};
+    int kind = type >> 20;
+    const char *n = (kind >= 0 && kind < (int)(sizeof(names) / sizeof(*names))) ? names[kind] : "?";
+    *len = (int)strlen(n);
+    memcpy(name, n, (size_t)*len + 1);
+    return MPI_SUCCESS;
+}
+
+/* the status of a file read carries the bytes read */
+int MPI_Get_count(const MPI_Status *status, MPI_Datatype type, int *count)
+{
+    *count = status->count / type_bytes(type);
+    return MPI_SUCCESS;
+}
+
+/* one rank: the neighbourhood graph has no edges to anyone else */
+int MPI_Dist_graph_create_adjacent(MPI_Comm old, int indegree, const int *sources, const int *sourceweights,
+                                   int outdegree, const int *dests, const int *destweights, MPI_Info info,
+                                   int reorder, MPI_Comm *comm)
+{
+    (void)sources;
+    (void)sourceweights;
+    (void)dests;
+    (void)destweights;
+    (void)info;
+    (void)reorder;
+    for (int i = 0; i < indegree; i++) {
+        if (sources[i] != 0) return 1;
+    }
+    for (int i = 0; i < outdegree; i++) {
+        if (dests[i] != 0) return 1;
+    }
+    *comm = old;
+    return MPI_SUCCESS;
+}
+
+/* ---- files: stdio reads at explicit offsets ------------------------------------------------- */
+
+struct shim_file {
+    FILE *f;
+    MPI_Offset pos;
+};
+
+int MPI_File_open(MPI_Comm comm, const char *name, int amode, MPI_Info info, MPI_File *fh)
+{
+    (void)comm;
+    (void)info;
+    if (amode != MPI_MODE_RDONLY) return 1;
+    FILE *f = fopen(name, "rb");
+    if (!f) return 1;
+    struct shim_file *h = calloc(1, sizeof(*h));
+    h->f = f;
+    *fh = h;
+    return MPI_SUCCESS;
+}
+
+int MPI_File_close(MPI_File *fh)
+{
+    if (*fh) {
+        fclose((*fh)->f);
+        free(*fh);
+        *fh = 0;
+    }
+    return MPI_SUCCESS;
+}
+
+int MPI_File_set_errhandler(MPI_File fh, MPI_Errhandler handler)
+{
+    (void)fh;
+    (void)handler;
+    return MPI_SUCCESS;
+}
+
+int MPI_File_read_at(MPI_File fh, MPI_Offset offset, void *buf, int count, MPI_Datatype type,
+                     MPI_Status *status)
+{
+    size_t bytes = (size_t)count * (size_t)type_bytes(type);
+    size_t got = 0;
+    if (fseeko(fh->f, (off_t)offset, SEEK_SET) == 0) {
+        got = fread(buf, 1, bytes, fh->f);
+    }
+    if (status) {
+        status->MPI_SOURCE = 0;
+        status->MPI_TAG = 0;
+        status->MPI_ERROR = MPI_SUCCESS;
+        status->count = (int)got;
+    }
+    return MPI_SUCCESS;
+}
+
+int MPI_File_seek(MPI_File fh, MPI_Offset offset, int whence)
+{
+    if (whence == MPI_SEEK_SET) fh->pos = offset;
+    else if (whence == MPI_SEEK_CUR) fh->pos += offset;
+    else return 1;
+    return MPI_SUCCESS;
+}
+
+int MPI_File_get_position(MPI_File fh, MPI_Offset *offset)
+{
+    *offset = fh->pos;
     return MPI_SUCCESS;
 }
