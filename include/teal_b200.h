@@ -337,6 +337,23 @@ int tg_host_mesh_cartesian(const double *min_coord, const double *max_coord, con
 int tg_host_mesh_cells(int num_nodes, const double *coord, int num_cells, int num_inner_cells,
                        const int *node_off, const int *node_idx, int num_entities,
                        const char *const *entity_names, const int *entity_cell_off, tg_host_mesh **mesh);
+/* The same with periodic entities, as mesh_read leaves a mesh with periodic links on one process
+ * (src/mesh/read.c:294-372): after the boundary face cells [num_inner_cells, off_boundary_cells)
+ * the periodic face cells [off_boundary_cells, num_cells), one entity per periodic surface after
+ * the boundary entities (off_boundary_entities), each with its rotation [9] (rows) and translation
+ * [3] (entity_rotation [num_entities][9], entity_translation [num_entities][3]: owner side to ghost
+ * side, read.c via gmsh.c:784-817), and the self-exchange of the periodic ghosts: num_neighbors
+ * entries of (receive tag, send tag) (neighbor_tag [num_neighbors][2]), ghost row ranges
+ * (neighbor_recv_off [num_neighbors + 1], from off_boundary_cells) and the inner cells each entry
+ * sends (neighbor_send_off [num_neighbors + 1], neighbor_send_idx), matched by tag as
+ * equations/exchange.c:8-51 does on one rank. */
+int tg_host_mesh_cells_periodic(int num_nodes, const double *coord, int num_cells, int num_inner_cells,
+                                int off_boundary_cells, const int *node_off, const int *node_idx, int num_entities,
+                                int off_boundary_entities, const char *const *entity_names,
+                                const int *entity_cell_off, const double *entity_rotation,
+                                const double *entity_translation, int num_neighbors, const int *neighbor_tag,
+                                const int *neighbor_recv_off, const int *neighbor_send_off,
+                                const int *neighbor_send_idx, tg_host_mesh **mesh);
 /* View of the generated arrays (pointers stay owned by the host mesh). */
 int tg_host_mesh_view(const tg_host_mesh *mesh, tg_mesh *view);
 /* Entity names (teal's: "domain", "left", "right", ...) and their cell ranges. */

@@ -109,19 +109,68 @@ int METIS_Free(void *ptr)
 
 #include "parmetis.h"
 
+/* ParMETIS' dual graph joins two elements when they share at least `ncommonnodes` nodes (its
+ * documented rule; unlike METIS_MeshToDual there is no rule for elements sharing all but one of
+ * their nodes). On one rank the order of each element's neighbours does not reach the reader's
+ * result; here it is the order of first encounter, as above. */
 int ParMETIS_V3_Mesh2Dual(idx_t *elmdist, idx_t *eptr, idx_t *eind, idx_t *numflag, idx_t *ncommonnodes,
-                          idx_t **xadj, idx_t **adjncy, MPI_Comm *comm)
+                          idx_t **xadj_out, idx_t **adjncy_out, MPI_Comm *comm)
 {
     int size = 1;
     MPI_Comm_size(*comm, &size);
-    if (size != 1 || elmdist[0] != 0) {
+    if (size != 1 || elmdist[0] != 0 || *numflag != 0) {
         return METIS_ERROR;
     }
-    idx_t ne = elmdist[1], nn = 0;
+    idx_t ne = elmdist[1], nn = 0, ncommon = *ncommonnodes;
     for (idx_t k = 0; k < eptr[ne]; k++) {
         if (eind[k] + 1 > nn) nn = eind[k] + 1;
     }
-    return METIS_MeshToDual(&ne, &nn, eptr, eind, ncommonnodes, numflag, xadj, adjncy);
+    idx_t *nptr = calloc((size_t)nn + 1, sizeof(idx_t));
+    for (idx_t k = 0; k < eptr[ne]; k++) nptr[eind[k] + 1] += 1;
+    for (idx_t n = 0; n < nn; n++) nptr[n + 1] += nptr[n];
+    idx_t *nind = malloc((size_t)(nptr[nn] > 0 ? nptr[nn] : 1) * sizeof(idx_t));
+    idx_t *fill = calloc((size_t)nn + 1, sizeof(idx_t));
+    for (idx_t e = 0; e < ne; e++) {
+        for (idx_t k = eptr[e]; k < eptr[e + 1]; k++) nind[nptr[eind[k]] + fill[eind[k]]++] = e;
+    }
+    idx_t *count = calloc((size_t)(ne > 0 ? ne : 1), sizeof(idx_t));
+    idx_t *seen = malloc((size_t)(ne > 0 ? ne : 1) * sizeof(idx_t));
+    idx_t *xadj = malloc(((size_t)ne + 1) * sizeof(idx_t));
+    size_t cap = 16, len = 0;
+    idx_t *adjncy = malloc(cap * sizeof(idx_t));
+    xadj[0] = 0;
+    for (idx_t e = 0; e < ne; e++) {
+        idx_t nseen = 0;
+        for (idx_t k = eptr[e]; k < eptr[e + 1]; k++) {
+            idx_t n = eind[k];
+            for (idx_t m = nptr[n]; m < nptr[n + 1]; m++) {
+                idx_t f = nind[m];
+                if (f == e) continue;
+                if (count[f] == 0) seen[nseen++] = f;
+                count[f] += 1;
+            }
+        }
+        for (idx_t q = 0; q < nseen; q++) {
+            idx_t f = seen[q];
+            if (count[f] >= ncommon) {
+                if (len == cap) {
+                    cap *= 2;
+                    adjncy = realloc(adjncy, cap * sizeof(idx_t));
+                }
+                adjncy[len++] = f;
+            }
+            count[f] = 0;
+        }
+        xadj[e + 1] = (idx_t)len;
+    }
+    free(nptr);
+    free(nind);
+    free(fill);
+    free(count);
+    free(seen);
+    *xadj_out = xadj;
+    *adjncy_out = adjncy;
+    return METIS_OK;
 }
 
 int ParMETIS_V3_PartKway(idx_t *vtxdist, idx_t *xadj, idx_t *adjncy, idx_t *vwgt, idx_t *adjwgt, idx_t *wgtflag,

@@ -899,20 +899,36 @@ extern "C" int tg_host_mesh_cartesian(const double *min_coord, const double *max
     return TG_OK;
 }
 
-// One process's mesh given as teal holds it before generation (mesh_read's output, src/mesh/read.c,
-// without partitioning or neighbours): nodes, cells as node lists (inner cells with 4, 5, 6 or 8
-// nodes in Gmsh order, then boundary face cells with 3 or 4 nodes), and entities as cell ranges.
-extern "C" int tg_host_mesh_cells(int num_nodes, const double *coord, int num_cells, int num_inner_cells,
-                                  const int *node_off, const int *node_idx, int num_entities,
-                                  const char *const *entity_names, const int *entity_cell_off,
-                                  tg_host_mesh **out)
+// One process's mesh given as teal holds it before generation (mesh_read's output, src/mesh/read.c):
+// nodes, cells as node lists (inner cells with 4, 5, 6 or 8 nodes in Gmsh order, then boundary face
+// cells with 3 or 4 nodes, then periodic face cells with 3 or 4 nodes), entities as cell ranges (inner,
+// boundary, periodic), the periodic entities' rotation and translation (from the owner's side to the
+// ghost's) and the periodic self-exchange (neighbour tags, receive and send offsets, sent cells).
+extern "C" int tg_host_mesh_cells_periodic(int num_nodes, const double *coord, int num_cells, int num_inner_cells,
+                                           int off_boundary_cells, const int *node_off, const int *node_idx,
+                                           int num_entities, int off_boundary_entities,
+                                           const char *const *entity_names, const int *entity_cell_off,
+                                           const double *entity_rotation, const double *entity_translation,
+                                           int num_neighbors, const int *neighbor_tag, const int *neighbor_recv_off,
+                                           const int *neighbor_send_off, const int *neighbor_send_idx,
+                                           tg_host_mesh **out)
 {
     if (!coord || !node_off || !node_idx || !entity_names || !entity_cell_off || !out) return TG_ERR_INVALID;
     *out = nullptr;
-    if (num_nodes <= 0 || num_inner_cells <= 0 || num_cells < num_inner_cells || num_entities < 1) {
+    if (num_nodes <= 0 || num_inner_cells <= 0 || off_boundary_cells < num_inner_cells ||
+        num_cells < off_boundary_cells || num_entities < 1 || num_neighbors < 0) {
         return TG_ERR_INVALID;
     }
     if (node_off[0] != 0 || entity_cell_off[0] != 0 || entity_cell_off[num_entities] != num_cells) {
+        return TG_ERR_INVALID;
+    }
+    if (off_boundary_entities < 1 || off_boundary_entities > num_entities ||
+        entity_cell_off[off_boundary_entities] != off_boundary_cells) {
+        return TG_ERR_INVALID;
+    }
+    if ((num_cells > off_boundary_cells || num_neighbors > 0) &&
+        (!entity_rotation || !entity_translation || !neighbor_tag || !neighbor_recv_off || !neighbor_send_off ||
+         !neighbor_send_idx)) {
         return TG_ERR_INVALID;
     }
     for (int i = 0; i < num_cells; i++) {
@@ -929,24 +945,54 @@ extern "C" int tg_host_mesh_cells(int num_nodes, const double *coord, int num_ce
         if (entity_cell_off[e + 1] <= num_inner_cells) num_inner_entities = e + 1;
     }
     if (entity_cell_off[num_inner_entities] != num_inner_cells) return TG_ERR_INVALID;
+    if (num_neighbors > 0) {
+        if (neighbor_recv_off[0] != off_boundary_cells || neighbor_recv_off[num_neighbors] != num_cells ||
+            neighbor_send_off[0] != 0) {
+            return TG_ERR_INVALID;
+        }
+        for (int k = 0; k < num_neighbors; k++) {
+            if (neighbor_recv_off[k + 1] < neighbor_recv_off[k] || neighbor_send_off[k + 1] < neighbor_send_off[k]) {
+                return TG_ERR_INVALID;
+            }
+        }
+        for (int j = 0; j < neighbor_send_off[num_neighbors]; j++) {
+            if (neighbor_send_idx[j] < 0 || neighbor_send_idx[j] >= num_inner_cells) return TG_ERR_INVALID;
+        }
+    }
+    else if (num_cells != off_boundary_cells) {
+        return TG_ERR_INVALID;
+    }
     tg_host_mesh *m = new tg_host_mesh();
     m->coord.resize(num_nodes);
     for (int v = 0; v < num_nodes; v++) m->coord[v] = {coord[3 * v], coord[3 * v + 1], coord[3 * v + 2]};
     m->num_cells = num_cells;
     m->num_inner = num_inner_cells;
-    m->off_boundary = m->off_periodic = num_cells;
+    m->off_boundary = off_boundary_cells;
+    m->off_periodic = num_cells;
     m->node_off.assign(node_off, node_off + num_cells + 1);
     m->node_idx.assign(node_idx, node_idx + node_off[num_cells]);
     m->num_inner_entities = num_inner_entities;
-    m->off_boundary_entities = num_entities;
+    m->off_boundary_entities = off_boundary_entities;
     for (int e = 0; e < num_entities; e++) {
         Entity en{};
         en.name = entity_names[e];
+        if (entity_rotation) memcpy(en.rotation, entity_rotation + 9 * (size_t)e, sizeof(en.rotation));
+        if (entity_translation) {
+            en.translation = {entity_translation[3 * e], entity_translation[3 * e + 1], entity_translation[3 * e + 2]};
+        }
         m->entities.push_back(en);
     }
     m->ent_cell_off.assign(entity_cell_off, entity_cell_off + num_entities + 1);
-    m->recv_off.assign(1, num_cells);
-    m->send_off.assign(1, 0);
+    if (num_neighbors > 0) {
+        m->tag.assign(neighbor_tag, neighbor_tag + 2 * (size_t)num_neighbors);
+        m->recv_off.assign(neighbor_recv_off, neighbor_recv_off + num_neighbors + 1);
+        m->send_off.assign(neighbor_send_off, neighbor_send_off + num_neighbors + 1);
+        m->send_idx.assign(neighbor_send_idx, neighbor_send_idx + neighbor_send_off[num_neighbors]);
+    }
+    else {
+        m->recv_off.assign(1, num_cells);
+        m->send_off.assign(1, 0);
+    }
     int rc = generate(*m);
     if (rc != TG_OK) {
         delete m;
@@ -954,6 +1000,17 @@ extern "C" int tg_host_mesh_cells(int num_nodes, const double *coord, int num_ce
     }
     *out = m;
     return TG_OK;
+}
+
+// The same without periodic entities: inner cells, then boundary face cells
+extern "C" int tg_host_mesh_cells(int num_nodes, const double *coord, int num_cells, int num_inner_cells,
+                                  const int *node_off, const int *node_idx, int num_entities,
+                                  const char *const *entity_names, const int *entity_cell_off,
+                                  tg_host_mesh **out)
+{
+    return tg_host_mesh_cells_periodic(num_nodes, coord, num_cells, num_inner_cells, num_cells, node_off, node_idx,
+                                       num_entities, num_entities, entity_names, entity_cell_off, nullptr, nullptr, 0,
+                                       nullptr, nullptr, nullptr, nullptr, out);
 }
 
 extern "C" int tg_host_mesh_view(const tg_host_mesh *m, tg_mesh *v)
