@@ -353,7 +353,16 @@ int tg_host_mesh_cells_periodic(int num_nodes, const double *coord, int num_cell
                                 const int *entity_cell_off, const double *entity_rotation,
                                 const double *entity_translation, int num_neighbors, const int *neighbor_tag,
                                 const int *neighbor_recv_off, const int *neighbor_send_off,
-                                const int *neighbor_send_idx, tg_host_mesh **mesh);
+                                const int *neighbor_send_idx, int num_splits, const char *const *split_entity,
+                                const double *split_root, const double *split_normal, tg_host_mesh **mesh);
+/* tg_host_mesh_cartesian with teal's mesh_split (src/mesh/split.c) applied before generation, in
+ * order: split i cuts the inner or boundary entity split_entity[i] by the plane through
+ * split_root[i][3] with normal split_normal[i][3] into "<name>-a" (cell node means on the
+ * non-positive side) and "<name>-b". tg_host_mesh_cells_periodic takes the same split lists. */
+int tg_host_mesh_cartesian_split(const double *min_coord, const double *max_coord, const int *num_cells,
+                                 const int *periodic, const double *displacement, int num_splits,
+                                 const char *const *split_entity, const double *split_root,
+                                 const double *split_normal, tg_host_mesh **mesh);
 /* View of the generated arrays (pointers stay owned by the host mesh). */
 int tg_host_mesh_view(const tg_host_mesh *mesh, tg_mesh *view);
 /* Entity names (teal's: "domain", "left", "right", ...) and their cell ranges. */

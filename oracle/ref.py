@@ -241,8 +241,10 @@ class RefEquations:
     def set_boundary_condition(self, entity, name, context=None):
         ctx = None
         if context is not None:
-            self._ctx_keep = np.ascontiguousarray(context, dtype=np.float64)
-            ctx = _d(self._ctx_keep)
+            # teal keeps the pointer (equations/set.c:92): one live array per entity
+            keep = self.__dict__.setdefault("_ctx_keep", {})
+            keep[entity] = np.ascontiguousarray(context, dtype=np.float64)
+            ctx = _d(keep[entity])
         lib().ref_set_boundary(self.ptr, entity.encode(), name.encode(), ctx)
 
     @property

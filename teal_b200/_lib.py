@@ -161,6 +161,9 @@ SIGNATURES = [
     ("tg_host_mesh_cells_periodic", ctypes.c_int,
      [ctypes.c_int, _dbl_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _int_p, _int_p, ctypes.c_int, ctypes.c_int,
       ctypes.POINTER(ctypes.c_char_p), _int_p, _dbl_p, _dbl_p, ctypes.c_int, _int_p, _int_p, _int_p, _int_p,
+      ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), _dbl_p, _dbl_p, ctypes.POINTER(_vp)]),
+    ("tg_host_mesh_cartesian_split", ctypes.c_int,
+     [_dbl_p, _dbl_p, _int_p, _int_p, _dbl_p, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), _dbl_p, _dbl_p,
       ctypes.POINTER(_vp)]),
     ("tg_host_mesh_view", ctypes.c_int, [_vp, ctypes.POINTER(TgMesh)]),
     ("tg_host_mesh_entity", ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), _int_p,

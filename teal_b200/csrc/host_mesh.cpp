@@ -881,15 +881,88 @@ int generate(tg_host_mesh &m)
     return geometry(m);
 }
 
+// mesh_split before generation (src/mesh/split.c:20-94): the cells of an inner or boundary entity
+// whose node mean lies on the plane's non-positive side come first (in order), the others after
+// them; the entity becomes "<name>-a" and "<name>-b", the second a copy of the first's transform;
+// cells the periodic self-exchange sends are renumbered with them (reorder.c:123-131)
+int split(tg_host_mesh &m, const char *name, const double *root_in, const double *normal_in)
+{
+    if (!name || !root_in || !normal_in) return TG_ERR_INVALID;
+    int e = -1;
+    for (int i = 0; i < m.off_boundary_entities; i++) {
+        if (m.entities[i].name == name) {
+            e = i;
+            break;
+        }
+    }
+    if (e < 0) return TG_ERR_INVALID;
+    const Vec root = {root_in[0], root_in[1], root_in[2]}, normal = {normal_in[0], normal_in[1], normal_in[2]};
+    const int beg = m.ent_cell_off[e], end = m.ent_cell_off[e + 1], n = end - beg;
+    std::vector<int> map(n);
+    int offset = 0;
+    for (int i = 0; i < n; i++) {
+        const int c = beg + i;
+        Vec mean = {0, 0, 0};
+        for (int j = m.node_off[c]; j < m.node_off[c + 1]; j++) mean = vadd(mean, m.coord[m.node_idx[j]]);
+        mean = vdiv(mean, (double)(m.node_off[c + 1] - m.node_off[c]));
+        map[i] = vdot(vsub(mean, root), normal) <= 0;
+        offset += map[i];
+    }
+    int lhs = 0, rhs = 0;
+    for (int i = 0; i < n; i++) map[i] = map[i] ? lhs++ : (offset + rhs++);
+    // the entity's node lists in their new order
+    std::vector<std::vector<int>> cells(n);
+    for (int i = 0; i < n; i++) {
+        const int c = beg + i;
+        cells[map[i]].assign(m.node_idx.begin() + m.node_off[c], m.node_idx.begin() + m.node_off[c + 1]);
+    }
+    std::vector<int> idx(m.node_idx.begin(), m.node_idx.begin() + m.node_off[beg]);
+    std::vector<int> off(m.node_off.begin(), m.node_off.begin() + beg + 1);
+    for (int i = 0; i < n; i++) {
+        idx.insert(idx.end(), cells[i].begin(), cells[i].end());
+        off.push_back((int)idx.size());
+    }
+    for (int c = end; c < m.num_cells; c++) {
+        idx.insert(idx.end(), m.node_idx.begin() + m.node_off[c], m.node_idx.begin() + m.node_off[c + 1]);
+        off.push_back((int)idx.size());
+    }
+    m.node_idx.swap(idx);
+    m.node_off.swap(off);
+    for (int &k : m.send_idx) {
+        if (beg <= k && k < end) k = beg + map[k - beg];
+    }
+    Entity copy = m.entities[e];
+    m.entities[e].name += "-a";
+    copy.name += "-b";
+    m.entities.insert(m.entities.begin() + e + 1, copy);
+    m.ent_cell_off.insert(m.ent_cell_off.begin() + e + 1, beg + offset);
+    if (e < m.num_inner_entities) m.num_inner_entities += 1;
+    m.off_boundary_entities += 1;  // the exchange tags stay as they are: they only pair entries
+    return TG_OK;
+}
+
+int split_all(tg_host_mesh &m, int num_splits, const char *const *entity, const double *root, const double *normal)
+{
+    if (num_splits < 0 || (num_splits > 0 && (!entity || !root || !normal))) return TG_ERR_INVALID;
+    for (int i = 0; i < num_splits; i++) {
+        int rc = split(m, entity[i], root + 3 * i, normal + 3 * i);
+        if (rc != TG_OK) return rc;
+    }
+    return TG_OK;
+}
+
 }  // namespace
 
-extern "C" int tg_host_mesh_cartesian(const double *min_coord, const double *max_coord, const int *num_cells,
-                                      const int *periodic, const double *displacement, tg_host_mesh **out)
+extern "C" int tg_host_mesh_cartesian_split(const double *min_coord, const double *max_coord, const int *num_cells,
+                                            const int *periodic, const double *displacement, int num_splits,
+                                            const char *const *split_entity, const double *split_root,
+                                            const double *split_normal, tg_host_mesh **out)
 {
     if (!min_coord || !max_coord || !num_cells || !periodic || !out) return TG_ERR_INVALID;
     *out = nullptr;
     tg_host_mesh *m = new tg_host_mesh();
     int rc = cartesian(*m, min_coord, max_coord, num_cells, periodic, displacement);
+    if (rc == TG_OK) rc = split_all(*m, num_splits, split_entity, split_root, split_normal);
     if (rc == TG_OK) rc = generate(*m);
     if (rc != TG_OK) {
         delete m;
@@ -897,6 +970,13 @@ extern "C" int tg_host_mesh_cartesian(const double *min_coord, const double *max
     }
     *out = m;
     return TG_OK;
+}
+
+extern "C" int tg_host_mesh_cartesian(const double *min_coord, const double *max_coord, const int *num_cells,
+                                      const int *periodic, const double *displacement, tg_host_mesh **out)
+{
+    return tg_host_mesh_cartesian_split(min_coord, max_coord, num_cells, periodic, displacement, 0, nullptr, nullptr,
+                                        nullptr, out);
 }
 
 // One process's mesh given as teal holds it before generation (mesh_read's output, src/mesh/read.c):
@@ -911,6 +991,8 @@ extern "C" int tg_host_mesh_cells_periodic(int num_nodes, const double *coord, i
                                            const double *entity_rotation, const double *entity_translation,
                                            int num_neighbors, const int *neighbor_tag, const int *neighbor_recv_off,
                                            const int *neighbor_send_off, const int *neighbor_send_idx,
+                                           int num_splits, const char *const *split_entity,
+                                           const double *split_root, const double *split_normal,
                                            tg_host_mesh **out)
 {
     if (!coord || !node_off || !node_idx || !entity_names || !entity_cell_off || !out) return TG_ERR_INVALID;
@@ -993,7 +1075,8 @@ extern "C" int tg_host_mesh_cells_periodic(int num_nodes, const double *coord, i
         m->recv_off.assign(1, num_cells);
         m->send_off.assign(1, 0);
     }
-    int rc = generate(*m);
+    int rc = split_all(*m, num_splits, split_entity, split_root, split_normal);
+    if (rc == TG_OK) rc = generate(*m);
     if (rc != TG_OK) {
         delete m;
         return rc;
@@ -1010,7 +1093,7 @@ extern "C" int tg_host_mesh_cells(int num_nodes, const double *coord, int num_ce
 {
     return tg_host_mesh_cells_periodic(num_nodes, coord, num_cells, num_inner_cells, num_cells, node_off, node_idx,
                                        num_entities, num_entities, entity_names, entity_cell_off, nullptr, nullptr, 0,
-                                       nullptr, nullptr, nullptr, nullptr, out);
+                                       nullptr, nullptr, nullptr, nullptr, 0, nullptr, nullptr, nullptr, out);
 }
 
 extern "C" int tg_host_mesh_view(const tg_host_mesh *m, tg_mesh *v)
