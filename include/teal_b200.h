@@ -233,6 +233,18 @@ int tg_residual(tg_ctx *ctx, const double *derivative, double *residual);
 int tg_advance(tg_ctx *ctx, int method, const void *context, double courant, double *time,
                double max_step, double *residual, double *step0);
 
+/* tg_set_primitive(prim_in) + tg_advance + tg_get_primitive(prim_out) as one call, with the
+ * download overlapped with the step's last stage (explicit methods on a single mesh, prim_out in
+ * pinned or registered host memory): that stage's face fluxes and cell updates run in chunks of
+ * cells and each chunk's rows are copied to the host as soon as they are final. The results are
+ * the bits of the three calls in sequence. prim_in (its first num_inner rows of 5) or null (the
+ * resident state), prim_out [num_cells][5] or null. Pageable prim_out, the implicit method and
+ * partitions run the three calls in sequence. The first chunked call builds the context's chunk plan
+ * (one host pass over the faces). This is the work of teal's Advance (src/simulation.h:6-7) on
+ * eqns->primitive.data, which the drop-in methods (tg_teal_*) call. */
+int tg_advance_host(tg_ctx *ctx, int method, const void *context, double courant, double *time,
+                    double max_step, const double *prim_in, double *prim_out, double *residual, double *step0);
+
 /* Unclipped step (step0) of the last step taken by `instance` (0 for a single mesh), as teal's run
  * loop prints it (simulation/run.c:95-96). */
 int tg_last_step(tg_ctx *ctx, int instance, double *step0);
@@ -305,9 +317,11 @@ int tg_lserk_alpha(int order, int stages, double *alpha);
 
 /* ---- drop-in Advance methods with teal's signature (src/simulation.h:6-7) ----------------------- */
 
-/* Bind a teal `Equations *` (used only as a lookup key) to a context and to the host primitive
- * array teal reads (`eqns->primitive.data`, [num_cells][5]). The host state is uploaded now;
- * after every drop-in Advance call the new state is copied back into that array. */
+/* Bind a teal `Equations *` (used only as a lookup key) to a single-mesh context and to the host
+ * primitive array teal reads (`eqns->primitive.data`, [num_cells][5]). The host state is uploaded
+ * now; every drop-in Advance call copies the new state back into that array while its last stage
+ * runs (tg_advance_host). A pageable array is page-locked in place (cudaHostRegister) until
+ * tg_unbind, which must come before teal frees it (equations_destroy). */
 int tg_bind(const void *eqns, tg_ctx *ctx, double *host_primitive);
 int tg_unbind(const void *eqns);
 

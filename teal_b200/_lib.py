@@ -127,6 +127,8 @@ SIGNATURES = [
     ("tg_residual", ctypes.c_int, [_vp, _vp, _vp]),
     ("tg_advance", ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_double, _dbl_p, ctypes.c_double,
                                   _vp, _dbl_p]),
+    ("tg_advance_host", ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_double, _dbl_p, ctypes.c_double,
+                                       _vp, _vp, _vp, _dbl_p]),
     ("tg_run", ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_double, ctypes.c_int, ctypes.c_double,
                               ctypes.c_int, ctypes.c_double, _dbl_p, _int_p, _vp]),
     ("tg_last_step", ctypes.c_int, [_vp, ctypes.c_int, _dbl_p]),

@@ -9,6 +9,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -183,6 +184,19 @@ struct Gmres {
 enum { SD_TIME, SD_STEP, SD_STEP0, SD_MAX_STEP, SD_MAX_TIME, SD_THRESHOLD, SD_RESIDUAL, SD_COUNT = SD_RESIDUAL + 5 };
 enum { SI_VARIABLE, SI_ITER, SI_MAX_ITER, SI_ACTIVE, SI_FAIL, SI_COUNT };
 
+// Chunks of a single-mesh context for steps whose host copies overlap the kernels (tg_advance_host):
+// cell chunks of consecutive cells (multiples of the gradient's 32-cell tiles), the inner faces whose
+// left cell lies in each chunk (teal sorts inner faces by their left cell), and the face chunks whose
+// flux records each cell chunk gathers (bit masks: at most 64 chunks)
+struct IoPlan {
+    int K = 0;
+    std::vector<int> cell_off;        // [K + 1]
+    std::vector<int> face_off;        // [K + 1]
+    std::vector<uint64_t> cell_face;  // [K]
+    cudaStream_t copy = nullptr;      // host copies
+    std::vector<cudaEvent_t> ev;      // [K + 1] a chunk's rows are gathered for the copy
+};
+
 struct tg_ctx {
     int device = 0;
     int source = TG_SOURCE_NONE;  // device source term kind and its parameters
@@ -194,6 +208,9 @@ struct tg_ctx {
     // sizes
     Sizes s{};
     int num_periodic = 0;  // periodic ghosts of the arena (redirected to their owners)
+    // work range of the next gradient / cell launches (cells) and face launches (faces); hi < 0: all
+    int cell_lo = 0, cell_hi = -1, face_lo = 0, face_hi = -1;
+    IoPlan *io = nullptr;  // chunks of the steps with overlapped host copies (built on first use)
 
     // equations (shared by every instance of the arena)
     int physics = 0, order = 2, flux = 0, viscous = 0, limiter = 0, precision = 0;
@@ -360,6 +377,11 @@ static void free_ctx(tg_ctx *c)
     if (c->hd) cudaFreeHost(c->hd);
     if (c->hi) cudaFreeHost(c->hi);
     if (c->pinned) cudaFreeHost(c->pinned);
+    if (c->io) {
+        if (c->io->copy) cudaStreamDestroy(c->io->copy);
+        for (cudaEvent_t e : c->io->ev) cudaEventDestroy(e);
+        delete c->io;
+    }
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
 }
@@ -1403,26 +1425,45 @@ static int run_boundary(tg_ctx *c, double *q, bool masked = false)
     return TG_OK;
 }
 
+// the context's sizes with the work range of its next cell-wise or face-wise launch
+static Sizes cell_sizes(const tg_ctx *c)
+{
+    Sizes s = c->s;
+    s.lo = c->cell_lo;
+    s.hi = c->cell_hi < 0 ? c->s.C : c->cell_hi;
+    return s;
+}
+
+static Sizes face_sizes(const tg_ctx *c)
+{
+    Sizes s = c->s;
+    s.lo = c->face_lo;
+    s.hi = c->face_hi < 0 ? c->s.F : c->face_hi;
+    return s;
+}
+
 template <typename R, bool MIXED>
 static void launch_gradient_s(tg_ctx *c, const Geometry<R> &g, bool fold, const double *q)
 {
-    dim3 grid((c->s.C + GRAD_CELLS - 1) / GRAD_CELLS);
+    const Sizes s = cell_sizes(c);
+    if (s.hi <= s.lo) return;
+    dim3 grid((s.hi - s.lo + GRAD_CELLS - 1) / GRAD_CELLS);
     R *rec = (R *)c->grad;
     switch (c->limiter) {
         case TG_LIMITER_NONE:
-            k_gradient<R, 0, true, MIXED, false><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec, c->st.error, c->wait_polls);
+            k_gradient<R, 0, true, MIXED, false><<<grid, GRAD_THREADS, 0, c->stream>>>(s, g, c->eps2, q, rec, c->st.error, c->wait_polls);
             break;
         case TG_LIMITER_BARTH_JESPERSEN:
             if (fold)
-                k_gradient<R, 1, true, MIXED, false><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec, c->st.error, c->wait_polls);
+                k_gradient<R, 1, true, MIXED, false><<<grid, GRAD_THREADS, 0, c->stream>>>(s, g, c->eps2, q, rec, c->st.error, c->wait_polls);
             else
-                k_gradient<R, 1, false, MIXED, false><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec, c->st.error, c->wait_polls);
+                k_gradient<R, 1, false, MIXED, false><<<grid, GRAD_THREADS, 0, c->stream>>>(s, g, c->eps2, q, rec, c->st.error, c->wait_polls);
             break;
         default:
             if (fold)
-                k_gradient<R, 2, true, MIXED, false><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec, c->st.error, c->wait_polls);
+                k_gradient<R, 2, true, MIXED, false><<<grid, GRAD_THREADS, 0, c->stream>>>(s, g, c->eps2, q, rec, c->st.error, c->wait_polls);
             else
-                k_gradient<R, 2, false, MIXED, false><<<grid, GRAD_THREADS, 0, c->stream>>>(c->s, g, c->eps2, q, rec, c->st.error, c->wait_polls);
+                k_gradient<R, 2, false, MIXED, false><<<grid, GRAD_THREADS, 0, c->stream>>>(s, g, c->eps2, q, rec, c->st.error, c->wait_polls);
             break;
     }
 }
@@ -1444,7 +1485,7 @@ static int run_gradient(tg_ctx *c, const double *q, int limiter_override = -1)
     bool fold = fold_psi(c);
     Launch l(c, TG_PROF_GRADIENT);
     if (is_exact(c)) {
-        GradientLaunch a{c->s,  c->g64, c->eps2,         q, (double *)c->grad, c->limiter, fold, !c->full_slots,
+        GradientLaunch a{cell_sizes(c), c->g64, c->eps2,  q, (double *)c->grad, c->limiter, fold, !c->full_slots,
                          c->st.error, c->wait_polls};
         cudaError_t e = launch_gradient_exact(a, c->stream);
         c->limiter = saved;
@@ -1463,7 +1504,7 @@ static int run_gradient(tg_ctx *c, const double *q, int limiter_override = -1)
 static int run_face(tg_ctx *c, const double *q)
 {
     FaceLaunch a;
-    a.s = c->s;
+    a.s = face_sizes(c);
     a.geom = is_fp64(c) ? (const void *)&c->g64 : (const void *)&c->g32;
     a.q = q;
     a.rec = c->grad;
@@ -1514,8 +1555,10 @@ static void launch_cell_s(tg_ctx *c, double alpha, int last, double *q, double *
     CellData cd{c->volume, c->proj, c->eps2};
     Source src{{c->src_par[0], c->src_par[1], c->src_par[2], c->src_par[3]},
                c->source == TG_SOURCE_DEVICE ? c->S : c->src_avg};
-    k_cell<MODE, NS, GT, SRC, false><<<(c->s.C + CELL_BLOCK - 1) / CELL_BLOCK, CELL_BLOCK, 0, c->stream>>>(
-        c->s, c->slot_face, c->slot_cnt, cd, (const GT *)c->G, c->U0, q, Rout, c->seg, c->st, alpha, last,
+    const Sizes s = cell_sizes(c);
+    if (s.hi <= s.lo) return;
+    k_cell<MODE, NS, GT, SRC, false><<<(s.hi - s.lo + CELL_BLOCK - 1) / CELL_BLOCK, CELL_BLOCK, 0, c->stream>>>(
+        s, c->slot_face, c->slot_cnt, cd, (const GT *)c->G, c->U0, q, Rout, c->seg, c->st, alpha, last,
         props_of(c), c->dtc, src, 0);
 }
 
@@ -1541,7 +1584,7 @@ static int launch_cell(tg_ctx *c, double alpha, int last, double *q, double *Rou
         a.ns = ns;
         a.source = c->source;
         a.two = (c->viscous == TG_VISCOUS_CENTRAL && c->order == 2) ? 1 : 0;
-        a.s = c->s;
+        a.s = cell_sizes(c);
         a.slot_face = c->slot_face;
         a.slot_cnt = c->slot_cnt;
         a.cd = CellData{c->volume, c->proj, c->eps2};
@@ -1576,8 +1619,8 @@ static int launch_cell(tg_ctx *c, double alpha, int last, double *q, double *Rou
     return TG_OK;
 }
 
-// boundary pass, gradient + limiter, face fluxes: everything of a residual before the gather
-static int run_fluxes(tg_ctx *c, double *q, bool masked = false)
+// what a residual needs before its gradients: the sources' Prepare pass and values, the boundary pass
+static int run_fluxes_pre(tg_ctx *c, double *q, bool masked)
 {
     for (size_t b = 0; b < c->bd_kernel.size(); b++) {
         if (!c->bd_kernel[b] && c->bd_kind[b] == TG_BC_CUSTOM)
@@ -1607,6 +1650,13 @@ static int run_fluxes(tg_ctx *c, double *q, bool masked = false)
         CU(cudaLaunchKernel(c->src_kernel, dim3((C + 127) / 128), dim3(128), args, 0, c->stream));
     }
     TRY(run_boundary(c, q, masked));
+    return TG_OK;
+}
+
+// boundary pass, gradient + limiter, face fluxes: everything of a residual before the gather
+static int run_fluxes(tg_ctx *c, double *q, bool masked = false)
+{
+    TRY(run_fluxes_pre(c, q, masked));
     if (c->order == 2) TRY(run_gradient(c, q));
     TRY(run_face(c, q));
     return TG_OK;
@@ -1907,6 +1957,197 @@ extern "C" int tg_advance(tg_ctx *c, int method, const void *context, double cou
     TRY(write_steps(c));
     TRY(step_graph(c, method, stages, alpha, courant, 0));
     TRY(launch_step(c, stages, alpha, courant));
+    TRY(read_steps(c));
+    TRY(check_error(c));
+    *time = hd_at(c, SD_TIME, 0);
+    if (residual) residual_of(c, 0, residual);
+    if (step0) *step0 = hd_at(c, SD_STEP0, 0);
+    return TG_OK;
+}
+
+// ---- steps with overlapped host copies ----------------------------------------------------------
+//
+// tg_advance_host takes one step from a host state to a host state. The new state goes down chunk
+// by chunk while the last stage runs: that stage's face fluxes and cell updates run in chunks of
+// consecutive cells, and each chunk's rows are copied to the host (copy stream) as soon as they are
+// final. Every element is computed by the same kernel with the same operations as in an unsplit
+// step, so the results are the same bits. (The first stage split the same way behind a chunked
+// upload gained nothing: the stage kernels run 2-3 times slower while a host copy is in flight.)
+
+#ifndef TG_IO_CHUNKS
+#define TG_IO_CHUNKS 8
+#endif
+constexpr int IO_CHUNKS = TG_IO_CHUNKS;
+
+static uint64_t io_bit(int k) { return uint64_t(1) << k; }
+
+static int build_io_plan(tg_ctx *c)
+{
+    const int C = c->s.C, F = c->s.F, Fin = c->s.F_in;
+    std::unique_ptr<IoPlan> p(new IoPlan);
+    // chunks of at least 64 gradient tiles
+    int K = std::max(1, std::min(IO_CHUNKS, C / (64 * GRAD_CELLS)));
+    const int per = ((C + K - 1) / K + GRAD_CELLS - 1) / GRAD_CELLS * GRAD_CELLS;
+    K = (C + per - 1) / per;
+    std::vector<int2> lr(F);
+    if (F > 0) {
+        CU(cudaMemcpyAsync(lr.data(), c->lr, sizeof(int2) * F, cudaMemcpyDeviceToHost, c->stream));
+        CU(cudaStreamSynchronize(c->stream));
+    }
+    bool sorted = true;
+    for (int f = 1; f < Fin && sorted; f++) sorted = lr[f].x >= lr[f - 1].x;
+    if (!sorted) K = 1;  // face chunks need inner faces ordered by their left cell
+    const int step = (K == 1) ? C : per;
+    p->K = K;
+    p->cell_off.resize(K + 1);
+    p->face_off.resize(K + 1);
+    for (int k = 0; k <= K; k++) p->cell_off[k] = std::min(C, k * step);
+    for (int k = 0; k < K; k++) {
+        int lo = 0, hi = Fin;  // first inner face whose left cell is >= cell_off[k]
+        while (lo < hi) {
+            int mid = lo + (hi - lo) / 2;
+            if (lr[mid].x < p->cell_off[k]) lo = mid + 1;
+            else hi = mid;
+        }
+        p->face_off[k] = lo;
+    }
+    p->face_off[0] = 0;
+    p->face_off[K] = Fin;
+    auto chunk = [&](int cell) { return std::min(K - 1, cell / step); };
+    p->cell_face.assign(K, 0);
+    for (int f = 0; f < Fin; f++) {
+        const int kl = chunk(lr[f].x), kr = chunk(lr[f].y);
+        p->cell_face[kl] |= io_bit(kl);
+        p->cell_face[kr] |= io_bit(kl);
+    }
+    CU(cudaStreamCreateWithFlags(&p->copy, cudaStreamNonBlocking));
+    p->ev.resize(K + 1, nullptr);
+    for (int k = 0; k <= K; k++) CU(cudaEventCreateWithFlags(&p->ev[k], cudaEventDisableTiming));
+    c->io = p.release();
+    return TG_OK;
+}
+
+static bool host_pinned(const void *ptr)
+{
+    cudaPointerAttributes at;
+    bool pinned = cudaPointerGetAttributes(&at, ptr) == cudaSuccess && at.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    return pinned;
+}
+
+// the step with its last stage in chunks, each chunk's rows copied into the pinned host array `out`
+// (or none with out == null); on return the copy stream has finished (also after an error)
+static int advance_chunked(tg_ctx *c, int stages, const double *alpha, double courant, double *out)
+{
+    IoPlan &p = *c->io;
+    const int K = p.K, C = c->s.C, Fin = c->s.F_in, F = c->s.F;
+    const long N = c->s.N;
+    const int rows = c->inst_row_off[1];
+    std::vector<char> fl(K, 0);
+    {
+        Launch l(c, TG_PROF_REDUCE);
+        k_inst_begin<<<c->ninst, INST_BLOCK, 0, c->stream>>>(c->seg, c->part_min, courant, c->st);
+    }
+    CU(cudaGetLastError());
+    // the stages before the last one as in an unsplit step
+    int i = 0;
+    for (; i < stages - 1; i++) {
+        c->t_time = c->st.time, c->t_step = c->st.step, c->t_coef = alpha[i];
+        TRY(run_fluxes(c, c->q, true));
+        TRY(launch_cell<1>(c, alpha[i + 1], 0, c->q, c->R));
+    }
+    // the last stage: sources, boundary ghosts, gradients and the boundary and periodic faces whole,
+    // then the inner faces and the cell updates chunk by chunk
+    c->t_time = c->st.time, c->t_step = c->st.step, c->t_coef = alpha[i];
+    TRY(run_fluxes_pre(c, c->q, true));
+    if (c->order == 2) TRY(run_gradient(c, c->q));
+    c->face_lo = Fin, c->face_hi = F;
+    TRY(run_face(c, c->q));
+    for (int k = 0; k < K; k++) {
+        for (int j = 0; j < K; j++) {
+            if (!fl[j] && (p.cell_face[k] & io_bit(j))) {
+                c->face_lo = p.face_off[j], c->face_hi = p.face_off[j + 1];
+                TRY(run_face(c, c->q));
+                fl[j] = 1;
+            }
+        }
+        c->cell_lo = p.cell_off[k], c->cell_hi = p.cell_off[k + 1];
+        TRY(launch_cell<1>(c, alpha[i + 1], 1, c->q, c->R));
+        c->cell_lo = 0, c->cell_hi = -1;
+        if (out) {
+            const int r0 = p.cell_off[k], n = p.cell_off[k + 1] - r0;
+            k_rows_gather<<<grid_of(n), BLOCK, 0, c->stream>>>(n, c->rowmap + r0, (int)N, c->q, c->aos + 5 * (size_t)r0);
+            CU(cudaGetLastError());
+            CU(cudaEventRecord(p.ev[k], c->stream));
+            CU(cudaStreamWaitEvent(p.copy, p.ev[k], 0));
+            CU(cudaMemcpyAsync(out + 5 * (size_t)r0, c->aos + 5 * (size_t)r0, sizeof(double) * 5 * (size_t)n,
+                               cudaMemcpyDeviceToHost, p.copy));
+        }
+    }
+    c->face_lo = 0, c->face_hi = -1;
+    // ghost rows (boundary ghosts as the last boundary pass left them, periodic ghosts from their owners)
+    if (out && rows > C) {
+        const int n = rows - C;
+        k_rows_gather<<<grid_of(n), BLOCK, 0, c->stream>>>(n, c->rowmap + C, (int)N, c->q, c->aos + 5 * (size_t)C);
+        CU(cudaGetLastError());
+        CU(cudaEventRecord(p.ev[K], c->stream));
+        CU(cudaStreamWaitEvent(p.copy, p.ev[K], 0));
+        CU(cudaMemcpyAsync(out + 5 * (size_t)C, c->aos + 5 * (size_t)C, sizeof(double) * 5 * (size_t)n,
+                           cudaMemcpyDeviceToHost, p.copy));
+    }
+    TRY(run_pieces(c, 1));
+    {
+        Launch l(c, TG_PROF_REDUCE);
+        k_inst_end<<<c->ninst, INST_BLOCK, 0, c->stream>>>(c->seg, c->part_sum, 1, c->st);
+    }
+    {
+        Launch l(c, TG_PROF_REDUCE);
+        k_count_active<<<1, 256, 0, c->stream>>>(c->ninst, c->st);
+    }
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(p.copy));
+    return TG_OK;
+}
+
+extern "C" int tg_advance_host(tg_ctx *c, int method, const void *context, double courant, double *time,
+                               double max_step, const double *prim_in, double *prim_out, double *residual,
+                               double *step0)
+{
+    if (!c || !time) return fail(TG_ERR_INVALID, "null argument");
+    if (c->ninst != 1)
+        return fail(TG_ERR_INVALID, "tg_advance_host takes a single-mesh context (batches: tg_batch_run)");
+    if (prim_in) TRY(tg_set_primitive(c, prim_in));
+    // the last stage runs in chunks when the new state goes to pinned host memory (pageable memory
+    // goes through the staging buffer in one piece)
+    const bool chunked = (method == TG_ADVANCE_EULER || method == TG_ADVANCE_LSERK) && c->halo == 0 &&
+                         c->nsend == 0 && !c->prof_on && prim_out && host_pinned(prim_out);
+    if (!chunked) {
+        TRY(tg_advance(c, method, context, courant, time, max_step, residual, step0));
+        if (prim_out) TRY(tg_get_primitive(c, prim_out));
+        return TG_OK;
+    }
+    if (!(courant > 0)) return fail(TG_ERR_INVALID, "invalid courant number (%g)", courant);
+    int stages;
+    const double *alpha;
+    TRY(rk_params(c, method, context, &stages, &alpha));
+    if (!c->io) TRY(build_io_plan(c));
+    if (!c->prepared) TRY(run_prepare(c));
+    hd_at(c, SD_TIME, 0) = *time;
+    hd_at(c, SD_MAX_STEP, 0) = max_step;
+    hd_at(c, SD_THRESHOLD, 0) = 0;
+    hi_at(c, SI_ITER, 0) = 0;
+    hi_at(c, SI_MAX_ITER, 0) = 0x7fffffff;
+    hi_at(c, SI_ACTIVE, 0) = 1;
+    hi_error(c) = 0;
+    TRY(write_steps(c));
+    const int rc = advance_chunked(c, stages, alpha, courant, prim_out);
+    c->cell_lo = 0, c->cell_hi = -1, c->face_lo = 0, c->face_hi = -1;
+    if (rc != TG_OK) {
+        // nothing may still write into the caller's buffer once this returns
+        cudaStreamSynchronize(c->stream);
+        cudaStreamSynchronize(c->io->copy);
+        return rc;
+    }
     TRY(read_steps(c));
     TRY(check_error(c));
     *time = hd_at(c, SD_TIME, 0);
@@ -2477,6 +2718,7 @@ extern "C" int tg_layout(tg_ctx *c, const char *name, void *out, long count)
 struct Binding {
     tg_ctx *ctx;
     double *host_primitive;
+    bool registered;  // page-locked in place by tg_bind (the step's copies then reach it directly)
 };
 static std::map<const void *, Binding> g_bindings;
 static std::mutex g_bind_mutex;
@@ -2484,23 +2726,37 @@ static std::mutex g_bind_mutex;
 extern "C" int tg_bind(const void *eqns, tg_ctx *c, double *host_primitive)
 {
     if (!eqns || !c || !host_primitive) return fail(TG_ERR_INVALID, "null argument");
+    if (c->ninst != 1) return fail(TG_ERR_INVALID, "tg_bind takes a single-mesh context");
     TRY(tg_set_primitive(c, host_primitive));
     std::lock_guard<std::mutex> lock(g_bind_mutex);
-    g_bindings[eqns] = Binding{c, host_primitive};
+    auto old = g_bindings.find(eqns);
+    if (old != g_bindings.end() && old->second.registered) cudaHostUnregister(old->second.host_primitive);
+    // teal's primitive array (teal_calloc, pageable) is page-locked in place, so each step's state
+    // goes down into it by DMA, chunk by chunk while the last stage runs; where that is refused the
+    // copies go through the context's pinned staging buffer
+    const size_t bytes = sizeof(double) * 5 * (size_t)c->inst_row_off[1];
+    bool reg = !host_pinned(host_primitive) &&
+               cudaHostRegister(host_primitive, bytes, cudaHostRegisterDefault) == cudaSuccess;
+    cudaGetLastError();
+    g_bindings[eqns] = Binding{c, host_primitive, reg};
     return TG_OK;
 }
 
 extern "C" int tg_unbind(const void *eqns)
 {
     std::lock_guard<std::mutex> lock(g_bind_mutex);
-    g_bindings.erase(eqns);
+    auto it = g_bindings.find(eqns);
+    if (it != g_bindings.end()) {
+        if (it->second.registered) cudaHostUnregister(it->second.host_primitive);
+        g_bindings.erase(it);
+    }
     return TG_OK;
 }
 
 static double dropin(int method, const void *eqns, double *time, void *residual, double max_step,
                      double courant, const void *context)
 {
-    Binding b{nullptr, nullptr};
+    Binding b{nullptr, nullptr, false};
     {
         std::lock_guard<std::mutex> lock(g_bind_mutex);
         auto it = g_bindings.find(eqns);
@@ -2508,8 +2764,10 @@ static double dropin(int method, const void *eqns, double *time, void *residual,
     }
     double step0 = 0;
     int rc = b.ctx ? TG_OK : fail(TG_ERR_INVALID, "equations are not bound to a device context");
-    if (rc == TG_OK) rc = tg_advance(b.ctx, method, context, courant, time, max_step, (double *)residual, &step0);
-    if (rc == TG_OK) rc = tg_get_primitive(b.ctx, b.host_primitive);
+    // the step, with the new state copied into teal's array while the last stage runs
+    if (rc == TG_OK)
+        rc = tg_advance_host(b.ctx, method, context, courant, time, max_step, nullptr, b.host_primitive,
+                             (double *)residual, &step0);
     if (rc != TG_OK) {
         fprintf(stderr, "[0] ERROR: %s\n", tg_last_error());
         fflush(stderr);

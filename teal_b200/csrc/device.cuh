@@ -65,6 +65,10 @@ struct CellData {
 struct Sizes {
     int C, N, F, F_in, F_bd;
     int SL;  // leading dimension of the per-cell slot arrays: C rounded up to 4 (16-byte rows)
+    // work range of one launch of the gradient, face and cell kernels, which a step whose host copies
+    // overlap its kernels splits in chunks: cells [lo, hi) (gradient: lo a multiple of 32; cell
+    // kernel) or faces [lo, hi) (face kernels); the launchers set it, [0, C) / [0, F) when unsplit
+    int lo, hi;
 };
 
 // Instances packed in one arena (a single mesh is one instance). Inner cells of instance i are

@@ -282,8 +282,8 @@ __global__ void __launch_bounds__(FACE_BLOCK, face_minb<R>(NS)) k_face(Sizes s, 
                                                    R *__restrict__ G, PressureRefOf<R> pr_ref)
 {
     static_assert(X == kExact, "exact kernels live in the exact translation units only");
-    const int f = blockIdx.x * FACE_BLOCK + threadIdx.x;
-    if (f >= s.F) {
+    const int f = s.lo + blockIdx.x * FACE_BLOCK + threadIdx.x;
+    if (f >= s.hi) {
         return;
     }
     DirectGeo<R> geo{g, s.F, f};
@@ -302,8 +302,8 @@ __global__ void __launch_bounds__(FACE_BLOCK, face_minb<R>(NS)) k_face_staged(Si
 {
     static_assert(X == kExact, "exact kernels live in the exact translation units only");
     __shared__ __align__(16) FaceTile<R, ORDER, NS> t;
-    const int f0 = blockIdx.x * FACE_BLOCK;
-    const int n = min(FACE_BLOCK, s.F - f0);
+    const int f0 = s.lo + blockIdx.x * FACE_BLOCK;
+    const int n = min(FACE_BLOCK, s.hi - f0);
     if (!t.stage(g, s.F, f0, n, err, polls)) {
         return;
     }

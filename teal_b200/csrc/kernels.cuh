@@ -72,9 +72,9 @@ __global__ void __launch_bounds__(GRAD_THREADS, GRAD_MINB) k_gradient(Sizes s, G
     __shared__ int s_cnt[MIXED ? GRAD_CELLS : 1];
     __shared__ uint64_t bar;
     __shared__ int s_J;
-    const int C = s.C;
-    const int base = blockIdx.x * GRAD_CELLS;
-    const int ncell = min(GRAD_CELLS, C - base);
+    const int tile = s.lo / GRAD_CELLS + blockIdx.x;
+    const int base = tile * GRAD_CELLS;
+    const int ncell = min(GRAD_CELLS, s.hi - base);
     const int v = threadIdx.x / GRAD_CELLS;  // variable of this warp
     const int l = threadIdx.x % GRAD_CELLS;
     const int c = base + min(l, ncell - 1);
@@ -84,17 +84,17 @@ __global__ void __launch_bounds__(GRAD_THREADS, GRAD_MINB) k_gradient(Sizes s, G
         // the whole tile by bulk copies; its slot count is the tile's largest, so a warp of
         // tetrahedra stops after 4
         if (threadIdx.x == 0) {
-            const long long t0 = __ldg(g.gtile_off + blockIdx.x);
-            const int J = int((__ldg(g.gtile_off + blockIdx.x + 1) - t0) / grad_tile_bytes<R>(1));
+            const long long t0 = __ldg(g.gtile_off + tile);
+            const int J = int((__ldg(g.gtile_off + tile + 1) - t0) / grad_tile_bytes<R>(1));
             s_J = J;
-            const unsigned char *tile = g.gtile + t0;
+            const unsigned char *tile_p = g.gtile + t0;
             const uint32_t nb = uint32_t(grad_tile_nbr_bytes<R>(J)), vb = uint32_t(grad_tile_vec_bytes<R>(J));
             mbar_init(&bar, 1);
             mbar_arrive_expect_tx(&bar, nb + vb + (LIM != 0 ? vb : 0u));
-            bulk_g2s(&s_nbr[0][0], tile, nb, &bar);
-            bulk_g2s(&s_w[0][0], tile + nb, vb, &bar);
+            bulk_g2s(&s_nbr[0][0], tile_p, nb, &bar);
+            bulk_g2s(&s_w[0][0], tile_p + nb, vb, &bar);
             if (LIM != 0) {
-                bulk_g2s(&s_off[0][0], tile + nb + vb, vb, &bar);
+                bulk_g2s(&s_off[0][0], tile_p + nb + vb, vb, &bar);
             }
         }
         if (threadIdx.x < GRAD_CELLS) {
@@ -106,18 +106,18 @@ __global__ void __launch_bounds__(GRAD_THREADS, GRAD_MINB) k_gradient(Sizes s, G
         // and offsets come by bulk copies; meanwhile the threads read their neighbour rows from the
         // tile's first part themselves and gather the neighbours' states (padding slots name the
         // cell itself), so the gathers overlap the copies
-        const unsigned char *tile = g.gtile + (size_t)blockIdx.x * (size_t)grad_tile_bytes<R>(MAX_SLOTS);
+        const unsigned char *tile_p = g.gtile + (size_t)tile * (size_t)grad_tile_bytes<R>(MAX_SLOTS);
         constexpr uint32_t nb = uint32_t(grad_tile_nbr_bytes<R>(MAX_SLOTS));
         constexpr uint32_t vb = uint32_t(grad_tile_vec_bytes<R>(MAX_SLOTS));
         if (threadIdx.x == 0) {
             mbar_init(&bar, 1);
             mbar_arrive_expect_tx(&bar, vb + (LIM != 0 ? vb : 0u));
-            bulk_g2s(&s_w[0][0], tile + nb, vb, &bar);
+            bulk_g2s(&s_w[0][0], tile_p + nb, vb, &bar);
             if (LIM != 0) {
-                bulk_g2s(&s_off[0][0], tile + nb + vb, vb, &bar);
+                bulk_g2s(&s_off[0][0], tile_p + nb + vb, vb, &bar);
             }
         }
-        const int *nbr = reinterpret_cast<const int *>(tile);
+        const int *nbr = reinterpret_cast<const int *>(tile_p);
 #pragma unroll
         for (int j = 0; j < MAX_SLOTS; j++) {
             qn[j] = __ldg(qv + __ldg(nbr + j * GRAD_CELLS + l));
@@ -296,8 +296,8 @@ __global__ void __launch_bounds__(CELL_BLOCK, CELL_MINB) k_cell(Sizes s, const i
 {
     static_assert(X == kExact, "exact kernels live in the exact translation units only");
     const int C = s.C, N = s.N;
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= C) {
+    int c = s.lo + blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= s.hi) {
         return;
     }
     // the stage update's inputs do not depend on the face records: their loads are issued first so

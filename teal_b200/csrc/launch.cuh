@@ -29,7 +29,10 @@ template <typename R, int FK, bool NS, int ORDER, bool FOLD>
 inline void launch_face_v(bool staged, const FaceLaunch &a, const Geometry<R> &g, const R *rec, R *G, cudaStream_t st)
 {
     constexpr bool X = kExact;
-    dim3 grid((a.s.F + FACE_BLOCK - 1) / FACE_BLOCK);
+    if (a.s.hi <= a.s.lo) {
+        return;
+    }
+    dim3 grid((a.s.hi - a.s.lo + FACE_BLOCK - 1) / FACE_BLOCK);
     R gm = R(a.gamma), mu = R(a.mu), pr = R(a.prandtl);
     PressureRefOf<R> pref{};
     if constexpr (sizeof(R) == sizeof(float)) {

@@ -13,7 +13,8 @@ static_assert(kExact, "stage_exact.cu is compiled with TG_EXACT_TU=1");
 template <bool MIXED>
 static void gradient_m(const GradientLaunch &a, cudaStream_t st)
 {
-    dim3 grid((a.s.C + GRAD_CELLS - 1) / GRAD_CELLS);
+    if (a.s.hi <= a.s.lo) return;
+    dim3 grid((a.s.hi - a.s.lo + GRAD_CELLS - 1) / GRAD_CELLS);
     switch (a.limiter) {
         case 0: k_gradient<double, 0, true, MIXED, true><<<grid, GRAD_THREADS, 0, st>>>(a.s, a.g, a.eps2, a.q, a.rec, a.err, a.polls); break;
         case 1:
@@ -43,7 +44,8 @@ cudaError_t launch_gradient_exact(const GradientLaunch &a, cudaStream_t st)
 template <int MODE, bool NS, int SRC>
 static void cell_s(const CellLaunch &a, cudaStream_t st)
 {
-    k_cell<MODE, NS, double, SRC, true><<<(a.s.C + CELL_BLOCK - 1) / CELL_BLOCK, CELL_BLOCK, 0, st>>>(
+    if (a.s.hi <= a.s.lo) return;
+    k_cell<MODE, NS, double, SRC, true><<<(a.s.hi - a.s.lo + CELL_BLOCK - 1) / CELL_BLOCK, CELL_BLOCK, 0, st>>>(
         a.s, a.slot_face, a.slot_cnt, a.cd, a.G, a.U0, a.q, a.Rout, a.seg, a.st, a.alpha, a.last, a.prop, a.dtc,
         a.src, a.two);
 }
