@@ -1972,8 +1972,8 @@ extern "C" int tg_advance(tg_ctx *c, int method, const void *context, double cou
 // consecutive cells, and each chunk's rows are copied to the host (copy stream) as soon as they are
 // final. Every element is computed by the same kernel with the same operations as in an unsplit
 // step, so the results are the same bits. (The first stage split the same way behind a chunked
-// upload gained nothing: periodic wraps and the face fluxes' look-ahead delay the chunks, and each
-// chunk boundary costs a kernel tail.)
+// upload gained nothing: in teal's breadth-first cell order periodic links join cells far apart,
+// so most chunks' gradients wait for chunks that arrive late, and each chunk costs a kernel tail.)
 
 #ifndef TG_IO_CHUNKS
 #define TG_IO_CHUNKS 8
