@@ -132,3 +132,20 @@ def test_implicit_method_and_shape_errors():
         ctx.advance_host(tb.TG_ADVANCE_LSERK, 0.9, 0.0, prim_in=start[:10])
     with pytest.raises(tb.TealError):
         ctx.advance_host(tb.TG_ADVANCE_LSERK, 0.9, 0.0, prim_out=np.zeros((want.shape[0], 5), np.float32))
+
+
+def test_one_chunk_mesh_and_batch_rejection():
+    # a mesh too small to split (one chunk) takes the same path with a single chunk
+    seq, ovl = run_pair(tgv(8), tb.TG_PRECISION_FP64, tb.TG_ADVANCE_LSERK, (3, 3), 2, pinned=True)
+    assert_same(seq, ovl)
+    # a batch arena has no single host state
+    import ctypes
+
+    from teal_b200 import _lib
+
+    b = tb.Batch([tgv(8), tgv(8)])
+    t = ctypes.c_double(0.0)
+    status = _lib.lib.tg_advance_host(b.handle, tb.TG_ADVANCE_LSERK, None, 0.9, ctypes.byref(t), 1e300, None, None,
+                                      None, None)
+    assert status == _lib.TG_ERR_INVALID
+    b.close()
