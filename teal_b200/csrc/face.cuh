@@ -137,6 +137,62 @@ struct FaceTile {
     __device__ __forceinline__ R corr_norm(int i) const { return at(R_CORR + 3, i); }
 };
 
+// Viscous flux of face f (element i of its tile): the face average of both cells' states and
+// unlimited gradients, corrected along the centre-to-centre direction, in the face normal's frame
+template <typename R, typename Geo>
+__device__ __forceinline__ Cons<R> viscous_face(const Geo &geo, int i, bool boundary, int2 c, int N,
+                                                const double *__restrict__ q, const R *__restrict__ rec, R gamma,
+                                                R mu, R prandtl)
+{
+    // face average corrected along the centre-to-centre direction (derivative.c:71-89)
+    Prim<R> ql = reload_prim<R>(q, N, c.x);
+    Prim<R> qr = reload_prim<R>(q, N, c.y);
+    R qlv[5] = {ql.rho, ql.u.x, ql.u.y, ql.u.z, ql.p};
+    R qrv[5] = {qr.rho, qr.u.x, qr.u.y, qr.u.z, qr.p};
+    R qm[5], gm[15];
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        qm[v] = (qlv[v] + qrv[v]) / R(2);
+    }
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        R ax, ay, az, ap, bx, by, bz, bp;
+        grad_rec_load(rec, c.x, v, ax, ay, az, ap);
+        if (boundary) {
+            gm[3 * v] = ax, gm[3 * v + 1] = ay, gm[3 * v + 2] = az;
+        }
+        else {
+            grad_rec_load(rec, c.y, v, bx, by, bz, bp);
+            gm[3 * v] = (ax + bx) / R(2), gm[3 * v + 1] = (ay + by) / R(2), gm[3 * v + 2] = (az + bz) / R(2);
+        }
+    }
+    V3<R> unit = geo.corr(i);
+    const R cnorm = geo.corr_norm(i);
+    const R inv_norm = R(1) / cnorm;
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        V3<R> gv = v3(gm[3 * v], gm[3 * v + 1], gm[3 * v + 2]);
+        const R dq = qrv[v] - qlv[v];
+        R adjust = dot(gv, unit) - (kExact ? (dq / cnorm) : (dq * inv_norm));
+        gv = sub(gv, mul(adjust, unit));
+        gm[3 * v] = gv.x;
+        gm[3 * v + 1] = gv.y;
+        gm[3 * v + 2] = gv.z;
+    }
+    Grad<R> gg;
+    gg.rho = v3(gm[0], gm[1], gm[2]);
+    gg.ux = v3(gm[3], gm[4], gm[5]);
+    gg.uy = v3(gm[6], gm[7], gm[8]);
+    gg.uz = v3(gm[9], gm[10], gm[11]);
+    gg.p = v3(gm[12], gm[13], gm[14]);
+    // the viscous flux needs only the normal row of the basis
+    Basis<R> nb;
+    nb.x = geo.normal_again(i);
+    nb.y = nb.x;
+    nb.z = nb.x;
+    return viscous_central(prim_from(qm), gg, gamma, mu, prandtl, nb);
+}
+
 // The flux record of face f (element i of its tile). The convective flux comes first (its
 // reconstruction streams the limited gradients), the viscous flux second (its face-averaged
 // gradient re-reads the unlimited gradients, which are still in L1).
@@ -211,53 +267,7 @@ __device__ __forceinline__ void face_flux(const Geo &geo, int i, int f, const Si
     R gf[5] = {fc.rho * area, fc.m.x * area, fc.m.y * area, fc.m.z * area, fc.e * area};
 
     if (NS && ORDER == 2) {
-        // face average corrected along the centre-to-centre direction (derivative.c:71-89)
-        Prim<R> ql = reload_prim<R>(q, N, c.x);
-        Prim<R> qr = reload_prim<R>(q, N, c.y);
-        R qlv[5] = {ql.rho, ql.u.x, ql.u.y, ql.u.z, ql.p};
-        R qrv[5] = {qr.rho, qr.u.x, qr.u.y, qr.u.z, qr.p};
-        R qm[5], gm[15];
-#pragma unroll
-        for (int v = 0; v < 5; v++) {
-            qm[v] = (qlv[v] + qrv[v]) / R(2);
-        }
-#pragma unroll
-        for (int v = 0; v < 5; v++) {
-            R ax, ay, az, ap, bx, by, bz, bp;
-            grad_rec_load(rec, c.x, v, ax, ay, az, ap);
-            if (boundary) {
-                gm[3 * v] = ax, gm[3 * v + 1] = ay, gm[3 * v + 2] = az;
-            }
-            else {
-                grad_rec_load(rec, c.y, v, bx, by, bz, bp);
-                gm[3 * v] = (ax + bx) / R(2), gm[3 * v + 1] = (ay + by) / R(2), gm[3 * v + 2] = (az + bz) / R(2);
-            }
-        }
-        V3<R> unit = geo.corr(i);
-        const R cnorm = geo.corr_norm(i);
-        const R inv_norm = R(1) / cnorm;
-#pragma unroll
-        for (int v = 0; v < 5; v++) {
-            V3<R> gv = v3(gm[3 * v], gm[3 * v + 1], gm[3 * v + 2]);
-            const R dq = qrv[v] - qlv[v];
-            R adjust = dot(gv, unit) - (kExact ? (dq / cnorm) : (dq * inv_norm));
-            gv = sub(gv, mul(adjust, unit));
-            gm[3 * v] = gv.x;
-            gm[3 * v + 1] = gv.y;
-            gm[3 * v + 2] = gv.z;
-        }
-        Grad<R> gg;
-        gg.rho = v3(gm[0], gm[1], gm[2]);
-        gg.ux = v3(gm[3], gm[4], gm[5]);
-        gg.uy = v3(gm[6], gm[7], gm[8]);
-        gg.uz = v3(gm[9], gm[10], gm[11]);
-        gg.p = v3(gm[12], gm[13], gm[14]);
-        // the viscous flux needs only the normal row of the basis
-        Basis<R> nb;
-        nb.x = geo.normal_again(i);
-        nb.y = nb.x;
-        nb.z = nb.x;
-        Cons<R> fv = viscous_central(prim_from(qm), gg, gamma, mu, prandtl, nb);
+        const Cons<R> fv = viscous_face<R>(geo, i, boundary, c, N, q, rec, gamma, mu, prandtl);
         if constexpr (kExact) {
             const R gv[5] = {fv.rho * area, fv.m.x * area, fv.m.y * area, fv.m.z * area, fv.e * area};
             flux_rec_store(G + flux_rec2_offset(s.F), s.F, f, gv);
