@@ -401,7 +401,7 @@ def run_split(args, world, rank, pg):
 
 
 def run_serving(args, world, rank):
-    """Serving benchmark: seeded Poisson arrivals of steady solve requests on
+    """Serving benchmark (the continuous-batching solve server): seeded Poisson arrivals of steady solve requests on
     the batch workload's ramp meshes (20k-2M cells, log-uniform), Mach 0.2-3.0, Euler or
     Navier-Stokes, flux scheme (roe / hllc / ausmd) and tolerance 1e-6..1e-10 per request, implicit
     Euler with teal's steady Newton-Krylov settings; served with continuous batching (lanes of one
@@ -509,8 +509,8 @@ def batch_problem(spec, flux="ausmd", limiter=("minmod", 0.0)):
 
 
 def run_batch_implicit(args, specs):
-    """Batched steady solves: every instance takes implicit Euler steps until its
-    maximum residual has dropped by `--drop` (1e-8) from its first step's, or `--steps` steps, in
+    """Batched steady solves on `--instances` ramp meshes of 8k-512k cells: every instance takes
+    implicit Euler steps until its maximum residual has dropped by `--drop` (1e-8) from its first step's, or `--steps` steps, in
     FP64 and in the FP32-matvec form (FP64 Newton residuals and Arnoldi, FP32 fluxes in the
     finite-difference matvec); all instances in one arena, each step one CUDA-graph launch with
     device-driven Newton / Arnoldi / Gram-Schmidt loops. The scheme is teal's steady airfoil case's
