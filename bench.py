@@ -510,8 +510,8 @@ def batch_problem(spec, flux="ausmd", limiter=("minmod", 0.0)):
 
 def run_batch_implicit(args, specs):
     """Batched steady solves on `--instances` ramp meshes of 8k-512k cells: every instance takes
-    implicit Euler steps until its maximum residual has dropped by `--drop` (1e-8) from its first step's, or `--steps` steps, in
-    FP64 and in the FP32-matvec form (FP64 Newton residuals and Arnoldi, FP32 fluxes in the
+    implicit Euler steps until its maximum residual has dropped by `--drop` (1e-8) from its first
+    step's, or `--steps` steps, in FP64 and in the FP32-matvec form (FP64 Newton residuals and Arnoldi, FP32 fluxes in the
     finite-difference matvec); all instances in one arena, each step one CUDA-graph launch with
     device-driven Newton / Arnoldi / Gram-Schmidt loops. The scheme is teal's steady airfoil case's
     (run/airfoil/run.c: hllc, Venkatakrishnan(1), Newton-Krylov {0.1, 0.3, 30}) at CFL 30: from the
